@@ -1,0 +1,180 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Run from the repository root after ``make -C oracle``:
+
+    python tests/golden/make_golden.py
+
+It needs the reference sources (for the shipped 4^3x8 configuration and the
+reference build in oracle/_ref).  Outputs are committed, so the tests (and the
+GPU box, which has no reference tree) only read them.
+
+Fixtures
+--------
+lat400.npz   4^3x8 configuration shipped with the reference (CONF/lat..400),
+             read by GLU's own NERSC reader, plus reference results:
+               Landau FACG / FASD (line-search SD) / FASD (GLU_GFIX_SD build,
+               fixed step), Coulomb FACG / FASD (GLU_GFIX_SD build)
+hb8.npz      8^4 SU(3) configuration from GLU's heatbath (beta 6.0, cold
+             start, seed 1, 500 sweeps of KP heatbath + 4 over-relaxation,
+             8 OpenMP threads), plus reference Landau FACG (alpha 0.08,
+             theta < 1e-14)
+
+Each solve stores the 1-thread reference trajectory (theta and functional at
+every derivative evaluation, SD start included), the iteration count, the
+final theta and the final links (hb8: every 8th site), and -- for Landau
+FACG -- the first 60
+in-loop thetas of the same reference run with 8 OpenMP threads.  The two
+reference runs differ only in summation order; their distance is the
+reference's own reproducibility envelope used as the trajectory tolerance.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+from oracle.oracle import REF_BIN, Reference  # noqa: E402
+
+REF = Path(os.environ.get("GLU_REFERENCE", "/root/reference"))
+OUT = Path(__file__).resolve().parent
+ENVELOPE_ITERS = 60
+
+HB_INPUT = """MODE = HEATBATH
+HEADER = UNIT
+    DIM_0 = 8
+    DIM_1 = 8
+    DIM_2 = 8
+    DIM_3 = 8
+CONFNO = 0
+RANDOM_TRANSFORM = NO
+SEED = 1
+GFTYPE = LANDAU
+    GF_TUNE = 0.08
+    ACCURACY = 14
+    MAX_ITERS = 650
+CUTTYPE = GLUON_PROPS
+    FIELD_DEFINITION = LINEAR
+    MOM_CUT = CYLINDER_CUT
+    MAX_T = 7
+    MAXMOM = 4
+    CYL_WIDTH = 2.0
+    ANGLE = 60
+    OUTPUT = ./
+SMEARTYPE = APE
+    DIRECTION = ALL
+    SMITERS = 100
+    ALPHA1 = 0.6
+    ALPHA2 = 0.4
+    ALPHA3 = 0.2
+U1_MEAS = U1_RECTANGLE
+    U1_ALPHA = 0.07957753876221914
+    U1_CHARGE = -1.0
+CONFIG_INFO = glu_b200_golden
+    STORAGE = NERSC_GAUGE
+BETA = 6.0
+    ITERS = 501
+    MEASURE = 100
+    OVER_ITERS = 4
+    SAVE = 500
+    THERM = 0
+"""
+
+
+def heatbath_8x4(tmp: Path) -> Path:
+    (tmp / "in_hb").write_text(HB_INPUT)
+    env = dict(os.environ, OMP_NUM_THREADS="8")
+    subprocess.run([str(REF_BIN), "-i", "in_hb", "-c", "hb8"], cwd=tmp,
+                   env=env, check=True, stdout=subprocess.DEVNULL)
+    return tmp / "hb8.500"
+
+
+def envelope(R: Reference, links, alpha: float, max_k: int) -> np.ndarray:
+    """In-loop theta after k = 1..max_k FACG iterations with 8 threads.
+
+    acc = 1e-30 never converges and never triggers a continuation run, so
+    FACG stops after exactly k iterations and returns that iteration's theta.
+    """
+    R.set_threads(8)
+    out = []
+    for k in range(1, max_k + 1):
+        R.put_links(links)
+        R.set_alpha(alpha)
+        out.append(R.landau_fa(1e-30, k, "FACG")["theta"])
+    R.set_threads(1)
+    return np.array(out)
+
+
+def landau_case(R: Reference, links, alpha, algo, acc=1e-14, max_iters=650):
+    R.put_links(links)
+    R.set_alpha(alpha)
+    r = R.landau_fa(acc, max_iters, algo, traj_cap=100000)
+    r["links"] = R.get_links()
+    return r
+
+
+def coulomb_case(R: Reference, links, alpha, algo, acc=1e-14, max_iters=650):
+    R.put_links(links)
+    R.set_alpha(alpha)
+    r = R.coulomb_fa(acc, max_iters, algo, traj_cap=100000)
+    r["links"] = R.get_links()
+    return r
+
+
+def pack(prefix: str, r: dict, store: dict, links=True):
+    store[f"{prefix}_iters"] = np.int64(r["iters"])
+    if "theta" in r:
+        store[f"{prefix}_theta"] = np.float64(r["theta"])
+    store[f"{prefix}_traj_theta"] = r["traj_theta"]
+    if "traj_func" in r:
+        store[f"{prefix}_traj_func"] = r["traj_func"]
+    if links:
+        store[f"{prefix}_links"] = r["links"]
+
+
+def main() -> None:
+    R = Reference()
+    RSD = Reference(sd_build=True)
+
+    # ---- 4^3 x 8 shipped configuration ---------------------------------
+    cfg = REF / "CONF" / "lat..400"
+    U = R.read_file(cfg)
+    RSD.read_file(cfg)
+    dims = np.array(R.dims, dtype=np.int64)
+    st = dict(dims=dims, links=U, plaquette=np.float64(R.plaquette()),
+              theta_test=np.float64(R.theta_test_lin()),
+              functional=np.float64(R.gauge_functional()))
+    pack("landau_facg", landau_case(R, U, 0.08, "FACG"), st)
+    st["landau_facg_env8"] = envelope(R, U, 0.08, ENVELOPE_ITERS)
+    pack("landau_fasd_ls", landau_case(R, U, 0.08, "FASD"), st)
+    pack("landau_fasd_sd", landau_case(RSD, U, 0.08, "FASD"), st)
+    pack("coulomb_facg", coulomb_case(R, U, 0.09, "FACG"), st)
+    pack("coulomb_fasd_sd", coulomb_case(RSD, U, 0.09, "FASD"), st)
+    np.savez(OUT / "lat400.npz", **st)
+    print("lat400:", {k: v for k, v in st.items() if k.endswith("iters")})
+
+    # ---- 8^4 heatbath configuration -------------------------------------
+    with tempfile.TemporaryDirectory() as td:
+        path = heatbath_8x4(Path(td))
+        U = R.read_file(path)
+        dims = np.array(R.dims, dtype=np.int64)
+        st = dict(dims=dims, links=U, plaquette=np.float64(R.plaquette()),
+                  theta_test=np.float64(R.theta_test_lin()),
+                  functional=np.float64(R.gauge_functional()))
+        r = landau_case(R, U, 0.08, "FACG")
+        pack("landau_facg", r, st, links=False)
+        # final links on every 8th site keep the fixture small
+        st["sub_stride"] = np.int64(8)
+        st["landau_facg_links_sub"] = r["links"][::8].copy()
+        st["landau_facg_env8"] = envelope(R, U, 0.08, ENVELOPE_ITERS)
+        np.savez(OUT / "hb8.npz", **st)
+        print("hb8:", st["landau_facg_iters"], "plaquette", st["plaquette"])
+
+
+if __name__ == "__main__":
+    main()
