@@ -1,0 +1,439 @@
+"""Benchmark: Landau gauge fixing of 32^3x64 SU(3) configurations to
+theta < 1e-14 (Fourier-accelerated CG), in gauge-fixed configurations per
+hour.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--precision mixed|fp64] [--dims 32,32,32,64]
+
+A step is one complete gauge fix (GLU's FACG to theta < 1e-14) of one
+configuration.  `value` is measured with the links resident in HBM (the
+device entry point gfix_landau_device); `e2e` is the same fix through the
+host entry point gfix_landau from pinned host memory, host->device and
+device->host copies inside the timed region.  Both run the mixed FP32->FP64
+path by default and report the plain FP64 path beside it.
+
+Input: the seeded synthetic stand-in of glu_b200.workload (the committed
+8^4 beta 6.0 GLU heatbath configuration repeated to 32^3x64, then a seeded
+random gauge transformation).  At N > 1 every rank fixes its own
+configuration (seed 2 + rank): weak scaling, no collective on the data path.
+
+The reference arm (--impl reference) times GLU itself, compiled from its
+sources (oracle/_ref), on the host cores: a bounded sample of FACG
+iterations on the same configuration, scaled by the iteration count of a
+full fix.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "gauge-fixed configs/hour (32^3x64 Landau FACG, theta<1e-14)"
+UNIT = "configs/hour"
+ACC = 1e-14
+ALPHA = 0.08
+MAX_ITERS = 20000
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--dims", default="32,32,32,64")
+    ap.add_argument("--profile-iters", type=int, default=20)
+    ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows: list[list[str]] = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(
+                    ["nvidia-smi", "-i", str(self.index),
+                     f"--query-gpu={self.Q}", "--format=csv,noheader,nounits"],
+                    capture_output=True, text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=6)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[4:8])
+                          if v.strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload(dims, rank):
+    from glu_b200.workload import tiled_config
+    return tiled_config(dims, seed=2 + rank)
+
+
+def _params(prec: str, cap: int = 0):
+    from glu_b200._lib import GfixParams
+    p = GfixParams()
+    p.gf_alpha = ALPHA
+    p.accuracy = ACC
+    p.max_iters = MAX_ITERS
+    p.algo = 0
+    p.sd_fixed_step = 0
+    p.precision = 1 if prec == "mixed" else 0
+    p.switch_theta = 1e-9
+    p.traj_cap = 0
+    return p
+
+
+def peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+KERNELS = ["k_deriv", "k_fft_xy_fwd", "k_fft_zt", "k_fft_xy_bwd_pr",
+           "k_dir_probe", "k_update", "k_scalar"]
+
+
+def traffic_from_profiles(name: str, prec: str, dims):
+    """dram read+write bytes per launch from the committed ncu summary"""
+    f = ROOT / "profiles" / "ncu_traffic.json"
+    if not f.exists():
+        return None
+    d = json.loads(f.read_text())
+    e = d.get(f"{name}:{prec}")
+    if not e:
+        return None
+    scale = np.prod(dims) / float(np.prod(e["dims"]))
+    return float(e["dram_bytes_per_launch"]) * scale
+
+
+def gpu_arm(args, dims, rank, world, local):
+    import ctypes as C
+    import torch
+    torch.cuda.set_device(local)
+    from glu_b200 import _lib
+    from glu_b200._lib import GfixResult, check
+    lib = _lib.load()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    U = workload(dims, rank)
+    flat = U.view(np.float64).reshape(-1)
+    host = torch.from_numpy(flat).pin_memory()
+    hwork = torch.empty_like(host).pin_memory()
+    dpristine = host.to("cuda")
+    dwork = torch.empty_like(dpristine)
+    cd = (C.c_size_t * 4)(*dims)
+    V = int(np.prod(dims))
+
+    def dev_fix(prec):
+        dwork.copy_(dpristine)
+        torch.cuda.synchronize()
+        r = GfixResult()
+        p = _params(prec)
+        check(lib.gfix_landau_device(dwork.data_ptr(), cd, C.byref(p), C.byref(r)))
+        return r
+
+    def host_fix(prec):
+        r = GfixResult()
+        p = _params(prec)
+        check(lib.gfix_landau(hwork.data_ptr(), cd, C.byref(p), C.byref(r)))
+        return r
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    out = {}
+    with Clocks(local) as clk:
+        for prec in ([args.precision, "fp64"] if args.precision == "mixed"
+                     else ["fp64"]):
+            for _ in range(args.warmup):
+                r = dev_fix(prec)
+            # resident inputs: K steps bracketed by barrier + sync
+            launches0 = lib.gfix_kernel_launches()
+            barrier()
+            a, b = ev(), ev()
+            a.record()
+            iters = []
+            for _ in range(args.steps):
+                r = dev_fix(prec)
+                iters.append(r.iters)
+            b.record()
+            barrier()
+            launches = lib.gfix_kernel_launches() - launches0
+            ms = max_over_ranks(a.elapsed_time(b))
+            # end to end: pinned host buffers, H2D + D2H inside each step
+            e_ms = 0.0
+            for _ in range(args.steps):
+                hwork.copy_(host)
+                barrier()
+                a2, b2 = ev(), ev()
+                a2.record()
+                r2 = host_fix(prec)
+                b2.record()
+                torch.cuda.synchronize()
+                e_ms += a2.elapsed_time(b2)
+            e_ms = max_over_ranks(e_ms)
+            out[prec] = dict(ms=ms, e2e_ms=e_ms, iters=iters, iters_fp32=r.iters_fp32,
+                             theta=r.theta, launches=launches, e2e_iters=r2.iters)
+    clocks = clk.summary()
+    res = dict(out=out, clocks=clocks, V=V)
+    # per-kernel device times for the roofline (events on the launch stream)
+    prof = {}
+    for prec in ("fp64", "mixed"):
+        ms = np.zeros(7)
+        by = np.zeros(7)
+        check(lib.gfix_profile_landau(
+            dpristine.data_ptr(), cd, C.byref(_params(prec)), args.profile_iters,
+            ms.ctypes.data_as(C.POINTER(C.c_double)),
+            by.ctypes.data_as(C.POINTER(C.c_double))))
+        prof["fp32" if prec == "mixed" else "fp64"] = (ms, by)
+    res["prof"] = prof
+    if dist is not None:
+        dist.destroy_process_group()
+    return res, U
+
+
+def reference_iters(dims):
+    """Iteration count of the reference's own full fix of this workload
+    (a property of algorithm and input), from the committed measurement."""
+    f = ROOT / "profiles" / "reference_full_fix.json"
+    if f.exists():
+        for e in json.loads(f.read_text()):
+            if tuple(e["dims"]) == tuple(dims):
+                return int(e["iters"]), e
+    return None, None
+
+
+def cpu_sample(U, dims, sample_s: float, nthreads: int):
+    """Seconds per FACG iteration of the reference (oracle/_ref) with
+    nthreads OpenMP threads, from two runs of k1 < k2 iterations (acc 1e-30:
+    exactly k iterations, no continuation), and the fixed cost of a call."""
+    from oracle.oracle import REF_SO, Oracle, Reference
+    if REF_SO.exists():
+        R = Reference()
+        R.setup(dims, nthreads, ALPHA)
+        kind = "reference"
+
+        def run(k):
+            R.put_links(U)
+            R.lib.ref_reset_fft_seconds()
+            t = time.perf_counter()
+            R.landau_fa(1e-30, k, "FACG")
+            return time.perf_counter() - t, R.fft_seconds()
+    else:  # the oracle port, single threaded
+        O = Oracle()
+        kind, nthreads = "port", 1
+
+        def run(k):
+            t = time.perf_counter()
+            O.landau(U, dims, ALPHA, 1e-30, k, "FACG")
+            return time.perf_counter() - t, 0.0
+    t1, f1 = run(1)
+    k2 = max(2, int(sample_s / max(t1, 1e-3)))
+    t2, f2 = run(k2)
+    s_iter = (t2 - t1) / (k2 - 1)
+    fixed = max(t1 - s_iter, 0.0)
+    return dict(kind=kind, cores=nthreads, s_iter=s_iter, fixed_s=fixed,
+                fft_thread_s_iter=(f2 - f1) / (k2 - 1), sample_iters=k2,
+                sample_s=t1 + t2)
+
+
+def emit(d):
+    print(json.dumps(d), flush=True)
+
+
+def reference_arm(args, dims, rank, world):
+    if rank != 0:
+        return
+    U = workload(dims, 0)
+    n_ref, meta = reference_iters(dims)
+    cores = os.cpu_count() or 1
+    for _ in range(max(args.warmup, 0) and 1):
+        cpu_sample(U, dims, min(args.cpu_sample_s, 5.0), cores)
+    samples = [cpu_sample(U, dims, args.cpu_sample_s, cores)
+               for _ in range(max(args.steps, 1))]
+    s_iter = statistics.median(s["s_iter"] for s in samples)
+    fixed = statistics.median(s["fixed_s"] for s in samples)
+    if n_ref is None:
+        emit({"impl": "reference", "unavailable":
+              "no recorded full-fix iteration count for dims %s" % (dims,)})
+        return
+    t_fix = fixed + s_iter * n_ref
+    value = 3600.0 / t_fix
+    s0 = samples[0]
+    emit({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+          "steps": args.steps, "warmup": args.warmup,
+          "ms_per_step": t_fix * 1e3, "higher_is_better": True,
+          "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+          "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled + random gauge)",
+          "config": {"workload": "Landau FACG theta<1e-14, %s" % "x".join(map(str, dims)),
+                     "dims": list(dims), "gf_alpha": ALPHA, "accuracy": ACC,
+                     "full_fix_iters": n_ref, "parallelism": "host OpenMP"},
+          "impl": "reference",
+          "cpu_baseline": {"value": value, "unit": UNIT, "cores": s0["cores"],
+                           "kind": s0["kind"],
+                           "sample": "%d x %d FACG iterations per step, "
+                                     "%.3f s/iteration x %d iterations" %
+                                     (len(samples), s0["sample_iters"], s_iter, n_ref)},
+          "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                  "d2h_bytes_per_step": 0}})
+
+
+def gpu_line(args, dims, world, res, cpu):
+    prec = args.precision
+    o = res["out"][prec]
+    steps = args.steps
+    ms_step = o["ms"] / steps
+    value = world * steps * 3600e3 / o["ms"]
+    e2e = world * steps * 3600e3 / o["e2e_ms"]
+    V = res["V"]
+    # dominant kernel over a whole fix: per-launch time x launches
+    peak, peak_src = peaks()
+    it32 = o["iters_fp32"] if prec == "mixed" else 0
+    it64 = o["iters"][-1] - it32
+    share = []
+    for tag, n in (("fp32", it32), ("fp64", it64)):
+        ms, by = res["prof"][tag]
+        for k in range(6):
+            share.append((ms[k] * n, tag, k, ms[k], by[k]))
+    tot = sum(s[0] for s in share)
+    top = max(share)
+    _, tag, k, k_ms, k_by = top
+    achieved = k_by / (k_ms * 1e-3) / 1e9
+    traffic = traffic_from_profiles(KERNELS[k], tag, dims)
+    per_kernel = {f"{KERNELS[j]}:{t}": {"ms": round(m, 5), "GB/s": round(b / (m * 1e-3) / 1e9, 1)}
+                  for t in ("fp32", "fp64") if (t != "fp32" or prec == "mixed")
+                  for j, (m, b) in enumerate(zip(*res["prof"][t])) if j < 6}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if prec == "mixed" else "f64",
+        "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled + seeded random gauge transform)",
+        "config": {"workload": "Landau FACG theta<1e-14, %s" % "x".join(map(str, dims)),
+                   "dims": list(dims), "gf_alpha": ALPHA, "accuracy": ACC,
+                   "precision": prec, "switch_theta": 1e-9 if prec == "mixed" else None,
+                   "iters": o["iters"][-1], "iters_fp32": it32,
+                   "final_theta": o["theta"],
+                   "fp64_only": {"value": world * steps * 3600e3 / res["out"]["fp64"]["ms"],
+                                 "ms_per_step": res["out"]["fp64"]["ms"] / steps,
+                                 "iters": res["out"]["fp64"]["iters"][-1],
+                                 "e2e": world * steps * 3600e3 / res["out"]["fp64"]["e2e_ms"]},
+                   "l2": "inputs (%.2f GB of links) larger than the 126 MB L2" % (V * 576 / 1e9),
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": V * 576,
+                "d2h_bytes_per_step": V * 576},
+        "roofline": {"bound": "hbm", "kernel": f"{KERNELS[k]} ({tag})",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src,
+                     "traffic": traffic, "algorithmic_bytes": k_by,
+                     "share_of_fix": top[0] / tot if tot else None,
+                     "per_kernel": per_kernel},
+        "gpu_launches": o["launches"],
+        "clocks": res["clocks"],
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    return line
+
+
+def main():
+    args = parse()
+    dims = tuple(int(x) for x in args.dims.split(","))
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        reference_arm(args, dims, rank, world)
+        return
+    res, U = gpu_arm(args, dims, rank, world, local)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            n_ref, _ = reference_iters(dims)
+            s = cpu_sample(U, dims, args.cpu_sample_s, os.cpu_count() or 1)
+            n_full = n_ref or res["out"]["fp64"]["iters"][-1]
+            t_fix = s["fixed_s"] + s["s_iter"] * n_full
+            cpu = {"value": 3600.0 / t_fix, "unit": UNIT, "cores": s["cores"],
+                   "kind": s["kind"],
+                   "sample": "%d FACG iterations (%.1f s); %.3f s/iteration x %d "
+                             "iterations of a full fix; FFT stand-in %.3f thread-s/iteration"
+                             % (s["sample_iters"], s["sample_s"], s["s_iter"], n_full,
+                                s["fft_thread_s_iter"])}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "kind": "unavailable", "sample": str(e)}
+    if rank == 0:
+        emit(gpu_line(args, dims, world, res, cpu))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,83 @@
+"""ctypes binding of libglu_gfix.so (the C ABI in include/glu_gfix.h).
+
+There is no CPU fallback: if the library is missing or cannot be loaded,
+every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+from .build import LIB
+
+_dp = C.POINTER(C.c_double)
+_szp = C.POINTER(C.c_size_t)
+
+
+class GfixParams(C.Structure):
+    _fields_ = [("gf_alpha", C.c_double), ("accuracy", C.c_double),
+                ("max_iters", C.c_size_t), ("algo", C.c_int),
+                ("sd_fixed_step", C.c_int), ("precision", C.c_int),
+                ("switch_theta", C.c_double), ("traj_theta", _dp),
+                ("traj_func", _dp), ("traj_cap", C.c_size_t)]
+
+
+class GfixResult(C.Structure):
+    _fields_ = [("iters", C.c_size_t), ("iters_fp32", C.c_size_t),
+                ("theta", C.c_double), ("traj_len", C.c_size_t),
+                ("gpu_ms", C.c_double), ("restarts", C.c_int)]
+
+
+# every symbol include/glu_gfix.h declares
+EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
+           "Coulomb_FA", "FOURIER_ACCELERATE2", "gfix_landau",
+           "gfix_landau_device", "gfix_coulomb", "gfix_coulomb_device",
+           "gfix_observables", "gfix_reunit", "gfix_fourier_accelerate",
+           "gfix_profile_landau",
+           "gfix_last_error", "gfix_release", "gfix_kernel_launches")
+
+_lib = None
+
+
+class GfixError(RuntimeError):
+    pass
+
+
+def load(path: Path | str | None = None):
+    """Load the library once; raises GfixError when it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB
+    if not p.exists():
+        raise GfixError(f"{p} is not built: run `python -m glu_b200.build`")
+    lib = C.CDLL(str(p))
+    for fn in ("gfix_landau", "gfix_landau_device"):
+        getattr(lib, fn).restype = C.c_int
+        getattr(lib, fn).argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
+                                     C.POINTER(GfixResult)]
+    for fn in ("gfix_coulomb", "gfix_coulomb_device"):
+        getattr(lib, fn).restype = C.c_int
+        getattr(lib, fn).argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
+                                     C.POINTER(GfixResult), _dp, _szp]
+    lib.gfix_observables.restype = C.c_int
+    lib.gfix_observables.argtypes = [C.c_void_p, _szp, _dp]
+    lib.gfix_reunit.restype = C.c_int
+    lib.gfix_reunit.argtypes = [C.c_void_p, _szp]
+    lib.gfix_fourier_accelerate.restype = C.c_int
+    lib.gfix_fourier_accelerate.argtypes = [C.c_void_p, _szp, C.c_int]
+    lib.gfix_profile_landau.restype = C.c_int
+    lib.gfix_profile_landau.argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
+                                        C.c_int, _dp, _dp]
+    lib.gfix_last_error.restype = C.c_char_p
+    lib.gfix_last_error.argtypes = []
+    lib.gfix_release.restype = None
+    lib.gfix_kernel_launches.restype = C.c_ulonglong
+    _lib = lib
+    return lib
+
+
+def check(rc: int):
+    if rc != 0:
+        msg = _lib.gfix_last_error().decode() if _lib else "library not loaded"
+        raise GfixError(msg)

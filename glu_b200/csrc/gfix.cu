@@ -1,0 +1,795 @@
+// Host engine and C ABI of the B200 Fourier-accelerated gauge fixing.
+//
+// An Engine<R> owns the device workspace of one lattice shape in working
+// precision R: SoA links, the in/in_old and sn ping-pong fields, partial
+// sums, twiddle and cos tables, a device-side control block (DevState) and
+// the CUDA graphs of one solver iteration.  The solver loops replay a graph
+// and only read the control block back every few iterations; all of GLU's
+// scalar control flow (theta, beta, alpha*, stop tests) runs on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/glu_gfix.h"
+#include "extra_kernels.cuh"
+#include "kernels.cuh"
+
+namespace gfix {
+
+static thread_local std::string g_err = "";
+static std::atomic<unsigned long long> g_launches{0};
+
+static int fail(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return -1;
+}
+
+#define CK(call)                                                        \
+  do {                                                                  \
+    cudaError_t e_ = (call);                                            \
+    if (e_ != cudaSuccess)                                              \
+      return fail("%s:%d %s: %s", __FILE__, __LINE__, #call,           \
+                  cudaGetErrorString(e_));                              \
+  } while (0)
+
+#define LAUNCHED(n) g_launches.fetch_add((n), std::memory_order_relaxed)
+
+constexpr size_t kSentinel = 123456789;
+
+// radices 8,4,2,3,5 then any prime <= kMaxRadix
+static int factorize(int n, FftAxis &ax) {
+  ax.n = n;
+  ax.nstages = 0;
+  int m = n;
+  const int pref[5] = {8, 4, 2, 3, 5};
+  for (int r : pref)
+    while (m % r == 0 && m > 1) {
+      if (ax.nstages == kMaxStages) return -1;
+      ax.radix[ax.nstages++] = r;
+      m /= r;
+    }
+  for (int p = 7; m > 1; p += 2)
+    while (m % p == 0) {
+      if (p > kMaxRadix || ax.nstages == kMaxStages) return -1;
+      ax.radix[ax.nstages++] = p;
+      m /= p;
+    }
+  if (ax.nstages == 0) ax.radix[ax.nstages++] = 1;
+  return 0;
+}
+
+struct Params {
+  double gf_alpha = 0.08, acc = 1e-14;
+  size_t max_iters = 1000;
+  int algo = GFIX_CG, sd_fixed = 0;
+  double *traj_theta = nullptr, *traj_func = nullptr;
+  size_t traj_cap = 0;
+};
+
+template <typename R>
+class Engine {
+ public:
+  size_t dims[4] = {0, 0, 0, 0};
+  int V = 0;
+  Ctx<R> c{};
+  cudaStream_t s = nullptr;
+  DevState *d_st = nullptr, *h_st = nullptr;
+  double *d_part = nullptr, *d_cs = nullptr, *d_traj = nullptr;
+  cx<R> *d_tw = nullptr, *d_U = nullptr, *d_F = nullptr, *d_G = nullptr;
+  double *d_aos = nullptr;  // AoS FP64 staging (only FP64 engines)
+  size_t traj_alloc = 0;
+  int nb_site = 0;
+  dim3 g_xy, g_zt;
+  size_t sm_xy = 0, sm_zt = 0;
+  cudaGraphExec_t gx_cg = nullptr, gx_sd = nullptr;
+  int gx_sd_fixed = -1;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  ~Engine() { release(); }
+
+  void release() {
+    if (gx_cg) cudaGraphExecDestroy(gx_cg);
+    if (gx_sd) cudaGraphExecDestroy(gx_sd);
+    gx_cg = gx_sd = nullptr;
+    cudaFree(d_st);
+    cudaFreeHost(h_st);
+    cudaFree(d_part);
+    cudaFree(d_cs);
+    cudaFree(d_traj);
+    cudaFree(d_tw);
+    cudaFree(d_U);
+    cudaFree(d_F);
+    cudaFree(d_G);
+    cudaFree(d_aos);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (s) cudaStreamDestroy(s);
+    d_st = nullptr;
+    h_st = nullptr;
+    s = nullptr;
+  }
+
+  int init(const size_t *d, bool with_G, bool with_staging) {
+    for (int i = 0; i < 4; i++) dims[i] = d[i];
+    const size_t Vs = d[0] * d[1] * d[2] * d[3];
+    if (Vs == 0 || Vs > (size_t)INT32_MAX / 4)
+      return fail("lattice volume %zu outside 1..2^29", Vs);
+    V = (int)Vs;
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&ev0));
+    CK(cudaEventCreate(&ev1));
+    for (int i = 0; i < 4; i++) {
+      c.L[i] = (int)d[i];
+      if (factorize(c.L[i], c.ax[i]) != 0)
+        return fail("extent %d has a prime factor above %d", c.L[i], kMaxRadix);
+    }
+    c.V = V;
+    c.ndim = 4;
+    c.maxp = 4.0 * 4 / (double)V;  // MAX_LANDAU
+    // twiddle pool: one table per axis
+    std::vector<cx<R>> tw;
+    for (int a = 0; a < 4; a++) {
+      c.ax[a].tw_off = (int)tw.size();
+      const int n = c.L[a];
+      for (int k = 0; k < n; k++) {
+        const double ang = 6.283185307179586476925286766559 * k / n;
+        tw.push_back(mk<R>((R)std::cos(ang), (R)(-std::sin(ang))));
+      }
+    }
+    CK(cudaMalloc(&d_tw, tw.size() * sizeof(cx<R>)));
+    CK(cudaMemcpy(d_tw, tw.data(), tw.size() * sizeof(cx<R>),
+                  cudaMemcpyHostToDevice));
+    c.tw = d_tw;
+    // cos tables as GLU evaluates them: cos(n * (TWOPI / L)) (init.c:66,
+    // geometry.c:176)
+    const int ld = *std::max_element(c.L, c.L + 4);
+    std::vector<double> cs(4 * (size_t)ld, 0.0);
+    for (int a = 0; a < 4; a++) {
+      const double twd = 6.283185307179586 / (double)c.L[a];
+      for (int n = 0; n < c.L[a]; n++) cs[a * ld + n] = std::cos(n * twd);
+    }
+    CK(cudaMalloc(&d_cs, cs.size() * sizeof(double)));
+    CK(cudaMemcpy(d_cs, cs.data(), cs.size() * sizeof(double),
+                  cudaMemcpyHostToDevice));
+    c.cs = d_cs;
+    c.cs_ld = ld;
+    // tiles
+    c.xy_pitch = c.L[0] + 1;
+    const int want_b = (sizeof(R) == 8) ? 2 : 4;
+    c.zt_b = 1;
+    for (int b = want_b; b >= 1; b--)
+      if (c.L[0] % b == 0) {
+        c.zt_b = b;
+        break;
+      }
+    sm_xy = 2 * (size_t)c.xy_pitch * c.L[1] * sizeof(cx<R>);
+    sm_zt = 2 * (size_t)c.zt_b * c.L[2] * c.L[3] * sizeof(cx<R>);
+    while (sm_zt > 200 * 1024 && c.zt_b > 1) {
+      c.zt_b = 1;
+      sm_zt = 2 * (size_t)c.L[2] * c.L[3] * sizeof(cx<R>);
+    }
+    if (sm_xy > 200 * 1024 || sm_zt > 200 * 1024)
+      return fail("FFT tile does not fit shared memory (xy %zu B, zt %zu B)",
+                  sm_xy, sm_zt);
+    CK(cudaFuncSetAttribute(k_fft_xy<R>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sm_xy));
+    CK(cudaFuncSetAttribute(k_fft_zt<R>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)sm_zt));
+    g_xy = dim3(V / (c.L[0] * c.L[1]), 4);
+    g_zt = dim3((c.L[0] / c.zt_b) * c.L[1], 4);
+    nb_site = (V + kSiteThreads - 1) / kSiteThreads;
+    const size_t nparts =
+        std::max<size_t>((size_t)nb_site, (size_t)g_xy.x * g_xy.y) + 1024;
+    CK(cudaMalloc(&d_part, nparts * 2 * sizeof(double)));
+    c.part = d_part;
+    CK(cudaMalloc(&d_st, sizeof(DevState)));
+    CK(cudaMallocHost(&h_st, sizeof(DevState)));
+    memset(h_st, 0, sizeof(DevState));
+    c.st = d_st;
+    CK(cudaMalloc(&d_U, (size_t)V * 36 * sizeof(cx<R>)));
+    CK(cudaMalloc(&d_F, (size_t)V * 16 * sizeof(cx<R>)));
+    c.U = d_U;
+    c.fb[0] = d_F;
+    c.fb[1] = d_F + (size_t)4 * V;
+    c.sb[0] = d_F + (size_t)8 * V;
+    c.sb[1] = d_F + (size_t)12 * V;
+    if (with_G) CK(cudaMalloc(&d_G, (size_t)V * 9 * sizeof(cx<R>)));
+    c.G = d_G;
+    if (with_staging) CK(cudaMalloc(&d_aos, (size_t)V * 36 * sizeof(double2)));
+    return 0;
+  }
+
+  int ensure_traj(size_t cap) {
+    if (cap <= traj_alloc) return 0;
+    cudaFree(d_traj);
+    d_traj = nullptr;
+    traj_alloc = 0;
+    CK(cudaMalloc(&d_traj, 2 * cap * sizeof(double)));
+    traj_alloc = cap;
+    return 0;
+  }
+
+  // --- launch sequences ------------------------------------------------
+  void scalar(int op, int nv) {
+    k_scalar<<<1, kScalarThreads, 0, s>>>(d_st, d_part, op, nv, (double)V);
+    LAUNCHED(1);
+  }
+  void theta(int op) {
+    k_deriv<R><<<nb_site, kSiteThreads, 0, s>>>(c);
+    LAUNCHED(1);
+    scalar(op, 2);
+  }
+  void fft(bool prsum) {
+    k_fft_xy<R><<<g_xy, 256, sm_xy, s>>>(c, 0, 0);
+    k_fft_zt<R><<<g_zt, 256, sm_zt, s>>>(c);
+    k_fft_xy<R><<<g_xy, 256, sm_xy, s>>>(c, 1, prsum ? 1 : 0);
+    LAUNCHED(3);
+  }
+  // an SD step (steep_Landau_FA, src/Gfix/FACG.c:181-199); main = one FASD
+  // iteration with its stop test
+  void sd_step(bool main, bool sd_fixed) {
+    theta(main ? OP_THETA_MAIN : OP_THETA_SD);
+    fft(false);
+    if (sd_fixed) {
+      scalar(OP_ALPHA_FIXED, 0);
+    } else {
+      k_dir_probe<R, false><<<nb_site, kSiteThreads, 0, s>>>(c);
+      LAUNCHED(1);
+      scalar(OP_PROBES, 2);
+    }
+    k_update<R, false><<<nb_site, kSiteThreads, 0, s>>>(c);
+    LAUNCHED(1);
+    if (main) scalar(OP_END_SD, 0);
+  }
+  // one CG iteration (src/Gfix/FACG.c:270-334)
+  void cg_iter() {
+    theta(OP_THETA_MAIN);
+    fft(true);
+    scalar(OP_PR, 2);
+    k_dir_probe<R, true><<<nb_site, kSiteThreads, 0, s>>>(c);
+    LAUNCHED(1);
+    scalar(OP_PROBES, 2);
+    k_update<R, true><<<nb_site, kSiteThreads, 0, s>>>(c);
+    LAUNCHED(1);
+    scalar(OP_END_CG, 0);
+  }
+
+  int capture(cudaGraphExec_t *out, bool cg, bool sd_fixed) {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const unsigned long long before = g_launches.load();
+    if (cg)
+      cg_iter();
+    else
+      sd_step(true, sd_fixed);
+    // captured launches run later; they are counted at replay
+    g_launches.store(before);
+    CK(cudaStreamEndCapture(s, &g));
+    CK(cudaGraphInstantiate(out, g, 0));
+    cudaGraphDestroy(g);
+    return 0;
+  }
+
+  unsigned long long per_iter_launches(bool cg, bool sd_fixed) const {
+    // k_deriv + scalar + 3 fft + ...
+    if (cg) return 2 + 3 + 1 + 2 + 1 + 1;
+    return 2 + 3 + (sd_fixed ? 1 : 2) + 1 + 1;
+  }
+
+  int read_state() {
+    CK(cudaMemcpyAsync(h_st, d_st, sizeof(DevState), cudaMemcpyDeviceToHost,
+                       s));
+    CK(cudaStreamSynchronize(s));
+    return 0;
+  }
+
+  // replay an iteration graph until the device says done
+  int replay(cudaGraphExec_t gx, unsigned long long per_iter) {
+    int batch = 2;
+    size_t guard = 0;
+    for (;;) {
+      for (int k = 0; k < batch; k++) {
+        CK(cudaGraphLaunch(gx, s));
+        LAUNCHED(per_iter);
+      }
+      if (read_state()) return -1;
+      if (h_st->done) return 0;
+      guard += batch;
+      if (guard > (size_t)h_st->max_iters + 64)
+        return fail("solver did not stop after %zu iterations", guard);
+      batch = std::min(batch * 2, 32);
+    }
+  }
+
+  // state for a new solve
+  int reset(const Params &p) {
+    if (p.traj_cap && ensure_traj(p.traj_cap)) return -1;
+    DevState st;
+    memset(&st, 0, sizeof st);
+    st.gf_alpha = p.gf_alpha;
+    st.acc = p.acc;
+    st.max_iters = (long long)p.max_iters;
+    st.sd_fixed = p.sd_fixed;
+    st.traj_cap = p.traj_cap ? (long long)p.traj_cap : 0;
+    st.traj_theta = p.traj_cap ? d_traj : nullptr;
+    st.traj_func = p.traj_cap ? d_traj + p.traj_cap : nullptr;
+    CK(cudaMemcpyAsync(d_st, &st, sizeof st, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    return 0;
+  }
+
+  int fetch_traj(const Params &p, size_t *len) {
+    *len = 0;
+    if (!p.traj_cap) return 0;
+    if (read_state()) return -1;
+    const size_t n = std::min<size_t>((size_t)h_st->traj_len, p.traj_cap);
+    if (n) {
+      if (p.traj_theta)
+        CK(cudaMemcpy(p.traj_theta, d_traj, n * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+      if (p.traj_func)
+        CK(cudaMemcpy(p.traj_func, d_traj + p.traj_cap, n * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+    }
+    *len = n;
+    return 0;
+  }
+
+  // theta_test_lin of the current links
+  int theta_test(double *out) {
+    k_begin_run<<<1, 1, 0, s>>>(d_st);
+    LAUNCHED(1);
+    theta(OP_THETA_TEST);
+    if (read_state()) return -1;
+    *out = h_st->tr_test;
+    return 0;
+  }
+
+  // GLU's FACG (src/Gfix/FACG.c:341-391) on the resident links
+  int solve_facg(const Params &p, size_t *iters, double *th) {
+    if (reset(p)) return -1;
+    if (theta_test(th)) return -1;
+    if (*th < p.acc) {
+      *iters = 0;
+      return 0;
+    }
+    if (!gx_cg && capture(&gx_cg, true, false)) return -1;
+    for (;;) {
+      k_begin_run<<<1, 1, 0, s>>>(d_st);
+      LAUNCHED(1);
+      sd_step(false, p.sd_fixed != 0);
+      k_copy_der<R><<<nb_site, kSiteThreads, 0, s>>>(c);
+      LAUNCHED(1);
+      scalar(OP_DER, 1);
+      if (replay(gx_cg, per_iter_launches(true, false))) return -1;
+      *th = h_st->tr;
+      const size_t loc = (size_t)h_st->iter;
+      if (loc >= p.max_iters) {
+        if (*th < 1E3 * p.acc) continue;  // continuation run
+        *iters = kSentinel;
+        return 0;
+      }
+      *iters = loc;
+      return 0;
+    }
+  }
+
+  // GLU's FASD (src/Gfix/FACG.c:395-446)
+  int solve_fasd(const Params &p, size_t *iters, double *th) {
+    if (reset(p)) return -1;
+    if (theta_test(th)) return -1;
+    if (*th < p.acc) {
+      *iters = 0;
+      return 0;
+    }
+    if (!gx_sd || gx_sd_fixed != p.sd_fixed) {
+      if (gx_sd) cudaGraphExecDestroy(gx_sd);
+      gx_sd = nullptr;
+      if (capture(&gx_sd, false, p.sd_fixed != 0)) return -1;
+      gx_sd_fixed = p.sd_fixed;
+    }
+    size_t total = 0;
+    for (;;) {
+      k_begin_run<<<1, 1, 0, s>>>(d_st);
+      LAUNCHED(1);
+      if (replay(gx_sd, per_iter_launches(false, p.sd_fixed != 0))) return -1;
+      *th = h_st->tr;
+      size_t loc = (size_t)h_st->iter;
+      if (loc >= p.max_iters) {
+        if (*th < 1E3 * p.acc) continue;  // loc_iters = 0, iters += 0
+        total = kSentinel;
+      }
+      total += loc;
+      *iters = total;
+      return 0;
+    }
+  }
+
+  int solve(const Params &p, size_t *iters, double *th) {
+    return p.algo == GFIX_CG ? solve_facg(p, iters, th)
+                             : solve_fasd(p, iters, th);
+  }
+
+  // Per-kernel device times of `n` CG iterations launched one by one with
+  // events between the launches (no graph).  ms[k] = average duration of
+  // one launch of kernel k, bytes[k] = its algorithmic HBM bytes:
+  //   0 k_deriv, 1 k_fft_xy fwd, 2 k_fft_zt, 3 k_fft_xy bwd (+PR sums),
+  //   4 k_dir_probe, 5 k_update, 6 the four k_scalar launches together
+  int profile_cg(const Params &p, int n, double *ms, double *bytes) {
+    if (reset(p)) return -1;
+    k_begin_run<<<1, 1, 0, s>>>(d_st);
+    sd_step(false, p.sd_fixed != 0);
+    k_copy_der<R><<<nb_site, kSiteThreads, 0, s>>>(c);
+    scalar(OP_DER, 1);
+    LAUNCHED(2);
+    std::vector<cudaEvent_t> ev(8);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int it = 0; it < n; it++) {
+      CK(cudaEventRecord(ev[0], s));
+      k_deriv<R><<<nb_site, kSiteThreads, 0, s>>>(c);
+      CK(cudaEventRecord(ev[1], s));
+      scalar(OP_THETA_MAIN, 2);
+      CK(cudaEventRecord(ev[2], s));
+      k_fft_xy<R><<<g_xy, 256, sm_xy, s>>>(c, 0, 0);
+      CK(cudaEventRecord(ev[3], s));
+      k_fft_zt<R><<<g_zt, 256, sm_zt, s>>>(c);
+      CK(cudaEventRecord(ev[4], s));
+      k_fft_xy<R><<<g_xy, 256, sm_xy, s>>>(c, 1, 1);
+      CK(cudaEventRecord(ev[5], s));
+      scalar(OP_PR, 2);
+      CK(cudaEventRecord(ev[6], s));
+      k_dir_probe<R, true><<<nb_site, kSiteThreads, 0, s>>>(c);
+      CK(cudaEventRecord(ev[7], s));
+      CK(cudaStreamSynchronize(s));
+      float t[7];
+      for (int k = 0; k < 7; k++) CK(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
+      acc[0] += t[0];
+      acc[6] += t[1] + t[5];
+      acc[1] += t[2];
+      acc[2] += t[3];
+      acc[3] += t[4];
+      acc[4] += t[6];
+      CK(cudaEventRecord(ev[0], s));
+      scalar(OP_PROBES, 2);
+      CK(cudaEventRecord(ev[1], s));
+      k_update<R, true><<<nb_site, kSiteThreads, 0, s>>>(c);
+      CK(cudaEventRecord(ev[2], s));
+      scalar(OP_END_CG, 0);
+      CK(cudaEventRecord(ev[3], s));
+      CK(cudaStreamSynchronize(s));
+      for (int k = 0; k < 3; k++) CK(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
+      acc[6] += t[0] + t[2];
+      acc[5] += t[1];
+      LAUNCHED(10);
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    const double B = sizeof(cx<R>) * (double)V;  // one complex per site
+    const double b[7] = {(36 + 4) * B, 8 * B, 8 * B, 12 * B,
+                         (36 + 4 + 4 + 4) * B, (36 + 4 + 36) * B, 0.0};
+    for (int k = 0; k < 7; k++) {
+      ms[k] = acc[k] / n;
+      if (bytes) bytes[k] = b[k];
+    }
+    return 0;
+  }
+
+  // links: device AoS FP64 -> SoA R (and back)
+  int from_aos(const double *aos) {
+    k_aos_to_soa<R><<<1184, 256, 0, s>>>(aos, d_U, V);
+    LAUNCHED(1);
+    CK(cudaGetLastError());
+    return 0;
+  }
+  int to_aos(double *aos) {
+    k_soa_to_aos<R><<<1184, 256, 0, s>>>(d_U, aos, V);
+    LAUNCHED(1);
+    CK(cudaGetLastError());
+    return 0;
+  }
+};
+
+// ---------------------------------------------------------------------
+// workspace cache: one engine per (device, shape, precision)
+
+struct Key {
+  int dev;
+  size_t d[4];
+  int prec;
+  bool operator<(const Key &o) const {
+    return std::tie(dev, d[0], d[1], d[2], d[3], prec) <
+           std::tie(o.dev, o.d[0], o.d[1], o.d[2], o.d[3], o.prec);
+  }
+};
+
+static std::map<Key, std::unique_ptr<Engine<double>>> g_e64;
+static std::map<Key, std::unique_ptr<Engine<float>>> g_e32;
+
+static Engine<double> *engine64(const size_t *d) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    fail("no CUDA device");
+    return nullptr;
+  }
+  Key k{dev, {d[0], d[1], d[2], d[3]}, 64};
+  auto it = g_e64.find(k);
+  if (it != g_e64.end()) return it->second.get();
+  auto e = std::make_unique<Engine<double>>();
+  if (e->init(d, false, true)) return nullptr;
+  Engine<double> *p = e.get();
+  g_e64[k] = std::move(e);
+  return p;
+}
+
+static Engine<float> *engine32(const size_t *d) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    fail("no CUDA device");
+    return nullptr;
+  }
+  Key k{dev, {d[0], d[1], d[2], d[3]}, 32};
+  auto it = g_e32.find(k);
+  if (it != g_e32.end()) return it->second.get();
+  auto e = std::make_unique<Engine<float>>();
+  if (e->init(d, true, false)) return nullptr;
+  Engine<float> *p = e.get();
+  g_e32[k] = std::move(e);
+  return p;
+}
+
+static Params to_params(const gfix_params *p) {
+  Params q;
+  q.gf_alpha = p->gf_alpha;
+  q.acc = p->accuracy;
+  q.max_iters = p->max_iters;
+  q.algo = p->algo;
+  q.sd_fixed = p->sd_fixed_step;
+  q.traj_theta = p->traj_theta;
+  q.traj_func = p->traj_func;
+  q.traj_cap = p->traj_cap;
+  return q;
+}
+
+// Landau solve of the links staged (AoS FP64) in e64->d_aos
+static int landau_staged(Engine<double> *e64, const gfix_params *gp,
+                         gfix_result *r) {
+  Params p = to_params(gp);
+  gfix_result res;
+  memset(&res, 0, sizeof res);
+  if (e64->from_aos(e64->d_aos)) return -1;
+  CK(cudaEventRecord(e64->ev0, e64->s));
+  size_t iters = 0;
+  double th = 0.0;
+  size_t tl = 0;
+  if (gp->precision == GFIX_MIXED) {
+    // FP32 phase on a converted copy, tracking the gauge transform G
+    Engine<float> *e32 = engine32(e64->dims);
+    if (!e32) return -1;
+    // e32 runs on e64's stream order: synchronise the two streams
+    CK(cudaStreamSynchronize(e64->s));
+    const size_t n = (size_t)e64->V * 36;
+    k_convert<double, float><<<1184, 256, 0, e32->s>>>(e64->d_U, e32->d_U, n);
+    k_identity<float><<<(e64->V + 255) / 256, 256, 0, e32->s>>>(e32->d_G,
+                                                                e64->V);
+    LAUNCHED(2);
+    Params p32 = p;
+    p32.acc = std::max(gp->switch_theta, gp->accuracy);
+    size_t it32 = 0;
+    double th32 = 0.0;
+    if (e32->solve(p32, &it32, &th32)) return -1;
+    size_t tl32 = 0;
+    if (e32->fetch_traj(p32, &tl32)) return -1;
+    if (it32 == kSentinel || it32 > 0) {
+      // hand over: U64 <- G U64 G^dag with G reunitarised in FP64
+      cx<double> *G64 = e64->c.fb[0];  // 9 V complex fit in the field pool
+      k_convert<float, double><<<1184, 256, 0, e32->s>>>(e32->d_G, G64,
+                                                          (size_t)e64->V * 9);
+      LAUNCHED(1);
+      CK(cudaStreamSynchronize(e32->s));
+      k_apply_gauge<<<e64->nb_site, kSiteThreads, 0, e64->s>>>(e64->c, G64);
+      LAUNCHED(1);
+    }
+    res.iters_fp32 = (it32 == kSentinel) ? p32.max_iters : it32;
+    Params p64 = p;
+    if (p.traj_cap) {
+      p64.traj_theta = p.traj_theta ? p.traj_theta + tl32 : nullptr;
+      p64.traj_func = p.traj_func ? p.traj_func + tl32 : nullptr;
+      p64.traj_cap = p.traj_cap > tl32 ? p.traj_cap - tl32 : 0;
+    }
+    size_t it64 = 0;
+    if (e64->solve(p64, &it64, &th)) return -1;
+    if (e64->fetch_traj(p64, &tl)) return -1;
+    tl += tl32;
+    iters = (it64 == kSentinel) ? kSentinel : res.iters_fp32 + it64;
+  } else {
+    if (e64->solve(p, &iters, &th)) return -1;
+    if (e64->fetch_traj(p, &tl)) return -1;
+  }
+  CK(cudaEventRecord(e64->ev1, e64->s));
+  if (e64->to_aos(e64->d_aos)) return -1;
+  CK(cudaStreamSynchronize(e64->s));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e64->ev0, e64->ev1));
+  res.iters = iters;
+  res.theta = th;
+  res.traj_len = tl;
+  res.gpu_ms = ms;
+  if (r) *r = res;
+  return 0;
+}
+
+}  // namespace gfix
+
+using namespace gfix;
+
+// ---------------------------------------------------------------------
+// flat C ABI
+
+extern "C" {
+
+const char *gfix_last_error(void) { return g_err.c_str(); }
+
+unsigned long long gfix_kernel_launches(void) { return g_launches.load(); }
+
+void gfix_release(void) {
+  g_e64.clear();
+  g_e32.clear();
+}
+
+static int check_params(const size_t *dims, const gfix_params *p) {
+  if (!dims || !p) return fail("null dims or params");
+  for (int i = 0; i < 4; i++)
+    if (dims[i] < 2) return fail("extent %zu of dimension %d below 2", dims[i], i);
+  if (p->algo != GFIX_CG && p->algo != GFIX_SD) return fail("unknown algo %d", p->algo);
+  if (p->precision != GFIX_FP64 && p->precision != GFIX_MIXED)
+    return fail("unknown precision %d", p->precision);
+  if (p->traj_cap && !p->traj_theta) return fail("traj_cap without traj_theta");
+  return 0;
+}
+
+int gfix_landau(double *links, const size_t dims[4], const gfix_params *p,
+                gfix_result *r) {
+  if (check_params(dims, p)) return -1;
+  if (!links) return fail("null links");
+  Engine<double> *e = engine64(dims);
+  if (!e) return -1;
+  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
+  if (landau_staged(e, p, r)) return -1;
+  CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
+  CK(cudaStreamSynchronize(e->s));
+  return 0;
+}
+
+int gfix_landau_device(double *d_links, const size_t dims[4],
+                       const gfix_params *p, gfix_result *r) {
+  if (check_params(dims, p)) return -1;
+  if (!d_links) return fail("null links");
+  Engine<double> *e = engine64(dims);
+  if (!e) return -1;
+  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+  // the caller's buffer is on the legacy default stream order
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpyAsync(e->d_aos, d_links, bytes, cudaMemcpyDeviceToDevice, e->s));
+  if (landau_staged(e, p, r)) return -1;
+  CK(cudaMemcpyAsync(d_links, e->d_aos, bytes, cudaMemcpyDeviceToDevice, e->s));
+  CK(cudaStreamSynchronize(e->s));
+  return 0;
+}
+
+int gfix_observables(const double *links, const size_t dims[4], double *out) {
+  if (!links || !dims || !out) return fail("null argument");
+  Engine<double> *e = engine64(dims);
+  if (!e) return -1;
+  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
+  if (e->from_aos(e->d_aos)) return -1;
+  Params p;
+  if (e->reset(p)) return -1;
+  double tt = 0;
+  if (e->theta_test(&tt)) return -1;
+  // theta_test leaves the functional sum of the same links in func
+  out[0] = tt;
+  out[1] = e->h_st->func;
+  k_plaquette<double><<<e->nb_site, kSiteThreads, 0, e->s>>>(e->c);
+  LAUNCHED(1);
+  std::vector<double> part(e->nb_site);
+  CK(cudaMemcpyAsync(part.data(), e->d_part, part.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost, e->s));
+  CK(cudaStreamSynchronize(e->s));
+  double sum = 0.0;
+  for (double v : part) sum += v;
+  out[2] = 2.0 * sum / (3.0 * 4 * 3 * (double)e->V);
+  return 0;
+}
+
+int gfix_reunit(double *links, const size_t dims[4]) {
+  if (!links || !dims) return fail("null argument");
+  Engine<double> *e = engine64(dims);
+  if (!e) return -1;
+  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
+  if (e->from_aos(e->d_aos)) return -1;
+  const size_t nl = (size_t)e->V * 4;
+  k_reunit_links<double><<<(unsigned)((nl + 255) / 256), 256, 0, e->s>>>(
+      e->d_U, nl, (size_t)e->V);
+  LAUNCHED(1);
+  if (e->to_aos(e->d_aos)) return -1;
+  CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
+  CK(cudaStreamSynchronize(e->s));
+  return 0;
+}
+
+int gfix_fourier_accelerate(double *fields, const size_t dims[4], int ndim) {
+  if (!fields || !dims) return fail("null argument");
+  if (ndim != 4) return fail("only the 4D (Landau) transform is built here");
+  Engine<double> *e = engine64(dims);
+  if (!e) return -1;
+  const size_t bytes = (size_t)e->V * 4 * sizeof(double2);
+  Params p;
+  if (e->reset(p)) return -1;
+  CK(cudaMemcpyAsync(e->c.fb[0], fields, bytes, cudaMemcpyHostToDevice, e->s));
+  e->fft(false);
+  CK(cudaMemcpyAsync(fields, e->c.fb[0], bytes, cudaMemcpyDeviceToHost, e->s));
+  CK(cudaStreamSynchronize(e->s));
+  return 0;
+}
+
+int gfix_profile_landau(const double *d_links, const size_t dims[4],
+                        const gfix_params *p, int iters, double *ms,
+                        double *bytes) {
+  if (check_params(dims, p)) return -1;
+  if (!d_links || !ms || iters < 1) return fail("bad profile arguments");
+  Engine<double> *e = engine64(dims);
+  if (!e) return -1;
+  const size_t n = (size_t)e->V * 36 * sizeof(double2);
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpyAsync(e->d_aos, d_links, n, cudaMemcpyDeviceToDevice, e->s));
+  if (e->from_aos(e->d_aos)) return -1;
+  Params q = to_params(p);
+  q.traj_cap = 0;
+  if (p->precision == GFIX_MIXED) {
+    Engine<float> *f = engine32(dims);
+    if (!f) return -1;
+    CK(cudaStreamSynchronize(e->s));
+    k_convert<double, float><<<1184, 256, 0, f->s>>>(e->d_U, f->d_U,
+                                                     (size_t)e->V * 36);
+    k_identity<float><<<(e->V + 255) / 256, 256, 0, f->s>>>(f->d_G, e->V);
+    LAUNCHED(2);
+    return f->profile_cg(q, iters, ms, bytes);
+  }
+  return e->profile_cg(q, iters, ms, bytes);
+}
+
+int gfix_coulomb(double *links, const size_t dims[4], const gfix_params *p,
+                 gfix_result *r, double *slice_theta, size_t *slice_iters) {
+  (void)links; (void)dims; (void)p; (void)r; (void)slice_theta;
+  (void)slice_iters;
+  return fail("Coulomb gauge fixing is not built yet");
+}
+
+int gfix_coulomb_device(double *d_links, const size_t dims[4],
+                        const gfix_params *p, gfix_result *r,
+                        double *slice_theta, size_t *slice_iters) {
+  return gfix_coulomb(d_links, dims, p, r, slice_theta, slice_iters);
+}
+
+}  // extern "C"

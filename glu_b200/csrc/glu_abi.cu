@@ -1,0 +1,253 @@
+// GLU's gauge-fixing entry points on top of the flat gfix_* interface.
+//
+// The caller is GLU (or a program built like it): `lat` is GLU's AoS
+// lattice, the lattice shape and GF_TUNE are read from GLU's global Latt.
+// Each call gathers the links into one contiguous buffer, runs the GPU
+// solve, scatters them back, and follows GLU's return conventions.
+#include <cuda_runtime.h>
+#include <omp.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/glu_gfix.h"
+#include "glu_compat.h"
+
+using gfix::glu_fftw_stuff;
+using gfix::glu_latt_info;
+using gfix::glu_site;
+
+// GLU's global lattice description (src/Run/Mainfile.c:30).  Weak: inside
+// the GLU program its own definition is the one every reference binds to.
+extern "C" {
+__attribute__((weak)) glu_latt_info Latt;
+}
+
+namespace {
+
+constexpr size_t kSentinel = 123456789;
+constexpr size_t kGluFailure = (size_t)-1;  // GLU_FAILURE returned as size_t
+
+// optional precision selection for the drop-in entry points:
+//   GLU_GFIX_PRECISION = FP64 (default) | MIXED
+//   GLU_GFIX_SWITCH    = x  (FP32 until theta < 10^-x, default 9)
+void env_precision(gfix_params *p) {
+  p->precision = GFIX_FP64;
+  p->switch_theta = 1e-9;
+  if (const char *s = getenv("GLU_GFIX_PRECISION"))
+    if (!strcmp(s, "MIXED") || !strcmp(s, "mixed")) p->precision = GFIX_MIXED;
+  if (const char *s = getenv("GLU_GFIX_SWITCH")) {
+    const double x = atof(s);
+    if (x > 0) p->switch_theta = pow(10.0, -x);
+  }
+}
+
+void dims_of(size_t *d) {
+  for (int i = 0; i < 4; i++) d[i] = Latt.dims[i];
+}
+
+size_t volume() { return Latt.dims[0] * Latt.dims[1] * Latt.dims[2] * Latt.dims[3]; }
+
+// lat[i].O[mu] (separate 144-byte allocations) <-> contiguous double[V][4][18]
+void gather(const glu_site *lat, double *buf, size_t V) {
+#pragma omp parallel for
+  for (long long i = 0; i < (long long)V; i++)
+    for (int mu = 0; mu < 4; mu++)
+      memcpy(buf + ((size_t)i * 4 + mu) * 18, lat[i].O[mu], 18 * sizeof(double));
+}
+
+void scatter(glu_site *lat, const double *buf, size_t V) {
+#pragma omp parallel for
+  for (long long i = 0; i < (long long)V; i++)
+    for (int mu = 0; mu < 4; mu++)
+      memcpy(lat[i].O[mu], buf + ((size_t)i * 4 + mu) * 18, 18 * sizeof(double));
+}
+
+struct Pinned {
+  double *p = nullptr;
+  explicit Pinned(size_t n) {
+    if (cudaMallocHost(&p, n * sizeof(double)) != cudaSuccess) p = nullptr;
+  }
+  ~Pinned() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+size_t landau_fa(glu_site *lat, double *th, double acc, size_t max_iters,
+                 int algo) {
+  size_t d[4];
+  dims_of(d);
+  const size_t V = volume();
+  Pinned buf(V * 72);
+  if (!buf.p) {
+    fprintf(stderr, "[FACG] allocation of temporaries failed\n");
+    return 0;
+  }
+  gather(lat, buf.p, V);
+  gfix_params p;
+  memset(&p, 0, sizeof p);
+  p.gf_alpha = Latt.gf_alpha;
+  p.accuracy = acc;
+  p.max_iters = max_iters;
+  p.algo = algo;
+#ifdef GLU_GFIX_SD
+  p.sd_fixed_step = 1;
+#endif
+  env_precision(&p);
+  gfix_result r;
+  if (gfix_landau(buf.p, d, &p, &r) != 0) {
+    fprintf(stderr, "[GF] GPU gauge fixing failed: %s\n", gfix_last_error());
+    return 0;
+  }
+  scatter(lat, buf.p, V);
+  *th = r.theta;
+  return r.iters;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t FACG(struct site *lat, struct fftw_stuff *FFTW, double *th,
+            const double acc, const size_t max_iters) {
+  (void)FFTW;
+  return landau_fa(reinterpret_cast<glu_site *>(lat), th, acc, max_iters,
+                   GFIX_CG);
+}
+
+size_t FASD(struct site *lat, struct fftw_stuff *FFTW, double *th,
+            const double acc, const size_t max_iters) {
+  (void)FFTW;
+  return landau_fa(reinterpret_cast<glu_site *>(lat), th, acc, max_iters,
+                   GFIX_SD);
+}
+
+void FOURIER_ACCELERATE3(struct fftw_stuff *FFTW) {
+  glu_fftw_stuff *F = reinterpret_cast<glu_fftw_stuff *>(FFTW);
+  size_t d[4];
+  dims_of(d);
+  const size_t V = volume();
+  std::vector<double> f(V * 8);
+  for (int k = 0; k < 4; k++)
+    memcpy(f.data() + (size_t)k * V * 2, F->in[k], V * 2 * sizeof(double));
+  if (gfix_fourier_accelerate(f.data(), d, 4) != 0) {
+    fprintf(stderr, "[GF] GPU Fourier acceleration failed: %s\n",
+            gfix_last_error());
+    return;
+  }
+  for (int k = 0; k < 4; k++)
+    memcpy(F->in[k], f.data() + (size_t)k * V * 2, V * 2 * sizeof(double));
+}
+
+size_t Landau(struct site *lat, const double accuracy, const size_t iter,
+              const char *infile) {
+  (void)infile;
+  glu_site *L = reinterpret_cast<glu_site *>(lat);
+  size_t d[4];
+  dims_of(d);
+  const size_t V = volume();
+  Pinned buf(V * 72);
+  if (!buf.p) return kGluFailure;
+  gather(L, buf.p, V);
+  gfix_params p;
+  memset(&p, 0, sizeof p);
+  p.gf_alpha = Latt.gf_alpha;
+  p.accuracy = accuracy;
+  p.max_iters = iter;
+  p.algo = GFIX_CG;
+#ifdef GLU_GFIX_SD
+  p.algo = GFIX_SD;
+  p.sd_fixed_step = 1;
+#endif
+  env_precision(&p);
+  gfix_result r;
+  if (gfix_landau(buf.p, d, &p, &r) != 0) {
+    fprintf(stderr, "[GF] GPU gauge fixing failed: %s\n", gfix_last_error());
+    return kGluFailure;
+  }
+  if (r.iters == kSentinel) {
+    fprintf(stderr,
+            "\n[GF] Insufficient Convergence ......\n\n"
+            "[GF] -> Try reducing the tuning parameter OR/AND\n"
+            "increasing the maximum number of iterations -< \n\n");
+    printf("\n[GF] Failure to converge to a sufficient solution \n"
+           "[GF] Please lower the GF_TUNE parameter from %g \n",
+           Latt.gf_alpha);
+    return kGluFailure;
+  }
+  // output_fixing_info (src/Gfix/Landau.c:42-66): reunitarise, report
+  gfix_reunit(buf.p, d);
+  double obs[3] = {0, 0, 0};
+  gfix_observables(buf.p, d, obs);
+  scatter(L, buf.p, V);
+  printf("[GF] Plaquette :: %1.15f \n[GF] Accuracy :: %1.4e\n", obs[2],
+         r.theta);
+  printf("[GF] Iters :: %zu\n", r.iters);
+  printf("[GF] Functional :: %1.15f\n", obs[1]);
+  return r.iters;
+}
+
+size_t Coulomb_FA(struct site *lat, struct fftw_stuff *FFTW,
+                  const double accuracy, const size_t max_iter,
+                  const int FACG_flag) {
+  (void)FFTW;
+  glu_site *L = reinterpret_cast<glu_site *>(lat);
+  size_t d[4];
+  dims_of(d);
+  const size_t V = volume();
+  Pinned buf(V * 72);
+  if (!buf.p) return 0;
+  gather(L, buf.p, V);
+  gfix_params p;
+  memset(&p, 0, sizeof p);
+  p.gf_alpha = Latt.gf_alpha;
+  p.accuracy = accuracy;
+  p.max_iters = max_iter;
+  p.algo = FACG_flag ? GFIX_CG : GFIX_SD;
+#ifdef GLU_GFIX_SD
+  p.sd_fixed_step = 1;
+#endif
+  env_precision(&p);
+  gfix_result r;
+  if (gfix_coulomb(buf.p, d, &p, &r, nullptr, nullptr) != 0) {
+    fprintf(stderr, "[CG] GPU Coulomb gauge fixing failed: %s\n",
+            gfix_last_error());
+    return 0;
+  }
+  scatter(L, buf.p, V);
+  return r.iters;
+}
+
+size_t Coulomb(struct site *lat, const double accuracy, const size_t iter) {
+  size_t it = Coulomb_FA(lat, nullptr, accuracy, iter,
+#ifdef GLU_GFIX_SD
+                         0
+#else
+                         1
+#endif
+  );
+  // latt_reunitU after the fix (src/Gfix/Coulomb.c:97)
+  glu_site *L = reinterpret_cast<glu_site *>(lat);
+  size_t d[4];
+  dims_of(d);
+  const size_t V = volume();
+  Pinned buf(V * 72);
+  if (!buf.p) return it;
+  gather(L, buf.p, V);
+  gfix_reunit(buf.p, d);
+  double obs[3] = {0, 0, 0};
+  gfix_observables(buf.p, d, obs);
+  scatter(L, buf.p, V);
+  printf("[GF] Tuning :: %f || Iterations :: %zu ||\n[GF] Plaquette :: %1.15f \n",
+         Latt.gf_alpha, it, obs[2]);
+  return it;
+}
+
+void FOURIER_ACCELERATE2(struct fftw_stuff *FFTW) {
+  (void)FFTW;
+  fprintf(stderr, "[GF] FOURIER_ACCELERATE2 on the GPU needs gfix_coulomb\n");
+}
+
+}  // extern "C"

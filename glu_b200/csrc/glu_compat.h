@@ -1,0 +1,45 @@
+// Layout mirrors of the GLU types the drop-in entry points read
+// (src/Headers/GLU_types.h, default build: NC = 3, ND = 4, double
+// precision, FFTW present).  Field order and types follow GLU exactly so
+// that a pointer handed over by GLU can be read here.
+#pragma once
+
+#include <stddef.h>
+#include <stdint.h>
+
+namespace gfix {
+
+// struct site (src/Headers/GLU_types.h:269-273)
+struct glu_site {
+  double **O;  // GLU_complex **O: O[mu] -> 9 complex, row-major
+  size_t neighbor[4];
+  size_t back[4];
+};
+
+// struct fftw_stuff (src/Headers/GLU_types.h:126-137)
+struct glu_fftw_stuff {
+  double **out;  // GLU_complex **
+  double **in;   // GLU_complex **
+  void *forward;
+  void *backward;
+  double *psq;
+};
+
+// struct latt_info (src/Headers/GLU_types.h:229-243)
+struct glu_latt_info {
+  size_t dims[4];
+  size_t Lsq;
+  size_t Lcu;
+  size_t Volume;
+  size_t flow;
+  double gf_alpha;
+  double sm_alpha[3];
+  int head;  // header_mode enum
+  uint32_t Seed[1];
+  double twiddles[4];
+  uint32_t Nthreads;
+  void *su2_data;
+  int argc;  // cline_arg enum
+};
+
+}  // namespace gfix

@@ -1,0 +1,612 @@
+// Device kernels of the Fourier-accelerated Landau gauge fixing on B200.
+//
+// One iteration of FACG (src/Gfix/FACG.c:270-334) is the launch sequence
+//   k_deriv          Delta(x) packed in 4 fields + theta and Re tr U partials
+//   k_scalar THETA   theta, functional, stop decision
+//   k_fft_xy  fwd    x,y passes of the 4D FFT, one xy-plane per block
+//   k_fft_zt         z,t passes, * psq, inverse t,z passes (one tile/block)
+//   k_fft_xy  bwd    inverse x,y passes fused with the PR sums
+//   k_scalar PR      beta (PR+ / FR switch at CG_TOL)
+//   k_dir_probe      sn <- in + beta sn, line-search probes of GLU's
+//                    line_search_Landau (src/Gfix/line_search.c:274-341)
+//   k_scalar PROBES  alpha* by the parabola of approx_minimum
+//   k_update         U_mu(x) <- g(x) U_mu(x) g(x+mu)^dag, g = reunit(1+a A)
+//   k_scalar END     iteration count, buffer parities, done flag
+// Every kernel first checks the device-side done flag, so a captured graph
+// of the iteration can be replayed past convergence as a no-op.
+//
+// HBM layout (SoA, site index s = x + Lx (y + Ly (z + Lz t))):
+//   U   cx<R>[4 mu][9 elements][V]        links
+//   fb  cx<R>[2][4 fields][V]             in / in_old (parity selects)
+//   sb  cx<R>[2][4 fields][V]             sn ping-pong (sparity selects)
+//   G   cx<R>[9][V]                        accumulated gauge transform
+//                                          (mixed precision only)
+#pragma once
+
+#include "fft.cuh"
+#include "su3.cuh"
+
+namespace gfix {
+
+constexpr double kCgTol = 5E-11;            // GLU_definitions.h:451-455
+constexpr double kVal49 = 0.4444444444444444;  // lin_derivs.c:72
+constexpr int kSiteThreads = 128;
+constexpr int kScalarThreads = 1024;
+
+enum ScalarOp : int {
+  OP_THETA_TEST = 0,  // theta_test_lin = 2 sum / (NC V)
+  OP_THETA_SD,        // theta of an SD start: reduction slots carry over
+  OP_THETA_MAIN,      // theta at the top of a CG/SD iteration
+  OP_PR,              // beta of the CG direction
+  OP_PROBES,          // alpha* from the probes (or the fixed step)
+  OP_DER,             // inold after the SD start
+  OP_END_CG,          // end of a CG iteration
+  OP_END_SD,          // end of an SD (FASD) iteration
+  OP_ALPHA_FIXED,     // step = gf_alpha (SD without line search)
+};
+
+struct DevState {
+  double tr;          // in-loop theta of the current iteration
+  double tr_test;     // theta_test_lin
+  double func;        // gauge functional of the current links
+  double inold, insum, sumconj, beta, alpha;
+  double ls_last[2];  // probe sums left in GLU's reduction slots
+  double insum_last;  // insum left in GLU's reduction slot
+  double gf_alpha, acc;
+  long long max_iters;
+  long long iter;     // loc_iters of the current run
+  long long traj_len, traj_cap;
+  double *traj_theta, *traj_func;
+  int use_ls;         // this step uses the line search
+  int stop;           // current iteration is the last one of the run
+  int done;           // run finished: kernels return at once
+  int parity;         // fb[parity] = in, fb[parity ^ 1] = in_old
+  int sparity;        // sb[sparity] = sn (old), sb[sparity ^ 1] = new
+  int nblocks;        // partials written by the last reduction kernel
+  int sd_fixed;       // GLU_GFIX_SD: fixed step gf_alpha in SD steps
+};
+
+// start of a solver run (GLU's steep_Landau_FACG / _FASD entry)
+__global__ void k_begin_run(DevState *st) {
+  st->iter = 0;
+  st->done = 0;
+  st->stop = 0;
+  st->use_ls = !st->sd_fixed;
+}
+
+template <typename R>
+struct Ctx {
+  cx<R> *U;
+  cx<R> *fb[2];
+  cx<R> *sb[2];
+  cx<R> *G;
+  DevState *st;
+  double *part;       // [nblocks][2] per-block partial sums
+  const cx<R> *tw;    // twiddle pool
+  const double *cs;   // cos tables, cs[mu * cs_ld + n] = cos(n 2pi/L_mu)
+  int cs_ld;
+  int L[4];
+  int V;
+  int ndim;           // FFT rank: 4 Landau, 3 Coulomb
+  int zt_b;           // x columns per zt tile
+  int xy_pitch;       // padded row pitch of the xy tile
+  double maxp;        // MAX_LANDAU = 4 ND / V or MAX_COULOMB = 4 (ND-1)/Lcu
+  FftAxis ax[4];
+};
+
+// ---------------------------------------------------------------------
+// helpers
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// deterministic block sum of NV values; thread 0 writes them to out[0..NV)
+template <int NV>
+__device__ __forceinline__ void block_sum_store(double (&v)[NV], double *out) {
+  __shared__ double sh[NV][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; k++) v[k] = warp_sum(v[k]);
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) sh[k][warp] = v[k];
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      double x = lane < nw ? sh[k][lane] : 0.0;
+      x = warp_sum(x);
+      if (lane == 0) out[k] = x;
+    }
+  }
+}
+
+__device__ __forceinline__ void coords(int s, const int *L, int *x) {
+  x[0] = s % L[0];
+  s /= L[0];
+  x[1] = s % L[1];
+  s /= L[1];
+  x[2] = s % L[2];
+  x[3] = s / L[2];
+}
+
+__device__ __forceinline__ int fwd_site(int s, int mu, const int *x,
+                                        const int *L, const int *stride) {
+  return x[mu] == L[mu] - 1 ? s - (L[mu] - 1) * stride[mu] : s + stride[mu];
+}
+__device__ __forceinline__ int bck_site(int s, int mu, const int *x,
+                                        const int *L, const int *stride) {
+  return x[mu] == 0 ? s + (L[mu] - 1) * stride[mu] : s - stride[mu];
+}
+
+template <typename R>
+__device__ __forceinline__ void strides(const Ctx<R> &c, int *st) {
+  st[0] = 1;
+  st[1] = c.L[0];
+  st[2] = c.L[0] * c.L[1];
+  st[3] = c.L[0] * c.L[1] * c.L[2];
+}
+
+template <typename R>
+__device__ __forceinline__ void load_link(const cx<R> *U, int V, int mu, int s,
+                                          cx<R> *u) {
+  const cx<R> *p = U + (size_t)mu * 9 * V + s;
+#pragma unroll
+  for (int e = 0; e < 9; e++) u[e] = p[(size_t)e * V];
+}
+
+template <typename R>
+__device__ __forceinline__ void store_link(cx<R> *U, int V, int mu, int s,
+                                           const cx<R> *u) {
+  cx<R> *p = U + (size_t)mu * 9 * V + s;
+#pragma unroll
+  for (int e = 0; e < 9; e++) p[(size_t)e * V] = u[e];
+}
+
+// ---------------------------------------------------------------------
+// K1: the gauge derivative, fused with the theta and functional sums
+// (src/Gfix/lin_derivs.c:74-193 packed as src/Gfix/FACG.c:54-60)
+
+template <typename R>
+__global__ void __launch_bounds__(kSiteThreads)
+    k_deriv(Ctx<R> c) {
+  if (c.st->done) return;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[2] = {0.0, 0.0};
+  if (s < c.V) {
+    int x[4], sd[4];
+    coords(s, c.L, x);
+    strides(c, sd);
+    R R0 = 0, R1 = 0, I1 = 0, R2 = 0, I2 = 0, R3 = 0, R4 = 0, I4 = 0;
+    double re = 0.0;
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+      const cx<R> *q = c.U + (size_t)mu * 9 * c.V + s;
+      const cx<R> *b = c.U + (size_t)mu * 9 * c.V + bck_site(s, mu, x, c.L, sd);
+      const size_t V = c.V;
+      const cx<R> q0 = q[0], q1 = q[V], q2 = q[2 * V], q3 = q[3 * V],
+                  q4 = q[4 * V], q5 = q[5 * V], q6 = q[6 * V], q7 = q[7 * V],
+                  q8 = q[8 * V];
+      const cx<R> b0 = b[0], b1 = b[V], b2 = b[2 * V], b3 = b[3 * V],
+                  b4 = b[4 * V], b5 = b[5 * V], b6 = b[6 * V], b7 = b[7 * V],
+                  b8 = b[8 * V];
+      R0 += R(2) * b0.y - b4.y - b8.y;
+      R0 += R(-2) * q0.y + q4.y + q8.y;
+      R1 += b1.x - b3.x - q1.x + q3.x;
+      I1 += b1.y + b3.y - q1.y - q3.y;
+      R2 += b2.x - b6.x - q2.x + q6.x;
+      I2 += b2.y + b6.y - q2.y - q6.y;
+      R3 += R(2) * b4.y - b0.y - b8.y;
+      R3 += R(-2) * q4.y + q0.y + q8.y;
+      R4 += b5.x - b7.x - q5.x + q7.x;
+      I4 += b5.y + b7.y - q5.y - q7.y;
+      re += (double)q0.x + (double)q4.x + (double)q8.x;
+    }
+    cx<R> *f = c.fb[c.st->parity];
+    const size_t V = c.V;
+    f[s] = mk<R>(-(R3 / R(3)), R0 / R(3));
+    f[V + s] = mk<R>(R(0.5) * R1, R(0.5) * I1);
+    f[2 * V + s] = mk<R>(R(0.5) * R2, R(0.5) * I2);
+    f[3 * V + s] = mk<R>(R(0.5) * R4, R(0.5) * I4);
+    const double d0 = R0, d1 = R1, e1 = I1, d2 = R2, e2 = I2, d3 = R3,
+                 d4 = R4, e4 = I4;
+    v[0] = kVal49 * (d0 * d0 + d3 * (d3 + d0)) +
+           (d1 * d1 + e1 * e1 + d2 * d2 + e2 * e2 + d4 * d4 + e4 * e4);
+    v[1] = re;
+  }
+  block_sum_store<2>(v, c.part + 2 * blockIdx.x);
+  if (threadIdx.x == 0 && blockIdx.x == 0) c.st->nblocks = gridDim.x;
+}
+
+// ---------------------------------------------------------------------
+// the 4D (or batched 3D) FFT with psq folded into the middle pass
+
+template <typename R>
+__device__ __forceinline__ const cx<R> *axis_tw(const Ctx<R> &c, int a) {
+  return c.tw + c.ax[a].tw_off;
+}
+
+// xy-plane pass: forward (bwd = 0) or inverse with the PR sums of
+// sum_PR3 (src/Gfix/FACG.c:99-145) fused in (prsum = 1).
+template <typename R>
+__global__ void __launch_bounds__(256) k_fft_xy(Ctx<R> c, int bwd, int prsum) {
+  if (c.st->done) return;
+  extern __shared__ unsigned char smem_raw[];
+  cx<R> *A = reinterpret_cast<cx<R> *>(smem_raw);
+  const int Lx = c.L[0], Ly = c.L[1], P = c.xy_pitch;
+  cx<R> *B = A + P * Ly;
+  const int plane = blockIdx.x, field = blockIdx.y;
+  const int par = c.st->parity;
+  const size_t base = (size_t)field * c.V + (size_t)plane * Lx * Ly;
+  cx<R> *data = c.fb[par] + base;
+  const int n = Lx * Ly;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const int x = e % Lx, y = e / Lx;
+    A[y * P + x] = data[e];
+  }
+  __syncthreads();
+  const PencilMap mx = {Ly, 1, 0, P, 1};   // rows
+  const PencilMap my = {Lx, Lx, 1, 0, P};  // columns
+  cx<R> *r = smem_fft(A, B, mx, c.ax[0], axis_tw(c, 0), bwd != 0);
+  cx<R> *o = (r == A) ? B : A;
+  r = smem_fft(r, o, my, c.ax[1], axis_tw(c, 1), bwd != 0);
+  double v[2] = {0.0, 0.0};
+  const cx<R> *old = c.fb[par ^ 1] + base;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const int x = e % Lx, y = e / Lx;
+    const cx<R> w = r[y * P + x];
+    data[e] = w;
+    if (prsum) {
+      const double a = w.x, b = w.y;
+      const cx<R> od = old[e];
+      const double tr = a - (double)od.x, ti = b - (double)od.y;
+      if (field == 0) {
+        v[0] += 2.0 * (a * a + b * b + a * b);
+        v[1] += 2.0 * (a * tr + b * ti) + (a * ti + b * tr);
+      } else {
+        v[0] += 2.0 * (a * a + b * b);
+        v[1] += 2.0 * (a * tr + b * ti);
+      }
+    }
+  }
+  if (prsum) {
+    block_sum_store<2>(v, c.part + 2 * (blockIdx.y * gridDim.x + blockIdx.x));
+    if (threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0)
+      c.st->nblocks = gridDim.x * gridDim.y;
+  }
+}
+
+// z(,t) pass: forward z (and t), multiply by psq = maxp / p^2 with
+// p^2 = 2 (D - sum_mu cos(2 pi n_mu / L_mu)), p = 0 -> 1
+// (src/Geometry/geometry.c:169-186), then inverse t (and z).
+// Landau: tile = zt_b consecutive x at fixed y, all z and t.
+// Coulomb: tile = zt_b consecutive x at fixed (y, t), all z.
+template <typename R>
+__global__ void __launch_bounds__(256) k_fft_zt(Ctx<R> c) {
+  if (c.st->done) return;
+  extern __shared__ unsigned char smem_raw[];
+  const int Lx = c.L[0], Ly = c.L[1], Lz = c.L[2], Lt = c.L[3];
+  const int Bw = c.zt_b;
+  const bool four = (c.ndim == 4);
+  const int nt = four ? Lt : 1;
+  cx<R> *A = reinterpret_cast<cx<R> *>(smem_raw);
+  cx<R> *Bf = A + Bw * Lz * nt;
+  int tile = blockIdx.x;
+  const int xb = tile % (Lx / Bw);
+  tile /= (Lx / Bw);
+  const int y = tile % Ly;
+  const int tslice = four ? 0 : tile / Ly;
+  const int field = blockIdx.y;
+  cx<R> *data = c.fb[c.st->parity] + (size_t)field * c.V;
+  const int x0 = xb * Bw;
+  const int n = Bw * Lz * nt;
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const int b = e % Bw, rest = e / Bw;
+    const int z = rest % Lz, t = four ? rest / Lz : tslice;
+    const size_t g = (size_t)(x0 + b) + (size_t)Lx * (y + (size_t)Ly * (z + (size_t)Lz * t));
+    A[e] = data[g];
+  }
+  __syncthreads();
+  const PencilMap mz = {nt * Bw, Bw, 1, Lz * Bw, Bw};
+  const PencilMap mt = {Lz * Bw, Lz * Bw, 1, 0, Lz * Bw};
+  cx<R> *r = smem_fft(A, Bf, mz, c.ax[2], axis_tw(c, 2), false);
+  if (four) {
+    cx<R> *o = (r == A) ? Bf : A;
+    r = smem_fft(r, o, mt, c.ax[3], axis_tw(c, 3), false);
+  }
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const int b = e % Bw, rest = e / Bw;
+    const int z = rest % Lz, t = rest / Lz;
+    double kcos = 0.0;
+    kcos += c.cs[0 * c.cs_ld + x0 + b];
+    kcos += c.cs[1 * c.cs_ld + y];
+    kcos += c.cs[2 * c.cs_ld + z];
+    if (four) kcos += c.cs[3 * c.cs_ld + t];
+    const double D = four ? 4.0 : 3.0;
+    const double p2 = (kcos == D) ? 1.0 : 2.0 * (D - kcos);
+    const R ps = (R)(c.maxp / p2);
+    r[e] = mk<R>(r[e].x * ps, r[e].y * ps);
+  }
+  __syncthreads();
+  {
+    cx<R> *o = (r == A) ? Bf : A;
+    if (four) {
+      r = smem_fft(r, o, mt, c.ax[3], axis_tw(c, 3), true);
+      o = (r == A) ? Bf : A;
+    }
+    r = smem_fft(r, o, mz, c.ax[2], axis_tw(c, 2), true);
+  }
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    const int b = e % Bw, rest = e / Bw;
+    const int z = rest % Lz, t = four ? rest / Lz : tslice;
+    const size_t g = (size_t)(x0 + b) + (size_t)Lx * (y + (size_t)Ly * (z + (size_t)Lz * t));
+    data[g] = r[e];
+  }
+}
+
+// ---------------------------------------------------------------------
+// K4: conjugate direction update fused with the line-search probes.
+// DIR: sn_new = in + beta sn_old (src/Gfix/FACG.c:315-323), else the
+// direction is `in` itself (an SD step).  Probes: per site the three
+// values of src/Gfix/line_search.c:296-313 at alpha = 0, 0.15, 0.30;
+// accumulated as differences to the alpha = 0 value, which leaves the
+// parabola of approx_minimum unchanged and avoids cancelling large sums.
+
+template <typename R, bool DIR>
+__device__ __forceinline__ void dir_at(const Ctx<R> &c, const cx<R> *in,
+                                       const cx<R> *so, R beta, int s,
+                                       cx<R> *f) {
+  const size_t V = c.V;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const cx<R> a = in[k * V + s];
+    if (DIR) {
+      const cx<R> b = so[k * V + s];
+      f[k] = mk<R>(fma(beta, b.x, a.x), fma(beta, b.y, a.y));
+    } else {
+      f[k] = a;
+    }
+  }
+}
+
+template <typename R, bool DIR>
+__global__ void __launch_bounds__(kSiteThreads) k_dir_probe(Ctx<R> c) {
+  if (c.st->done) return;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int par = c.st->parity, spar = c.st->sparity;
+  const cx<R> *in = c.fb[par];
+  const cx<R> *so = c.sb[spar];
+  cx<R> *sn = c.sb[spar ^ 1];
+  const R beta = (R)c.st->beta;
+  const bool probes = c.st->use_ls != 0;
+  double v[2] = {0.0, 0.0};
+  if (s < c.V) {
+    cx<R> f[4];
+    dir_at<R, DIR>(c, in, so, beta, s, f);
+    if (DIR) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) sn[(size_t)k * c.V + s] = f[k];
+    }
+    if (probes) {
+      int x[4], sd[4];
+      coords(s, c.L, x);
+      strides(c, sd);
+      cx<R> A1[9], A2[9], Bm[9], U[9];
+      set_gauge(A1, f[0], f[1], f[2], f[3], R(0.15));
+      set_gauge(A2, f[0], f[1], f[2], f[3], R(0.30));
+      R d1 = 0, d2 = 0;
+#pragma unroll 1
+      for (int mu = 0; mu < 4; mu++) {
+        const int y = fwd_site(s, mu, x, c.L, sd);
+        cx<R> fy[4];
+        dir_at<R, DIR>(c, in, so, beta, y, fy);
+        load_link(c.U, c.V, mu, s, U);
+        const R t0 = U[0].x + U[4].x + U[8].x;
+        set_gauge(Bm, fy[0], fy[1], fy[2], fy[3], R(0.15));
+        d1 += re_tr_abc_dag(A1, U, Bm) - t0;
+        set_gauge(Bm, fy[0], fy[1], fy[2], fy[3], R(0.30));
+        d2 += re_tr_abc_dag(A2, U, Bm) - t0;
+      }
+      v[0] = d1;
+      v[1] = d2;
+    }
+  }
+  if (probes) {
+    block_sum_store<2>(v, c.part + 2 * blockIdx.x);
+    if (threadIdx.x == 0 && blockIdx.x == 0) c.st->nblocks = gridDim.x;
+  }
+}
+
+// ---------------------------------------------------------------------
+// K5: the link update of egauge_Landau (src/Gfix/line_search.c:60-97):
+// g(x) = reunit(1 + alpha A(x)), U_mu(x) <- g(x) U_mu(x) g(x+mu)^dag.
+// SN selects the direction: the new conjugate direction or `in`.
+// With G (mixed precision) the transform is accumulated, G(x) <- g(x) G(x).
+
+template <typename R, bool SN>
+__global__ void __launch_bounds__(kSiteThreads) k_update(Ctx<R> c) {
+  if (c.st->done) return;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= c.V) return;
+  const cx<R> *d = SN ? c.sb[c.st->sparity ^ 1] : c.fb[c.st->parity];
+  const R alpha = (R)c.st->alpha;
+  const size_t V = c.V;
+  int x[4], sd[4];
+  coords(s, c.L, x);
+  strides(c, sd);
+  cx<R> A[9], Bm[9], U[9];
+  set_gauge(A, d[s], d[V + s], d[2 * V + s], d[3 * V + s], alpha);
+#pragma unroll 1
+  for (int mu = 0; mu < 4; mu++) {
+    const int y = fwd_site(s, mu, x, c.L, sd);
+    set_gauge(Bm, d[y], d[V + y], d[2 * V + y], d[3 * V + y], alpha);
+    load_link(c.U, c.V, mu, s, U);
+    gtransform(A, U, Bm);
+    store_link(c.U, c.V, mu, s, U);
+  }
+  if (c.G) {
+    cx<R> g[9], r[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) g[e] = c.G[(size_t)e * V + s];
+    multab(r, A, g);
+#pragma unroll
+    for (int e = 0; e < 9; e++) c.G[(size_t)e * V + s] = r[e];
+  }
+}
+
+// sn = in_old = in after an SD start, with sum_DER3 (src/Gfix/FACG.c:148-178)
+template <typename R>
+__global__ void __launch_bounds__(256) k_copy_der(Ctx<R> c) {
+  if (c.st->done) return;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const cx<R> *in = c.fb[c.st->parity];
+  cx<R> *sn = c.sb[c.st->sparity];
+  double v[1] = {0.0};
+  if (s < c.V) {
+    double l = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const cx<R> a = in[(size_t)k * c.V + s];
+      sn[(size_t)k * c.V + s] = a;
+      const double ar = a.x, ai = a.y;
+      l += (k == 0) ? (ar * ar + ai * ai + ar * ai) : (ar * ar + ai * ai);
+    }
+    v[0] = 2.0 * l;
+  }
+  block_sum_store<1>(v, c.part + blockIdx.x);
+  if (threadIdx.x == 0 && blockIdx.x == 0) c.st->nblocks = gridDim.x;
+}
+
+// ---------------------------------------------------------------------
+// scalar logic: one block reduces the partials in a fixed order and applies
+// GLU's control flow for the step.
+
+__device__ __forceinline__ double approx_minimum(const double *al,
+                                                 const double *f) {
+  // src/Gfix/line_search.c:38-57
+  const double A = f[0] / ((al[0] - al[1]) * (al[0] - al[2]));
+  const double B = f[1] / ((al[1] - al[0]) * (al[1] - al[2]));
+  const double C = f[2] / ((al[2] - al[0]) * (al[2] - al[1]));
+  const double Sol = (al[0] * (B + C) + al[1] * (A + C) + al[2] * (A + B)) /
+                     (2 * (A + B + C));
+  if (Sol > al[2]) return al[2];
+  if (isnan(Sol) || isinf(Sol) || Sol < al[0]) return 0.08;
+  return Sol;
+}
+
+__global__ void __launch_bounds__(kScalarThreads)
+    k_scalar(DevState *st, const double *part, int op, int nv, double norm_v) {
+  if (st->done) return;
+  const int nb = st->nblocks;
+  double a[2] = {0.0, 0.0};
+  if (op != OP_END_CG && op != OP_END_SD && op != OP_ALPHA_FIXED) {
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+      a[0] += part[(size_t)nv * i];
+      if (nv > 1) a[1] += part[(size_t)nv * i + 1];
+    }
+    __shared__ double tot[2];
+    block_sum_store<2>(a, tot);
+    __syncthreads();
+    a[0] = tot[0];
+    a[1] = tot[1];
+  }
+  if (threadIdx.x != 0) return;
+  // norm_v = number of sites V
+  const double V = norm_v;
+  switch (op) {
+    case OP_THETA_TEST:
+      st->tr_test = 2.0 * a[0] / (3.0 * V);
+      st->func = 1.0 - a[1] / (12.0 * V);
+      break;
+    case OP_THETA_SD:
+    case OP_THETA_MAIN: {
+      st->tr = a[0] / (3.0 * V);  // GFNORM_LANDAU
+      st->func = 1.0 - a[1] / (12.0 * V);
+      if (st->traj_theta && st->traj_len < st->traj_cap) {
+        st->traj_theta[st->traj_len] = st->tr;
+        st->traj_func[st->traj_len] = st->func;
+        st->traj_len++;
+      }
+      if (op == OP_THETA_MAIN) {
+        // the top of a loop iteration zeroes GLU's reduction slots
+        st->ls_last[0] = st->ls_last[1] = 0.0;
+        st->stop = !((st->tr > st->acc) && (st->iter + 1 < st->max_iters));
+      }
+      break;
+    }
+    case OP_PR: {
+      st->insum = a[0];
+      st->sumconj = a[1];
+      const double b = st->sumconj / st->inold;
+      double beta = (b < 0.0) ? 0.0 : b;  // PRfmax (src/Gfix/CG.c:37-41)
+      if (st->tr < kCgTol) beta = st->insum / st->inold;
+      st->beta = beta;
+      st->inold = st->insum;
+      st->insum_last = st->insum;
+      st->use_ls = st->tr > kCgTol;
+      break;
+    }
+    case OP_PROBES: {
+      if (st->use_ls) {
+        const double d1 = a[0] + st->ls_last[0], d2 = a[1] + st->ls_last[1];
+        st->ls_last[0] = d1;
+        st->ls_last[1] = d2;
+        const double al[3] = {0.0, 0.15, 0.30};
+        const double f[3] = {0.0, -d1, -d2};
+        st->alpha = approx_minimum(al, f);
+      } else {
+        st->alpha = st->gf_alpha;
+      }
+      break;
+    }
+    case OP_ALPHA_FIXED:
+      st->alpha = st->gf_alpha;
+      break;
+    case OP_DER:
+      st->inold = st->insum_last + a[0];
+      st->parity ^= 1;  // in_old = in
+      break;
+    case OP_END_CG:
+      st->iter++;
+      st->parity ^= 1;
+      st->sparity ^= 1;
+      if (st->stop) st->done = 1;
+      break;
+    case OP_END_SD:
+      st->iter++;
+      if (st->stop) st->done = 1;
+      break;
+  }
+}
+
+// ---------------------------------------------------------------------
+// layout conversion: host AoS double[V][4][9][2] <-> device SoA cx<R>
+
+template <typename R>
+__global__ void k_aos_to_soa(const double *__restrict__ aos, cx<R> *U, int V) {
+  const size_t n = (size_t)V * 36;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int s = (int)(i / 36), r = (int)(i % 36);  // r = mu*9 + e
+    const double2 v = reinterpret_cast<const double2 *>(aos)[i];
+    U[(size_t)r * V + s] = mk<R>((R)v.x, (R)v.y);
+  }
+}
+
+template <typename R>
+__global__ void k_soa_to_aos(const cx<R> *U, double *__restrict__ aos, int V) {
+  const size_t n = (size_t)V * 36;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int s = (int)(i / 36), r = (int)(i % 36);
+    const cx<R> v = U[(size_t)r * V + s];
+    reinterpret_cast<double2 *>(aos)[i] = make_double2((double)v.x, (double)v.y);
+  }
+}
+
+}  // namespace gfix

@@ -1,0 +1,195 @@
+"""Python mirror of GLU's gauge-fixing interface, backed by libglu_gfix.so.
+
+Names, arguments and return conventions follow the reference:
+
+* ``FACG`` / ``FASD`` -- src/Gfix/FACG.c:341 / :395: return the iteration
+  count (``SENTINEL`` = 123456789 on non-convergence) and theta.
+* ``Landau`` -- src/Gfix/Landau.c:261: FA solve, reunitarisation.
+* ``Coulomb_FA`` / ``Coulomb`` -- src/Gfix/CFACG.c:531 / Coulomb.c:32.
+* ``theta_test_lin``, ``gauge_functional`` (src/Gfix/gftests.c:214, :132),
+  ``av_plaquette`` (src/Field/plaqs_links.c:243), ``latt_reunitU``
+  (src/Geometry/random_config.c:43).
+
+Links are numpy complex128 arrays of shape (V, 4, 3, 3) in GLU's memory
+order (site index x fastest), or (Lt, Lz, Ly, Lx, 4, 3, 3); ``dims`` is
+(Lx, Ly, Lz, Lt) as in GLU's ``Latt.dims``.  The functions return new
+arrays and leave their input untouched.  Every call runs on the GPU; there
+is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import GfixParams, GfixResult, check
+
+SENTINEL = 123456789
+GLU_FAILURE = (1 << 64) - 1  # GLU_FAILURE (-1) returned through size_t
+
+
+@dataclass
+class FixResult:
+    links: np.ndarray
+    iters: int
+    theta: float
+    iters_fp32: int = 0
+    gpu_ms: float = 0.0
+    traj_theta: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    traj_func: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    slice_theta: np.ndarray | None = None
+    slice_iters: np.ndarray | None = None
+
+
+def _dims(dims):
+    d = tuple(int(x) for x in dims)
+    if len(d) != 4:
+        raise ValueError("dims must be (Lx, Ly, Lz, Lt)")
+    return (C.c_size_t * 4)(*d), d
+
+
+def _links(links, d):
+    a = np.ascontiguousarray(links, dtype=np.complex128).reshape(-1, 4, 3, 3)
+    if a.shape[0] != int(np.prod(d)):
+        raise ValueError(f"links hold {a.shape[0]} sites, dims {d} need "
+                         f"{int(np.prod(d))}")
+    return a.copy()
+
+
+def _params(alpha, acc, max_iters, algo, sd_fixed, precision, switch, cap):
+    tt = np.zeros(max(cap, 1))
+    tf = np.zeros(max(cap, 1))
+    p = GfixParams()
+    p.gf_alpha = float(alpha)
+    p.accuracy = float(acc)
+    p.max_iters = int(max_iters)
+    p.algo = {"CG": 0, "FACG": 0, "SD": 1, "FASD": 1}[algo]
+    p.sd_fixed_step = int(bool(sd_fixed))
+    p.precision = {"FP64": 0, "MIXED": 1}[precision]
+    p.switch_theta = float(switch)
+    p.traj_theta = tt.ctypes.data_as(C.POINTER(C.c_double)) if cap else None
+    p.traj_func = tf.ctypes.data_as(C.POINTER(C.c_double)) if cap else None
+    p.traj_cap = int(cap)
+    return p, tt, tf
+
+
+def landau_fix(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
+               algo="FACG", sd_fixed_step=False, precision="FP64",
+               switch_theta=1e-9, traj_cap=0) -> FixResult:
+    """Landau FA gauge fixing (GLU's FACG/FASD) of a copy of `links`."""
+    lib = _lib.load()
+    cd, d = _dims(dims)
+    U = _links(links, d)
+    p, tt, tf = _params(gf_alpha, accuracy, max_iters, algo, sd_fixed_step,
+                        precision, switch_theta, traj_cap)
+    r = GfixResult()
+    check(lib.gfix_landau(U.ctypes.data, cd, C.byref(p), C.byref(r)))
+    n = r.traj_len
+    return FixResult(U, int(r.iters), float(r.theta), int(r.iters_fp32),
+                     float(r.gpu_ms), tt[:n].copy(), tf[:n].copy())
+
+
+def coulomb_fix(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
+                algo="FACG", sd_fixed_step=False, precision="FP64",
+                switch_theta=1e-9, traj_cap=0) -> FixResult:
+    """Coulomb FA gauge fixing of all slices (GLU's Coulomb_FA)."""
+    lib = _lib.load()
+    cd, d = _dims(dims)
+    U = _links(links, d)
+    p, tt, tf = _params(gf_alpha, accuracy, max_iters, algo, sd_fixed_step,
+                        precision, switch_theta, traj_cap)
+    r = GfixResult()
+    sth = np.zeros(d[3])
+    sit = np.zeros(d[3], dtype=np.uintp)
+    check(lib.gfix_coulomb(U.ctypes.data, cd, C.byref(p), C.byref(r),
+                           sth.ctypes.data_as(C.POINTER(C.c_double)),
+                           sit.ctypes.data_as(C.POINTER(C.c_size_t))))
+    n = r.traj_len
+    return FixResult(U, int(r.iters), float(r.theta), int(r.iters_fp32),
+                     float(r.gpu_ms), tt[:n].copy(), tf[:n].copy(), sth,
+                     sit.astype(np.int64))
+
+
+# --- GLU-named entry points -------------------------------------------------
+
+def FACG(links, dims, gf_alpha, acc, max_iters, **kw):
+    """src/Gfix/FACG.c:341 -> (links, iters, theta)."""
+    r = landau_fix(links, dims, gf_alpha, acc, max_iters, "FACG", **kw)
+    return r.links, r.iters, r.theta
+
+
+def FASD(links, dims, gf_alpha, acc, max_iters, **kw):
+    """src/Gfix/FACG.c:395 -> (links, iters, theta)."""
+    r = landau_fix(links, dims, gf_alpha, acc, max_iters, "FASD", **kw)
+    return r.links, r.iters, r.theta
+
+
+def Landau(links, dims, gf_alpha, accuracy, max_iters, **kw):
+    """src/Gfix/Landau.c:261 -> (links, iters); iters = GLU_FAILURE when the
+    solve does not converge."""
+    r = landau_fix(links, dims, gf_alpha, accuracy, max_iters, "FACG", **kw)
+    if r.iters == SENTINEL:
+        return r.links, GLU_FAILURE
+    return latt_reunitU(r.links, dims), r.iters
+
+
+def Coulomb_FA(links, dims, gf_alpha, accuracy, max_iters, facg=True, **kw):
+    """src/Gfix/CFACG.c:531 -> (links, iters)."""
+    r = coulomb_fix(links, dims, gf_alpha, accuracy, max_iters,
+                    "FACG" if facg else "FASD", **kw)
+    return r.links, r.iters
+
+
+def Coulomb(links, dims, gf_alpha, accuracy, max_iters, **kw):
+    """src/Gfix/Coulomb.c:32 -> (links, iters), links reunitarised."""
+    U, it = Coulomb_FA(links, dims, gf_alpha, accuracy, max_iters, **kw)
+    return latt_reunitU(U, dims), it
+
+
+def observables(links, dims):
+    lib = _lib.load()
+    cd, d = _dims(dims)
+    U = _links(links, d)
+    out = np.zeros(3)
+    check(lib.gfix_observables(U.ctypes.data, cd,
+                               out.ctypes.data_as(C.POINTER(C.c_double))))
+    return out
+
+
+def theta_test_lin(links, dims):
+    return float(observables(links, dims)[0])
+
+
+def gauge_functional(links, dims):
+    return float(observables(links, dims)[1])
+
+
+def av_plaquette(links, dims):
+    return float(observables(links, dims)[2])
+
+
+def latt_reunitU(links, dims):
+    lib = _lib.load()
+    cd, d = _dims(dims)
+    U = _links(links, d)
+    check(lib.gfix_reunit(U.ctypes.data, cd))
+    return U
+
+
+def fourier_accelerate(fields, dims):
+    """The GPU FOURIER_ACCELERATE3 on 4 packed fields of shape (4, V)."""
+    lib = _lib.load()
+    cd, d = _dims(dims)
+    f = np.ascontiguousarray(fields, dtype=np.complex128).copy()
+    check(lib.gfix_fourier_accelerate(f.ctypes.data, cd, 4))
+    return f
+
+
+def kernel_launches() -> int:
+    return int(_lib.load().gfix_kernel_launches())
+
+
+def release():
+    _lib.load().gfix_release()

@@ -1,0 +1,59 @@
+"""Seeded synthetic inputs with the shapes of the benchmark configurations.
+
+GLU's benchmark inputs are heatbath configurations (beta 6.0, thousands of
+sweeps) that take hours to generate on a CPU.  The stand-in used here keeps
+their local value distribution exactly: the committed 8^4 GLU heatbath
+configuration (beta 6.0, 500 sweeps, tests/golden/hb8.npz) is repeated
+periodically to the requested extents (each a multiple of 8) and a seeded
+random SU(3) gauge transformation is applied, so the solver starts from a
+random point of the gauge orbit as GLU's RANDOM_TRANSFORM option does.
+Plaquette and every gauge-invariant local observable equal those of the
+heatbath configuration.
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+
+GOLDEN = Path(__file__).resolve().parents[1] / "tests" / "golden"
+
+
+def base_config():
+    g = np.load(GOLDEN / "hb8.npz")
+    return g["links"].reshape(-1, 4, 3, 3), tuple(int(x) for x in g["dims"])
+
+
+def random_su3(n: int, rng: np.random.Generator) -> np.ndarray:
+    """n random SU(3) matrices: Gram-Schmidt of two Gaussian columns, third
+    column the conjugate cross product."""
+    z = rng.normal(size=(n, 3, 2)) + 1j * rng.normal(size=(n, 3, 2))
+    c0 = z[:, :, 0] / np.linalg.norm(z[:, :, 0], axis=1, keepdims=True)
+    c1 = z[:, :, 1] - np.sum(np.conj(c0) * z[:, :, 1], axis=1, keepdims=True) * c0
+    c1 /= np.linalg.norm(c1, axis=1, keepdims=True)
+    c2 = np.conj(np.cross(c0, c1))
+    return np.stack([c0, c1, c2], axis=2)
+
+
+def tiled_config(dims, seed: int = 2, transform: bool = True) -> np.ndarray:
+    """Links of shape (V, 4, 3, 3) for dims (Lx, Ly, Lz, Lt)."""
+    base, bd = base_config()
+    Lx, Ly, Lz, Lt = (int(d) for d in dims)
+    if any(L % b for L, b in zip((Lx, Ly, Lz, Lt), bd)):
+        raise ValueError(f"extents {dims} must be multiples of {bd}")
+    b = base.reshape(bd[3], bd[2], bd[1], bd[0], 4, 3, 3)
+    t = np.tile(b, (Lt // bd[3], Lz // bd[2], Ly // bd[1], Lx // bd[0], 1, 1, 1))
+    U = np.ascontiguousarray(t.reshape(-1, 4, 3, 3))
+    if not transform:
+        return U
+    rng = np.random.default_rng(seed)
+    V = U.shape[0]
+    g = random_su3(V, rng).reshape(Lt, Lz, Ly, Lx, 3, 3)
+    gd = np.conj(np.swapaxes(g, -1, -2))
+    Ug = U.reshape(Lt, Lz, Ly, Lx, 4, 3, 3)
+    out = np.empty_like(Ug)
+    axis = {0: 3, 1: 2, 2: 1, 3: 0}
+    for mu in range(4):
+        gfwd = np.roll(gd, -1, axis=axis[mu])
+        out[..., mu, :, :] = np.matmul(np.matmul(g, Ug[..., mu, :, :]), gfwd)
+    return np.ascontiguousarray(out.reshape(-1, 4, 3, 3))

@@ -1,0 +1,172 @@
+/*
+ * glu_gfix.h -- C ABI of the B200 (sm_100a) Fourier-accelerated gauge
+ * fixing library libglu_gfix.so.
+ *
+ * Two layers are exported.
+ *
+ * 1. GLU's own gauge-fixing entry points, with GLU's signatures, so that the
+ *    GLU program links against this library in place of the archive members
+ *    FACG.o, Landau.o, Coulomb.o and CFACG.o.  The structs are GLU's
+ *    (src/Headers/GLU_types.h) for the default build NC = 3, ND = 4, double
+ *    precision, with FFTW: they are only forward-declared here, and the
+ *    library reads them with that layout.  Dimensions and the tuning
+ *    parameter come from GLU's global `Latt` (src/Headers/Mainfile.h:74).
+ *
+ * 2. A flat interface with plain pointers and sizes (gfix_*), which the
+ *    GLU entry points and the Python package glu_b200 both call.
+ *
+ * Link layout of the flat interface: double[V][4][9][2] -- site index
+ * s = x + Lx (y + Ly (z + Lz t)), then mu, then a row-major 3x3 complex
+ * matrix as (re, im) -- GLU's in-memory order of lat[s].O[mu][a*3+b].
+ *
+ * All calls are synchronous: on return the links have been copied back.
+ * A call uses the current CUDA device.  Calls are not re-entrant (GLU's are
+ * not either): the library keeps one cached workspace per lattice shape.
+ */
+#ifndef GLU_B200_GFIX_H
+#define GLU_B200_GFIX_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* GLU types, by reference only (src/Headers/GLU_types.h) */
+struct site;
+struct fftw_stuff;
+
+/* ---------------------------------------------------------------------
+ * GLU entry points
+ * ------------------------------------------------------------------- */
+
+/* Landau gauge fixing by Fourier-accelerated non-linear CG.
+ * Replaces src/Gfix/FACG.c:341-391 (declared src/Headers/FACG.h:37-41).
+ * Returns the iteration count, 123456789 on non-convergence; *th receives
+ * the final in-loop theta.  FFTW may be NULL: plans and p^2 live on the GPU. */
+size_t FACG(struct site *lat, struct fftw_stuff *FFTW, double *th,
+            const double acc, const size_t max_iters);
+
+/* Landau gauge fixing by Fourier-accelerated steepest descent.
+ * Replaces src/Gfix/FACG.c:395-446 (src/Headers/FACG.h:54-58). */
+size_t FASD(struct site *lat, struct fftw_stuff *FFTW, double *th,
+            const double acc, const size_t max_iters);
+
+/* FFT, multiply by FFTW->psq, inverse FFT of the 4 packed fields
+ * FFTW->in[0..3] in place, on the GPU.  Replaces src/Gfix/FACG.c:77-95. */
+void FOURIER_ACCELERATE3(struct fftw_stuff *FFTW);
+
+/* Landau driver: FA solve, up to GF_GLU_FAILURES-1 random restarts,
+ * reunitarisation and the "[GF]" summary.  Replaces
+ * src/Gfix/Landau.c:261-374 (src/Headers/Landau.h:51-54).  Restarts use the
+ * links as they were on entry instead of re-reading `infile`. */
+size_t Landau(struct site *lat, const double accuracy, const size_t iter,
+              const char *infile);
+
+/* Coulomb driver: all time slices solved together, slice transforms of the
+ * links, final reunitarisation.  Replaces src/Gfix/Coulomb.c:32-106
+ * (src/Headers/Coulomb.h:40-42). */
+size_t Coulomb(struct site *lat, const double accuracy, const size_t iter);
+
+/* Coulomb FA solve of every slice plus the slice transforms.  Replaces
+ * src/Gfix/CFACG.c:531-636 (src/Headers/CFACG.h:37-41); FACG is GLU's
+ * GLU_bool (0 = steepest descent, 1 = CG). */
+size_t Coulomb_FA(struct site *lat, struct fftw_stuff *FFTW,
+                  const double accuracy, const size_t max_iter, const int FACG);
+
+/* 3D version of FOURIER_ACCELERATE3 over one slice of Lx*Ly*Lz sites.
+ * Replaces src/Gfix/CFACG.c:69-88. */
+void FOURIER_ACCELERATE2(struct fftw_stuff *FFTW);
+
+/* ---------------------------------------------------------------------
+ * flat interface
+ * ------------------------------------------------------------------- */
+
+enum gfix_algo { GFIX_CG = 0, GFIX_SD = 1 };
+enum gfix_precision { GFIX_FP64 = 0, GFIX_MIXED = 1 };
+
+typedef struct gfix_params {
+  double gf_alpha;       /* GLU's GF_TUNE (Latt.gf_alpha)                  */
+  double accuracy;       /* stop when theta < accuracy (10^-ACCURACY)      */
+  size_t max_iters;      /* GLU's MAX_ITERS                                */
+  int algo;              /* GFIX_CG (FACG) or GFIX_SD (FASD)               */
+  int sd_fixed_step;     /* 1: GLU built with GLU_GFIX_SD (fixed step)     */
+  int precision;         /* GFIX_FP64 or GFIX_MIXED                        */
+  double switch_theta;   /* MIXED: FP32 until theta < switch_theta         */
+  double *traj_theta;    /* optional host arrays, one entry per derivative */
+  double *traj_func;     /*   evaluation (theta, gauge functional)         */
+  size_t traj_cap;
+} gfix_params;
+
+typedef struct gfix_result {
+  size_t iters;          /* GLU's return value (123456789 if failed)       */
+  size_t iters_fp32;     /* MIXED: iterations spent in FP32                */
+  double theta;          /* final in-loop theta                            */
+  size_t traj_len;
+  double gpu_ms;         /* device time of the solve (CUDA events)         */
+  int restarts;
+} gfix_result;
+
+/* Landau FA gauge fixing of host links (double[V][4][9][2]) in place.
+ * dims = {Lx, Ly, Lz, Lt}.  Returns 0, or a negative error code (see
+ * gfix_last_error). */
+int gfix_landau(double *links, const size_t dims[4], const gfix_params *p,
+                gfix_result *r);
+
+/* As gfix_landau, but `d_links` is a device pointer to the same layout
+ * (links already resident in HBM); nothing crosses PCIe but scalars. */
+int gfix_landau_device(double *d_links, const size_t dims[4],
+                       const gfix_params *p, gfix_result *r);
+
+/* Coulomb FA gauge fixing of host links in place: every time slice solved
+ * as an independent 3D problem in one batched launch sequence, then the
+ * slice transforms (no final reunitarisation; gfix_reunit does that).
+ * slice_theta / slice_iters (length Lt, may be NULL) receive per-slice
+ * results; traj_theta records the accelerated theta of every slice at every
+ * FFT round, slice-major with stride traj_cap / Lt. */
+int gfix_coulomb(double *links, const size_t dims[4], const gfix_params *p,
+                 gfix_result *r, double *slice_theta, size_t *slice_iters);
+
+int gfix_coulomb_device(double *d_links, const size_t dims[4],
+                        const gfix_params *p, gfix_result *r,
+                        double *slice_theta, size_t *slice_iters);
+
+/* Observables on host links: theta_test_lin (src/Gfix/gftests.c:214-250),
+ * gauge functional (gftests.c:132-147), average plaquette
+ * (src/Field/plaqs_links.c:243-265).  out[0..2] in that order. */
+int gfix_observables(const double *links, const size_t dims[4], double *out);
+
+/* Reunitarise every link (GLU's latt_reunitU, src/Geometry/random_config.c:
+ * 42-57) on the GPU, host links in place. */
+int gfix_reunit(double *links, const size_t dims[4]);
+
+/* In place: fields (4 packed fields of vol complex numbers each, double[4]
+ * [vol][2]) <- IDFT(psq * DFT(fields)) over ndim = 4 (dims[0..3]) or 3
+ * (one slice, dims[0..2]); psq = MAX / p^2 as GLU builds it. */
+int gfix_fourier_accelerate(double *fields, const size_t dims[4], int ndim);
+
+/* Measurement aid: run `iters` Landau CG iterations from the device links
+ * `d_links` (not modified) with CUDA events between the kernel launches.
+ * ms[k] = mean duration of one launch of kernel k, bytes[k] = algorithmic
+ * HBM bytes of one launch, for k = 0 derivative+theta, 1 xy FFT forward,
+ * 2 zt FFT with psq, 3 xy FFT inverse + PR sums, 4 direction + line-search
+ * probes, 5 link update, 6 the scalar-control launches of one iteration.
+ * precision GFIX_MIXED profiles the FP32 kernels. */
+int gfix_profile_landau(const double *d_links, const size_t dims[4],
+                        const gfix_params *p, int iters, double *ms,
+                        double *bytes);
+
+/* message of the last failed call (thread-local, never NULL) */
+const char *gfix_last_error(void);
+
+/* free the cached device workspaces */
+void gfix_release(void);
+
+/* number of kernels launched by this library since load (all devices) */
+unsigned long long gfix_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GLU_B200_GFIX_H */

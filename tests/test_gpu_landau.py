@@ -1,0 +1,162 @@
+"""Landau FA gauge fixing on the GPU against the oracle and the reference.
+
+All calls go through the C ABI (libglu_gfix.so via ctypes)."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from glu_b200 import gfix  # noqa: E402
+
+
+def _rel(a, b):
+    return np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+
+
+def _dims(g):
+    return tuple(int(d) for d in g["dims"])
+
+
+def _envelope_prefix(g, tol=1e-10):
+    env = _rel(g["landau_facg_env8"],
+               g["landau_facg_traj_theta"][1:1 + len(g["landau_facg_env8"])])
+    bad = np.nonzero(env > tol)[0]
+    return int(bad[0]) + 1 if len(bad) else len(env) + 1
+
+
+@pytest.mark.parametrize("case", ["lat400", "hb8"])
+def test_observables_match_oracle(oracle, case, request):
+    g = request.getfixturevalue(case)
+    d = _dims(g)
+    th, fn, pl = gfix.observables(g["links"], d)
+    assert abs(th - oracle.theta_test_lin(g["links"], d)) < 1e-12 * th
+    assert abs(fn - g["functional"]) < 1e-14
+    assert abs(pl - g["plaquette"]) < 1e-13
+
+
+@pytest.mark.parametrize("dims", [(4, 4, 4, 8), (8, 6, 4, 12), (6, 10, 5, 3)])
+def test_fourier_accelerate_matches_oracle(oracle, dims):
+    rng = np.random.default_rng(7)
+    V = int(np.prod(dims))
+    f = rng.normal(size=(4, V)) + 1j * rng.normal(size=(4, V))
+    got = gfix.fourier_accelerate(f, dims)
+    ref = oracle.fourier_accelerate(f, dims, 4)
+    assert np.abs(got - ref).max() < 1e-13 * np.abs(ref).max()
+
+
+def test_reunit_matches_oracle(oracle, lat400):
+    g = lat400
+    rng = np.random.default_rng(1)
+    U = g["links"] + 1e-3 * (rng.normal(size=g["links"].shape)
+                             + 1j * rng.normal(size=g["links"].shape))
+    got = gfix.latt_reunitU(U, _dims(g))
+    ref = oracle.reunit(U)
+    assert np.abs(got - ref).max() < 1e-14
+
+
+@pytest.mark.parametrize("case", ["lat400", "hb8"])
+def test_landau_facg_matches_reference(case, request):
+    g = request.getfixturevalue(case)
+    d = _dims(g)
+    r = gfix.landau_fix(g["links"], d, 0.08, 1e-14, 650, "FACG", traj_cap=5000)
+    ref = g["landau_facg_traj_theta"]
+    n = _envelope_prefix(g)
+    # theta to 1e-10 relative wherever the reference reproduces itself to
+    # 1e-10 across OpenMP thread counts
+    assert _rel(r.traj_theta[:n], ref[:n]).max() < 1e-10
+    assert np.abs(r.traj_func[:n] - g["landau_facg_traj_func"][:n]).max() < 1e-13
+    # beyond it, within 100x the reference's own spread
+    m = min(len(g["landau_facg_env8"]), len(r.traj_theta) - 1, len(ref) - 1)
+    env = np.abs(g["landau_facg_env8"][:m] - ref[1:1 + m])
+    assert np.all(np.abs(r.traj_theta[1:1 + m] - ref[1:1 + m])
+                  <= 100 * env + 1e-10 * ref[1:1 + m])
+    assert abs(r.iters - int(g["landau_facg_iters"])) <= 3
+    assert r.theta < 1e-14
+    # gauge invariance: plaquette unchanged
+    assert abs(gfix.av_plaquette(r.links, d) - g["plaquette"]) < 1e-13
+
+
+def test_landau_fasd_fixed_step_matches_reference(lat400):
+    """GLU_GFIX_SD semantics: no line search, the whole run agrees."""
+    g = lat400
+    d = _dims(g)
+    r = gfix.landau_fix(g["links"], d, 0.08, 1e-14, 650, "FASD",
+                        sd_fixed_step=True, traj_cap=5000)
+    ref = g["landau_fasd_sd_traj_theta"]
+    assert r.iters == int(g["landau_fasd_sd_iters"])
+    assert _rel(r.traj_theta[: len(ref)], ref).max() < 1e-9
+    # links at the same iteration count
+    assert np.abs(r.links - g["landau_fasd_sd_links"]).max() < 1e-12
+
+
+def test_landau_fasd_line_search_matches_reference(lat400):
+    g = lat400
+    d = _dims(g)
+    r = gfix.landau_fix(g["links"], d, 0.08, 1e-14, 650, "FASD", traj_cap=5000)
+    ref = g["landau_fasd_ls_traj_theta"]
+    assert _rel(r.traj_theta[:20], ref[:20]).max() < 1e-10
+    assert abs(r.iters - int(g["landau_fasd_ls_iters"])) <= 10
+    assert r.theta < 1e-14
+
+
+def test_landau_matches_oracle_step_by_step(oracle, lat400):
+    """Iteration-count-matched links against the oracle for a short run
+    (acc 1e-30 never converges; both stop after exactly k iterations)."""
+    g = lat400
+    d = _dims(g)
+    for k in (1, 2, 5):
+        r = gfix.landau_fix(g["links"], d, 0.08, 1e-30, k, "FACG")
+        o = oracle.landau(g["links"], d, 0.08, 1e-30, k, "FACG")
+        assert r.iters == o["iters"] == gfix.SENTINEL
+        assert abs(r.theta - o["theta"]) < 1e-12 * o["theta"]
+        assert np.abs(r.links - o["links"]).max() < 1e-13
+
+
+def test_mixed_precision_reaches_fp64_accuracy(hb8):
+    g = hb8
+    d = _dims(g)
+    r = gfix.landau_fix(g["links"], d, 0.08, 1e-14, 2000, "FACG",
+                        precision="MIXED", switch_theta=1e-9)
+    assert r.iters != gfix.SENTINEL
+    assert r.theta < 1e-14
+    assert r.iters_fp32 > 0
+    # the links stay on the gauge orbit of the input to FP64 accuracy
+    assert abs(gfix.av_plaquette(r.links, d) - g["plaquette"]) < 1e-13
+    th, fn, _ = gfix.observables(r.links, d)
+    assert th < 1e-13
+    # same Landau-gauge functional as the FP64 solve (same Gribov region)
+    r64 = gfix.landau_fix(g["links"], d, 0.08, 1e-14, 2000, "FACG")
+    assert abs(fn - gfix.gauge_functional(r64.links, d)) < 1e-8
+
+
+def test_nonconvergence_sentinel(lat400):
+    g = lat400
+    r = gfix.landau_fix(g["links"], _dims(g), 0.08, 1e-14, 4, "FACG")
+    assert r.iters == gfix.SENTINEL
+
+
+def test_already_fixed_returns_zero(lat400):
+    g = lat400
+    d = _dims(g)
+    fixed = g["landau_facg_links"]
+    r = gfix.landau_fix(fixed, d, 0.08, 1e-10, 100, "FACG")
+    assert r.iters == 0
+
+
+def test_random_odd_lattice_against_oracle(oracle):
+    """Extents with radix-3 and radix-5 factors and an odd extent."""
+    from glu_b200.workload import random_su3
+    d = (6, 5, 4, 3)
+    V = int(np.prod(d))
+    rng = np.random.default_rng(11)
+    U = random_su3(V * 4, rng).reshape(V, 4, 3, 3)
+    # a smooth-ish config: mix with the identity and reunitarise
+    U = oracle.reunit(np.eye(3) + 0.3 * U)
+    r = gfix.landau_fix(U, d, 0.08, 1e-30, 3, "FACG", traj_cap=10)
+    o = oracle.landau(U, d, 0.08, 1e-30, 3, "FACG", traj_cap=10)
+    assert _rel(r.traj_theta, o["traj_theta"]).max() < 1e-11
+    assert np.abs(r.links - o["links"]).max() < 1e-12
