@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--profile-iters", type=int, default=20)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="only the per-kernel event timing of --profile-iters "
+                         "CG iterations (a short, bounded launch list for ncu)")
     return ap.parse_args()
 
 
@@ -408,10 +411,35 @@ def gpu_line(args, dims, world, res, cpu):
     return line
 
 
+def profile_only(args, dims):
+    import ctypes as C
+    import torch
+    from glu_b200 import _lib
+    from glu_b200._lib import check
+    lib = _lib.load()
+    U = workload(dims, 0)
+    d = torch.from_numpy(U.view(np.float64).reshape(-1)).to("cuda")
+    cd = (C.c_size_t * 4)(*dims)
+    ms = np.zeros(7)
+    by = np.zeros(7)
+    check(lib.gfix_profile_landau(d.data_ptr(), cd, C.byref(_params(args.precision)),
+                                  args.profile_iters,
+                                  ms.ctypes.data_as(C.POINTER(C.c_double)),
+                                  by.ctypes.data_as(C.POINTER(C.c_double))))
+    tag = "fp32" if args.precision == "mixed" else "fp64"
+    emit({"profile": tag, "dims": list(dims), "iters": args.profile_iters,
+          "kernels": {f"{KERNELS[k]}:{tag}": {"ms": ms[k], "bytes": by[k],
+                                              "GB/s": by[k] / (ms[k] * 1e-3) / 1e9 if ms[k] else None}
+                      for k in range(7)}})
+
+
 def main():
     args = parse()
     dims = tuple(int(x) for x in args.dims.split(","))
     rank, world, local = dist_env()
+    if args.profile_only:
+        profile_only(args, dims)
+        return
     if args.impl == "reference":
         reference_arm(args, dims, rank, world)
         return

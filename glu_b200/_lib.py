@@ -6,6 +6,7 @@ every entry point raises.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 from .build import LIB
@@ -48,7 +49,10 @@ def load(path: Path | str | None = None):
     global _lib
     if _lib is not None:
         return _lib
-    p = Path(path) if path else LIB
+    # GLU_GFIX_LIB selects another build of the same library (e.g. a
+    # variant under comparison); the default is the in-tree build
+    env = os.environ.get("GLU_GFIX_LIB")
+    p = Path(path) if path else (Path(env) if env else LIB)
     if not p.exists():
         raise GfixError(f"{p} is not built: run `python -m glu_b200.build`")
     lib = C.CDLL(str(p))

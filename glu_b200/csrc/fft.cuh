@@ -3,9 +3,10 @@
 // src/Gfix/FACG.c:77-95 and src/Gfix/CFACG.c:69-88, where FFTW transforms
 // each packed field, multiplies by psq and transforms back).
 //
-// Algorithm: Stockham auto-sort, one radix-R butterfly per thread and stage,
-// ping-pong between two shared-memory tiles.  Radices 8, 4, 2, 3, 5 have
-// register kernels; any other prime factor uses a direct DFT.  Twiddles come
+// Algorithm: Stockham auto-sort in place: per stage each thread loads its
+// radix-R butterflies into registers, the block synchronises, and the
+// outputs overwrite the tile.  Radices 8, 4 and 2 have dedicated register
+// kernels; 3, 5 and 7 use a direct DFT.  Twiddles come
 // from a table tw[k] = exp(-2 pi i k / N) computed on the host in FP64;
 // the backward (+i) direction conjugates them.  Like FFTW, neither direction
 // normalises.
@@ -16,23 +17,55 @@
 namespace gfix {
 
 constexpr int kMaxStages = 12;
-constexpr int kMaxRadix = 16;
+constexpr int kMaxRadix = 7;   // largest prime factor of an extent
+
+// one Stockham stage: radix r, nb = N / r butterflies per pencil, Ns the
+// product of the earlier radices, step0 = N / (Ns r); *_sh = log2 of nb or
+// Ns when it is a power of two (else -1), so that the index arithmetic of
+// the common power-of-two sizes needs no integer division
+struct FftStage {
+  int r, nb, Ns, step0, nb_sh, ns_sh;
+};
 
 struct FftAxis {
   int n;
   int nstages;
-  int radix[kMaxStages];
   int tw_off;  // offset of this length's table inside the twiddle pool
+  FftStage st[kMaxStages];
 };
 
 // pencil p, element j -> tile offset (p / pin) * ps_hi + (p % pin) * ps_lo
 // + j * js
 struct PencilMap {
-  int npencil, pin, ps_lo, ps_hi, js;
+  int npencil, pin, pin_sh, ps_lo, ps_hi, js;
 };
 
+__host__ __device__ __forceinline__ int log2_if_pow2(int v) {
+  if (v <= 0 || (v & (v - 1))) return -1;
+  int k = 0;
+  while ((1 << k) < v) k++;
+  return k;
+}
+
+__device__ __forceinline__ int fdiv(int x, int d, int sh) {
+  return sh >= 0 ? (x >> sh) : x / d;
+}
+
+__device__ __forceinline__ PencilMap pmap(int npencil, int pin, int ps_lo,
+                                          int ps_hi, int js) {
+  PencilMap m;
+  m.npencil = npencil;
+  m.pin = pin;
+  m.pin_sh = log2_if_pow2(pin);
+  m.ps_lo = ps_lo;
+  m.ps_hi = ps_hi;
+  m.js = js;
+  return m;
+}
+
 __device__ __forceinline__ int pencil_off(const PencilMap &m, int p) {
-  return (p / m.pin) * m.ps_hi + (p % m.pin) * m.ps_lo;
+  const int q = fdiv(p, m.pin, m.pin_sh);
+  return q * m.ps_hi + (p - q * m.pin) * m.ps_lo;
 }
 
 template <typename R>
@@ -42,15 +75,15 @@ __device__ __forceinline__ cx<R> twiddle(const cx<R> *tw, int k, bool bwd) {
   return w;
 }
 
-// in-register DFT of size r: v[q] <- sum_s v[s] W_r^{sq}, W_r = tw[N/r]
-template <typename R>
-__device__ __forceinline__ void dft_reg(cx<R> *v, int r, const cx<R> *tw,
-                                        int N, bool bwd) {
-  if (r == 2) {
+// in-register DFT of size RDX: v[q] <- sum_s v[s] W^{sq}, W = tw[N/RDX]
+template <typename R, int RDX>
+__device__ __forceinline__ void dft_reg(cx<R> *v, const cx<R> *tw, int N,
+                                        bool bwd) {
+  if constexpr (RDX == 2) {
     cx<R> a = v[0], b = v[1];
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
-  } else if (r == 4) {
+  } else if constexpr (RDX == 4) {
     const cx<R> w = twiddle(tw, N / 4, bwd);
     cx<R> a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
     cx<R> b0 = cadd(v[1], v[3]), b1 = cmul(csub(v[1], v[3]), w);
@@ -58,7 +91,7 @@ __device__ __forceinline__ void dft_reg(cx<R> *v, int r, const cx<R> *tw,
     v[1] = cadd(a1, b1);
     v[2] = csub(a0, b0);
     v[3] = csub(a1, b1);
-  } else if (r == 8) {
+  } else if constexpr (RDX == 8) {
     const cx<R> w4 = twiddle(tw, N / 4, bwd);
     cx<R> e[4], o[4];
 #pragma unroll
@@ -86,76 +119,91 @@ __device__ __forceinline__ void dft_reg(cx<R> *v, int r, const cx<R> *tw,
       v[q + 4] = csub(e[q], t);
     }
   } else {
-    // direct DFT for 3, 5 and any other prime
-    cx<R> out[kMaxRadix];
-    const int sr = N / r;
-    for (int q = 0; q < r; q++) {
+    // direct DFT for 3, 5, 7
+    cx<R> out[RDX];
+    const int sr = N / RDX;
+#pragma unroll
+    for (int q = 0; q < RDX; q++) {
       cx<R> acc = v[0];
-      for (int s = 1; s < r; s++)
-        acc = cadd(acc, cmul(v[s], twiddle(tw, ((s * q) % r) * sr, bwd)));
+#pragma unroll
+      for (int s = 1; s < RDX; s++)
+        acc = cadd(acc, cmul(v[s], twiddle(tw, ((s * q) % RDX) * sr, bwd)));
       out[q] = acc;
     }
-    for (int q = 0; q < r; q++) v[q] = out[q];
+#pragma unroll
+    for (int q = 0; q < RDX; q++) v[q] = out[q];
   }
 }
 
-// One Stockham stage of compile-time radix RDX (0 = runtime radix r with
-// the generic direct DFT) over every pencil of the tile.
-template <typename R, int RDX>
-__device__ __forceinline__ void stockham_stage(const cx<R> *src, cx<R> *dst,
-                                               const PencilMap &m, int N,
-                                               int r_rt, int Ns,
+// Elements one thread holds per stage (PT): a tile of n elements is handled
+// by at least n / PT threads.  8 in FP64 and 16 in FP32 keep the butterflies
+// in registers; 16 in FP64 serves tiles too large for 512 threads.
+
+// One in-place Stockham stage of radix RDX over every pencil of the tile:
+// each thread reads its butterflies into registers, the block synchronises,
+// and the results overwrite the same tile.
+template <typename R, int PT, int RDX>
+__device__ __forceinline__ void stockham_stage(cx<R> *buf, const PencilMap &m,
+                                               const FftStage S, int N,
                                                const cx<R> *tw, bool bwd) {
-  constexpr int RMAX = RDX ? RDX : kMaxRadix;
-  const int r = RDX ? RDX : r_rt;
-  const int nb = N / r;
+  constexpr int K = (PT + RDX - 1) / RDX;
+  const int nb = S.nb, Ns = S.Ns;
   const int total = m.npencil * nb;
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int p = idx / nb, j = idx - p * nb;
-    const int po = pencil_off(m, p);
-    const int jm = j % Ns;
-    const int step = jm * (N / (Ns * r));
-    cx<R> v[RMAX];
+  cx<R> v[K][RDX];
+  int dst[K];
 #pragma unroll
-    for (int s = 0; s < RMAX; s++) {
-      if (RDX == 0 && s >= r) break;
-      v[s] = src[po + (j + s * nb) * m.js];
-      if (s > 0 && step) v[s] = cmul(v[s], twiddle(tw, s * step, bwd));
-    }
-    dft_reg(v, r, tw, N, bwd);
-    const int base = (j / Ns) * Ns * r + jm;
+  for (int k = 0; k < K; k++) {
+    const int idx = threadIdx.x + k * blockDim.x;
+    dst[k] = -1;
+    if (idx < total) {
+      const int p = fdiv(idx, nb, S.nb_sh), j = idx - p * nb;
+      const int po = pencil_off(m, p);
+      const int jq = fdiv(j, Ns, S.ns_sh), jm = j - jq * Ns;
+      const int step = jm * S.step0;
 #pragma unroll
-    for (int s = 0; s < RMAX; s++) {
-      if (RDX == 0 && s >= r) break;
-      dst[po + (base + s * Ns) * m.js] = v[s];
+      for (int s = 0; s < RDX; s++) {
+        v[k][s] = buf[po + (j + s * nb) * m.js];
+        if (s > 0 && step) v[k][s] = cmul(v[k][s], twiddle(tw, s * step, bwd));
+      }
+      dft_reg<R, RDX>(v[k], tw, N, bwd);
+      dst[k] = po + (jq * Ns * RDX + jm) * m.js;
     }
   }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    if (dst[k] >= 0) {
+#pragma unroll
+      for (int s = 0; s < RDX; s++) buf[dst[k] + s * Ns * m.js] = v[k][s];
+    }
+  }
+  __syncthreads();
 }
 
-// Full transform of every pencil of a tile; returns the buffer that holds
-// the result (a or b).  All threads of the block must call it.
-template <typename R>
-__device__ cx<R> *smem_fft(cx<R> *a, cx<R> *b, const PencilMap &m,
-                           const FftAxis &ax, const cx<R> *tw, bool bwd) {
+// Full in-place transform of every pencil of a tile.  Radices 2, 3, 4, 5,
+// 7, 8 (the host rejects extents with other prime factors).  All threads of
+// the block must call it, with blockDim.x * PT >= tile elements.
+// ODD adds the radix-5 and radix-7 stages (direct DFTs, more registers).
+// `ax` should live in shared memory: its stage table is indexed at run time.
+template <typename R, int PT, bool ODD>
+__device__ void smem_fft(cx<R> *buf, const PencilMap &m, const FftAxis &ax,
+                         const cx<R> *tw, bool bwd) {
   const int N = ax.n;
-  int Ns = 1;
-  cx<R> *src = a, *dst = b;
   for (int st = 0; st < ax.nstages; st++) {
-    const int r = ax.radix[st];
-    switch (r) {
-      case 8: stockham_stage<R, 8>(src, dst, m, N, r, Ns, tw, bwd); break;
-      case 4: stockham_stage<R, 4>(src, dst, m, N, r, Ns, tw, bwd); break;
-      case 2: stockham_stage<R, 2>(src, dst, m, N, r, Ns, tw, bwd); break;
-      case 3: stockham_stage<R, 3>(src, dst, m, N, r, Ns, tw, bwd); break;
-      default: stockham_stage<R, 0>(src, dst, m, N, r, Ns, tw, bwd); break;
+    const FftStage S = ax.st[st];
+    switch (S.r) {
+      case 8: stockham_stage<R, PT, 8>(buf, m, S, N, tw, bwd); break;
+      case 4: stockham_stage<R, PT, 4>(buf, m, S, N, tw, bwd); break;
+      case 2: stockham_stage<R, PT, 2>(buf, m, S, N, tw, bwd); break;
+      case 3: stockham_stage<R, PT, 3>(buf, m, S, N, tw, bwd); break;
+      default:
+        if constexpr (ODD) {
+          if (S.r == 5) stockham_stage<R, PT, 5>(buf, m, S, N, tw, bwd);
+          if (S.r == 7) stockham_stage<R, PT, 7>(buf, m, S, N, tw, bwd);
+        }
+        break;
     }
-    __syncthreads();
-    cx<R> *t = src;
-    src = dst;
-    dst = t;
-    Ns *= r;
   }
-  return src;
 }
 
 }  // namespace gfix

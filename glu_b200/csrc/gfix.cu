@@ -52,25 +52,34 @@ static int fail(const char *fmt, ...) {
 
 constexpr size_t kSentinel = 123456789;
 
-// radices 8,4,2,3,5 then any prime <= kMaxRadix
+// radices 8, 4, 2, 3, 5, 7 and the Stockham stage table of length n
 static int factorize(int n, FftAxis &ax) {
   ax.n = n;
   ax.nstages = 0;
   int m = n;
-  const int pref[5] = {8, 4, 2, 3, 5};
+  int rad[kMaxStages];
+  int ns = 0;
+  const int pref[6] = {8, 4, 2, 3, 5, 7};
   for (int r : pref)
     while (m % r == 0 && m > 1) {
-      if (ax.nstages == kMaxStages) return -1;
-      ax.radix[ax.nstages++] = r;
+      if (ns == kMaxStages) return -1;
+      rad[ns++] = r;
       m /= r;
     }
-  for (int p = 7; m > 1; p += 2)
-    while (m % p == 0) {
-      if (p > kMaxRadix || ax.nstages == kMaxStages) return -1;
-      ax.radix[ax.nstages++] = p;
-      m /= p;
-    }
-  if (ax.nstages == 0) ax.radix[ax.nstages++] = 1;
+  if (m > 1) return -1;  // a prime factor above kMaxRadix
+  if (ns == 0) rad[ns++] = 1;
+  int Ns = 1;
+  for (int k = 0; k < ns; k++) {
+    FftStage &S = ax.st[k];
+    S.r = rad[k];
+    S.nb = n / rad[k];
+    S.Ns = Ns;
+    S.step0 = n / (Ns * rad[k]);
+    S.nb_sh = log2_if_pow2(S.nb);
+    S.ns_sh = log2_if_pow2(Ns);
+    Ns *= rad[k];
+  }
+  ax.nstages = ns;
   return 0;
 }
 
@@ -97,8 +106,12 @@ class Engine {
   int nb_site = 0;
   dim3 g_xy, g_zt;
   size_t sm_xy = 0, sm_zt = 0;
+  int bd_xy = 256, bd_zt = 256, pt_xy = 8, pt_zt = 8;
+  bool odd = false;
   cudaGraphExec_t gx_cg = nullptr, gx_sd = nullptr;
   int gx_sd_fixed = -1;
+  bool primed = false;
+  bool graph_ok = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
   ~Engine() { release(); }
@@ -171,28 +184,43 @@ class Engine {
     c.cs_ld = ld;
     // tiles
     c.xy_pitch = c.L[0] + 1;
-    const int want_b = (sizeof(R) == 8) ? 2 : 4;
+    const int want_b = 2;
     c.zt_b = 1;
     for (int b = want_b; b >= 1; b--)
       if (c.L[0] % b == 0) {
         c.zt_b = b;
         break;
       }
-    sm_xy = 2 * (size_t)c.xy_pitch * c.L[1] * sizeof(cx<R>);
-    sm_zt = 2 * (size_t)c.zt_b * c.L[2] * c.L[3] * sizeof(cx<R>);
-    while (sm_zt > 200 * 1024 && c.zt_b > 1) {
-      c.zt_b = 1;
-      sm_zt = 2 * (size_t)c.L[2] * c.L[3] * sizeof(cx<R>);
-    }
-    if (sm_xy > 200 * 1024 || sm_zt > 200 * 1024)
-      return fail("FFT tile does not fit shared memory (xy %zu B, zt %zu B)",
-                  sm_xy, sm_zt);
-    CK(cudaFuncSetAttribute(k_fft_xy<R>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)sm_xy));
-    CK(cudaFuncSetAttribute(k_fft_zt<R>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)sm_zt));
+    // tiles are transformed in place, one element per thread and stage for
+    // kPerThread elements: at most 512 threads, so tiles up to 8192
+    constexpr int pt_small = 8;
+    auto threads_for = [](size_t n, int pt) {
+      size_t t = (n + pt - 1) / pt;
+      t = std::max<size_t>(128, (t + 31) / 32 * 32);
+      return t;
+    };
+    while (c.zt_b > 1 && (size_t)c.zt_b * c.L[2] * c.L[3] > 512u * pt_small)
+      c.zt_b /= 2;
+    while (c.zt_b > 1 && c.L[0] % c.zt_b) c.zt_b /= 2;
+    const size_t n_xy = (size_t)c.L[0] * c.L[1];
+    const size_t n_zt = (size_t)c.zt_b * c.L[2] * c.L[3];
+    if (n_xy > 8192 || n_zt > 8192)
+      return fail("FFT tile of %zu / %zu elements exceeds 8192", n_xy, n_zt);
+    odd = false;
+    for (int a = 0; a < 4; a++)
+      for (int k = 0; k < c.ax[a].nstages; k++)
+        odd |= (c.ax[a].st[k].r == 5 || c.ax[a].st[k].r == 7);
+    pt_xy = (n_xy <= 512u * pt_small && !odd) ? pt_small : 16;
+    pt_zt = (n_zt <= 512u * pt_small && !odd) ? pt_small : 16;
+    bd_xy = (int)threads_for(n_xy, pt_xy);
+    bd_zt = (int)threads_for(n_zt, pt_zt);
+    // tile (padded) plus the twiddle tables of its two axes
+    sm_xy = ((size_t)c.xy_pitch * c.L[1] + c.L[0] + c.L[1]) * sizeof(cx<R>);
+    sm_zt = ((size_t)(c.zt_b * c.L[2] + 1) * c.L[3] + c.L[2] + c.L[3]) *
+            sizeof(cx<R>);
+    // the dynamic shared-memory limit is an attribute of the function, not
+    // of a launch: raise it once to the largest tile any engine can use
+    if (set_smem_limits()) return -1;
     g_xy = dim3(V / (c.L[0] * c.L[1]), 4);
     g_zt = dim3((c.L[0] / c.zt_b) * c.L[1], 4);
     nb_site = (V + kSiteThreads - 1) / kSiteThreads;
@@ -237,11 +265,47 @@ class Engine {
     LAUNCHED(1);
     scalar(op, 2);
   }
+  static int set_smem_limits() {
+    static bool done = false;
+    if (done) return 0;
+    const int lim = (8192 + 8192 / 8 + 1024) * (int)sizeof(cx<R>);
+    CK(cudaFuncSetAttribute(k_fft_xy<R, 8, false>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    CK(cudaFuncSetAttribute(k_fft_xy<R, 16, false>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    CK(cudaFuncSetAttribute(k_fft_xy<R, 16, true>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    CK(cudaFuncSetAttribute(k_fft_zt<R, 8, false>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    CK(cudaFuncSetAttribute(k_fft_zt<R, 16, false>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    CK(cudaFuncSetAttribute(k_fft_zt<R, 16, true>,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    done = true;
+    return 0;
+  }
+  void fft_xy(int bwd, int prsum) {
+    if (odd)
+      k_fft_xy<R, 16, true><<<g_xy, bd_xy, sm_xy, s>>>(c, bwd, prsum);
+    else if (pt_xy == 8)
+      k_fft_xy<R, 8, false><<<g_xy, bd_xy, sm_xy, s>>>(c, bwd, prsum);
+    else
+      k_fft_xy<R, 16, false><<<g_xy, bd_xy, sm_xy, s>>>(c, bwd, prsum);
+    LAUNCHED(1);
+  }
+  void fft_zt() {
+    if (odd)
+      k_fft_zt<R, 16, true><<<g_zt, bd_zt, sm_zt, s>>>(c);
+    else if (pt_zt == 8)
+      k_fft_zt<R, 8, false><<<g_zt, bd_zt, sm_zt, s>>>(c);
+    else
+      k_fft_zt<R, 16, false><<<g_zt, bd_zt, sm_zt, s>>>(c);
+    LAUNCHED(1);
+  }
   void fft(bool prsum) {
-    k_fft_xy<R><<<g_xy, 256, sm_xy, s>>>(c, 0, 0);
-    k_fft_zt<R><<<g_zt, 256, sm_zt, s>>>(c);
-    k_fft_xy<R><<<g_xy, 256, sm_xy, s>>>(c, 1, prsum ? 1 : 0);
-    LAUNCHED(3);
+    fft_xy(0, 0);
+    fft_zt();
+    fft_xy(1, prsum ? 1 : 0);
   }
   // an SD step (steep_Landau_FA, src/Gfix/FACG.c:181-199); main = one FASD
   // iteration with its stop test
@@ -272,9 +336,28 @@ class Engine {
     scalar(OP_END_CG, 0);
   }
 
+  // Launch every kernel of the iteration once with the done flag set: each
+  // returns at once, but the module loading that CUDA defers to a kernel's
+  // first launch happens here and not inside a stream capture.
+  int prime() {
+    if (primed) return 0;
+    k_set_done<<<1, 1, 0, s>>>(d_st, 1);
+    cg_iter();
+    sd_step(true, false);
+    sd_step(true, true);
+    k_copy_der<R><<<nb_site, kSiteThreads, 0, s>>>(c);
+    k_set_done<<<1, 1, 0, s>>>(d_st, 0);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    primed = true;
+    return 0;
+  }
+
   int capture(cudaGraphExec_t *out, bool cg, bool sd_fixed) {
+    if (prime()) return -1;
     cudaGraph_t g;
-    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    CK(cudaGetLastError());
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
     const unsigned long long before = g_launches.load();
     if (cg)
       cg_iter();
@@ -301,21 +384,49 @@ class Engine {
     return 0;
   }
 
-  // replay an iteration graph until the device says done
-  int replay(cudaGraphExec_t gx, unsigned long long per_iter) {
+  // replay an iteration (graph, or direct launches when the graph could
+  // not be built) until the device says done
+  int replay(cudaGraphExec_t gx, bool cg, bool sd_fixed) {
+    const unsigned long long per_iter = per_iter_launches(cg, sd_fixed);
     int batch = 2;
     size_t guard = 0;
     for (;;) {
       for (int k = 0; k < batch; k++) {
-        CK(cudaGraphLaunch(gx, s));
-        LAUNCHED(per_iter);
+        if (gx) {
+          CK(cudaGraphLaunch(gx, s));
+          LAUNCHED(per_iter);
+        } else if (cg) {
+          cg_iter();
+        } else {
+          sd_step(true, sd_fixed);
+        }
       }
+      CK(cudaGetLastError());
       if (read_state()) return -1;
       if (h_st->done) return 0;
       guard += batch;
       if (guard > (size_t)h_st->max_iters + 64)
         return fail("solver did not stop after %zu iterations", guard);
       batch = std::min(batch * 2, 32);
+    }
+  }
+
+  // build the iteration graph; on failure run without one (graph_ok = 0)
+  void ensure_graph(cudaGraphExec_t *gx, bool cg, bool sd_fixed) {
+    if (*gx || !graph_ok) return;
+    if (capture(gx, cg, sd_fixed)) {
+      cudaStreamCaptureStatus st;
+      if (cudaStreamIsCapturing(s, &st) == cudaSuccess &&
+          st != cudaStreamCaptureStatusNone) {
+        cudaGraph_t g;
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+      }
+      cudaGetLastError();
+      *gx = nullptr;
+      graph_ok = false;
+      fprintf(stderr, "[GF] CUDA graph capture failed (%s); launching the "
+              "iteration kernels directly\n", g_err.c_str());
     }
   }
 
@@ -328,6 +439,7 @@ class Engine {
     st.acc = p.acc;
     st.max_iters = (long long)p.max_iters;
     st.sd_fixed = p.sd_fixed;
+    st.cg_tol = sizeof(R) == 8 ? 5E-11 : 1E-6;
     st.traj_cap = p.traj_cap ? (long long)p.traj_cap : 0;
     st.traj_theta = p.traj_cap ? d_traj : nullptr;
     st.traj_func = p.traj_cap ? d_traj + p.traj_cap : nullptr;
@@ -371,7 +483,7 @@ class Engine {
       *iters = 0;
       return 0;
     }
-    if (!gx_cg && capture(&gx_cg, true, false)) return -1;
+    ensure_graph(&gx_cg, true, false);
     for (;;) {
       k_begin_run<<<1, 1, 0, s>>>(d_st);
       LAUNCHED(1);
@@ -379,7 +491,7 @@ class Engine {
       k_copy_der<R><<<nb_site, kSiteThreads, 0, s>>>(c);
       LAUNCHED(1);
       scalar(OP_DER, 1);
-      if (replay(gx_cg, per_iter_launches(true, false))) return -1;
+      if (replay(gx_cg, true, false)) return -1;
       *th = h_st->tr;
       const size_t loc = (size_t)h_st->iter;
       if (loc >= p.max_iters) {
@@ -400,17 +512,17 @@ class Engine {
       *iters = 0;
       return 0;
     }
-    if (!gx_sd || gx_sd_fixed != p.sd_fixed) {
+    if (gx_sd_fixed != p.sd_fixed) {
       if (gx_sd) cudaGraphExecDestroy(gx_sd);
       gx_sd = nullptr;
-      if (capture(&gx_sd, false, p.sd_fixed != 0)) return -1;
       gx_sd_fixed = p.sd_fixed;
     }
+    ensure_graph(&gx_sd, false, p.sd_fixed != 0);
     size_t total = 0;
     for (;;) {
       k_begin_run<<<1, 1, 0, s>>>(d_st);
       LAUNCHED(1);
-      if (replay(gx_sd, per_iter_launches(false, p.sd_fixed != 0))) return -1;
+      if (replay(gx_sd, false, p.sd_fixed != 0)) return -1;
       *th = h_st->tr;
       size_t loc = (size_t)h_st->iter;
       if (loc >= p.max_iters) {
@@ -449,11 +561,11 @@ class Engine {
       CK(cudaEventRecord(ev[1], s));
       scalar(OP_THETA_MAIN, 2);
       CK(cudaEventRecord(ev[2], s));
-      k_fft_xy<R><<<g_xy, 256, sm_xy, s>>>(c, 0, 0);
+      fft_xy(0, 0);
       CK(cudaEventRecord(ev[3], s));
-      k_fft_zt<R><<<g_zt, 256, sm_zt, s>>>(c);
+      fft_zt();
       CK(cudaEventRecord(ev[4], s));
-      k_fft_xy<R><<<g_xy, 256, sm_xy, s>>>(c, 1, 1);
+      fft_xy(1, 1);
       CK(cudaEventRecord(ev[5], s));
       scalar(OP_PR, 2);
       CK(cudaEventRecord(ev[6], s));
@@ -606,6 +718,16 @@ static int landau_staged(Engine<double> *e64, const gfix_params *gp,
       CK(cudaStreamSynchronize(e32->s));
       k_apply_gauge<<<e64->nb_site, kSiteThreads, 0, e64->s>>>(e64->c, G64);
       LAUNCHED(1);
+      // a phase that ended non-finite hands over nothing: restart in FP64
+      // from the staged input links
+      double tt = 0.0;
+      if (e64->reset(p) || e64->theta_test(&tt)) return -1;
+      if (!std::isfinite(th32) || !std::isfinite(tt)) {
+        if (e64->from_aos(e64->d_aos)) return -1;
+        it32 = 0;
+        tl32 = 0;
+        res.restarts++;
+      }
     }
     res.iters_fp32 = (it32 == kSentinel) ? p32.max_iters : it32;
     Params p64 = p;

@@ -64,7 +64,12 @@ struct DevState {
   int sparity;        // sb[sparity] = sn (old), sb[sparity ^ 1] = new
   int nblocks;        // partials written by the last reduction kernel
   int sd_fixed;       // GLU_GFIX_SD: fixed step gf_alpha in SD steps
+  double cg_tol;      // CG_TOL: 5e-11 in FP64, 1e-6 in FP32 (GLU's
+                      // SINGLE_PREC value, GLU_definitions.h:451-455)
 };
+
+// set or clear the done flag (used to run every kernel once as a no-op)
+__global__ void k_set_done(DevState *st, int v) { st->done = v; }
 
 // start of a solver run (GLU's steep_Landau_FACG / _FASD entry)
 __global__ void k_begin_run(DevState *st) {
@@ -226,128 +231,7 @@ __global__ void __launch_bounds__(kSiteThreads)
 // ---------------------------------------------------------------------
 // the 4D (or batched 3D) FFT with psq folded into the middle pass
 
-template <typename R>
-__device__ __forceinline__ const cx<R> *axis_tw(const Ctx<R> &c, int a) {
-  return c.tw + c.ax[a].tw_off;
-}
-
-// xy-plane pass: forward (bwd = 0) or inverse with the PR sums of
-// sum_PR3 (src/Gfix/FACG.c:99-145) fused in (prsum = 1).
-template <typename R>
-__global__ void __launch_bounds__(256) k_fft_xy(Ctx<R> c, int bwd, int prsum) {
-  if (c.st->done) return;
-  extern __shared__ unsigned char smem_raw[];
-  cx<R> *A = reinterpret_cast<cx<R> *>(smem_raw);
-  const int Lx = c.L[0], Ly = c.L[1], P = c.xy_pitch;
-  cx<R> *B = A + P * Ly;
-  const int plane = blockIdx.x, field = blockIdx.y;
-  const int par = c.st->parity;
-  const size_t base = (size_t)field * c.V + (size_t)plane * Lx * Ly;
-  cx<R> *data = c.fb[par] + base;
-  const int n = Lx * Ly;
-  for (int e = threadIdx.x; e < n; e += blockDim.x) {
-    const int x = e % Lx, y = e / Lx;
-    A[y * P + x] = data[e];
-  }
-  __syncthreads();
-  const PencilMap mx = {Ly, 1, 0, P, 1};   // rows
-  const PencilMap my = {Lx, Lx, 1, 0, P};  // columns
-  cx<R> *r = smem_fft(A, B, mx, c.ax[0], axis_tw(c, 0), bwd != 0);
-  cx<R> *o = (r == A) ? B : A;
-  r = smem_fft(r, o, my, c.ax[1], axis_tw(c, 1), bwd != 0);
-  double v[2] = {0.0, 0.0};
-  const cx<R> *old = c.fb[par ^ 1] + base;
-  for (int e = threadIdx.x; e < n; e += blockDim.x) {
-    const int x = e % Lx, y = e / Lx;
-    const cx<R> w = r[y * P + x];
-    data[e] = w;
-    if (prsum) {
-      const double a = w.x, b = w.y;
-      const cx<R> od = old[e];
-      const double tr = a - (double)od.x, ti = b - (double)od.y;
-      if (field == 0) {
-        v[0] += 2.0 * (a * a + b * b + a * b);
-        v[1] += 2.0 * (a * tr + b * ti) + (a * ti + b * tr);
-      } else {
-        v[0] += 2.0 * (a * a + b * b);
-        v[1] += 2.0 * (a * tr + b * ti);
-      }
-    }
-  }
-  if (prsum) {
-    block_sum_store<2>(v, c.part + 2 * (blockIdx.y * gridDim.x + blockIdx.x));
-    if (threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0)
-      c.st->nblocks = gridDim.x * gridDim.y;
-  }
-}
-
-// z(,t) pass: forward z (and t), multiply by psq = maxp / p^2 with
-// p^2 = 2 (D - sum_mu cos(2 pi n_mu / L_mu)), p = 0 -> 1
-// (src/Geometry/geometry.c:169-186), then inverse t (and z).
-// Landau: tile = zt_b consecutive x at fixed y, all z and t.
-// Coulomb: tile = zt_b consecutive x at fixed (y, t), all z.
-template <typename R>
-__global__ void __launch_bounds__(256) k_fft_zt(Ctx<R> c) {
-  if (c.st->done) return;
-  extern __shared__ unsigned char smem_raw[];
-  const int Lx = c.L[0], Ly = c.L[1], Lz = c.L[2], Lt = c.L[3];
-  const int Bw = c.zt_b;
-  const bool four = (c.ndim == 4);
-  const int nt = four ? Lt : 1;
-  cx<R> *A = reinterpret_cast<cx<R> *>(smem_raw);
-  cx<R> *Bf = A + Bw * Lz * nt;
-  int tile = blockIdx.x;
-  const int xb = tile % (Lx / Bw);
-  tile /= (Lx / Bw);
-  const int y = tile % Ly;
-  const int tslice = four ? 0 : tile / Ly;
-  const int field = blockIdx.y;
-  cx<R> *data = c.fb[c.st->parity] + (size_t)field * c.V;
-  const int x0 = xb * Bw;
-  const int n = Bw * Lz * nt;
-  for (int e = threadIdx.x; e < n; e += blockDim.x) {
-    const int b = e % Bw, rest = e / Bw;
-    const int z = rest % Lz, t = four ? rest / Lz : tslice;
-    const size_t g = (size_t)(x0 + b) + (size_t)Lx * (y + (size_t)Ly * (z + (size_t)Lz * t));
-    A[e] = data[g];
-  }
-  __syncthreads();
-  const PencilMap mz = {nt * Bw, Bw, 1, Lz * Bw, Bw};
-  const PencilMap mt = {Lz * Bw, Lz * Bw, 1, 0, Lz * Bw};
-  cx<R> *r = smem_fft(A, Bf, mz, c.ax[2], axis_tw(c, 2), false);
-  if (four) {
-    cx<R> *o = (r == A) ? Bf : A;
-    r = smem_fft(r, o, mt, c.ax[3], axis_tw(c, 3), false);
-  }
-  for (int e = threadIdx.x; e < n; e += blockDim.x) {
-    const int b = e % Bw, rest = e / Bw;
-    const int z = rest % Lz, t = rest / Lz;
-    double kcos = 0.0;
-    kcos += c.cs[0 * c.cs_ld + x0 + b];
-    kcos += c.cs[1 * c.cs_ld + y];
-    kcos += c.cs[2 * c.cs_ld + z];
-    if (four) kcos += c.cs[3 * c.cs_ld + t];
-    const double D = four ? 4.0 : 3.0;
-    const double p2 = (kcos == D) ? 1.0 : 2.0 * (D - kcos);
-    const R ps = (R)(c.maxp / p2);
-    r[e] = mk<R>(r[e].x * ps, r[e].y * ps);
-  }
-  __syncthreads();
-  {
-    cx<R> *o = (r == A) ? Bf : A;
-    if (four) {
-      r = smem_fft(r, o, mt, c.ax[3], axis_tw(c, 3), true);
-      o = (r == A) ? Bf : A;
-    }
-    r = smem_fft(r, o, mz, c.ax[2], axis_tw(c, 2), true);
-  }
-  for (int e = threadIdx.x; e < n; e += blockDim.x) {
-    const int b = e % Bw, rest = e / Bw;
-    const int z = rest % Lz, t = four ? rest / Lz : tslice;
-    const size_t g = (size_t)(x0 + b) + (size_t)Lx * (y + (size_t)Ly * (z + (size_t)Lz * t));
-    data[g] = r[e];
-  }
-}
+#include "fft_pass.cuh"
 
 // ---------------------------------------------------------------------
 // K4: conjugate direction update fused with the line-search probes.
@@ -544,11 +428,11 @@ __global__ void __launch_bounds__(kScalarThreads)
       st->sumconj = a[1];
       const double b = st->sumconj / st->inold;
       double beta = (b < 0.0) ? 0.0 : b;  // PRfmax (src/Gfix/CG.c:37-41)
-      if (st->tr < kCgTol) beta = st->insum / st->inold;
+      if (st->tr < st->cg_tol) beta = st->insum / st->inold;
       st->beta = beta;
       st->inold = st->insum;
       st->insum_last = st->insum;
-      st->use_ls = st->tr > kCgTol;
+      st->use_ls = st->tr > st->cg_tol;
       break;
     }
     case OP_PROBES: {

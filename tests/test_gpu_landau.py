@@ -158,5 +158,8 @@ def test_random_odd_lattice_against_oracle(oracle):
     U = oracle.reunit(np.eye(3) + 0.3 * U)
     r = gfix.landau_fix(U, d, 0.08, 1e-30, 3, "FACG", traj_cap=10)
     o = oracle.landau(U, d, 0.08, 1e-30, 3, "FACG", traj_cap=10)
-    assert _rel(r.traj_theta, o["traj_theta"]).max() < 1e-11
+    ot = o["traj_theta"]
+    # theta falls by six decades in three steps here: compare against the
+    # scale of the run, not of the tiny last value
+    assert np.all(np.abs(r.traj_theta - ot) <= 1e-11 * ot + 1e-14 * ot[0])
     assert np.abs(r.links - o["links"]).max() < 1e-12
