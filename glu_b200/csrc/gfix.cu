@@ -315,7 +315,7 @@ class Engine {
     if (sd_fixed) {
       scalar(OP_ALPHA_FIXED, 0);
     } else {
-      k_dir_probe<R, false><<<nb_site, kSiteThreads, 0, s>>>(c);
+      k_dir_probe<R, false, double><<<nb_site, kSiteThreads, 0, s>>>(c);
       LAUNCHED(1);
       scalar(OP_PROBES, 2);
     }
@@ -328,7 +328,7 @@ class Engine {
     theta(OP_THETA_MAIN);
     fft(true);
     scalar(OP_PR, 2);
-    k_dir_probe<R, true><<<nb_site, kSiteThreads, 0, s>>>(c);
+    k_dir_probe<R, true, double><<<nb_site, kSiteThreads, 0, s>>>(c);
     LAUNCHED(1);
     scalar(OP_PROBES, 2);
     k_update<R, true><<<nb_site, kSiteThreads, 0, s>>>(c);
@@ -439,7 +439,9 @@ class Engine {
     st.acc = p.acc;
     st.max_iters = (long long)p.max_iters;
     st.sd_fixed = p.sd_fixed;
-    st.cg_tol = sizeof(R) == 8 ? 5E-11 : 1E-6;
+    // GLU's CG_TOL (5e-11) in both phases: with FP64 probe arithmetic the
+    // FP32 phase keeps its line search down to the precision switch
+    st.cg_tol = 5E-11;
     st.traj_cap = p.traj_cap ? (long long)p.traj_cap : 0;
     st.traj_theta = p.traj_cap ? d_traj : nullptr;
     st.traj_func = p.traj_cap ? d_traj + p.traj_cap : nullptr;
@@ -569,7 +571,7 @@ class Engine {
       CK(cudaEventRecord(ev[5], s));
       scalar(OP_PR, 2);
       CK(cudaEventRecord(ev[6], s));
-      k_dir_probe<R, true><<<nb_site, kSiteThreads, 0, s>>>(c);
+      k_dir_probe<R, true, double><<<nb_site, kSiteThreads, 0, s>>>(c);
       CK(cudaEventRecord(ev[7], s));
       CK(cudaStreamSynchronize(s));
       float t[7];

@@ -64,8 +64,7 @@ struct DevState {
   int sparity;        // sb[sparity] = sn (old), sb[sparity ^ 1] = new
   int nblocks;        // partials written by the last reduction kernel
   int sd_fixed;       // GLU_GFIX_SD: fixed step gf_alpha in SD steps
-  double cg_tol;      // CG_TOL: 5e-11 in FP64, 1e-6 in FP32 (GLU's
-                      // SINGLE_PREC value, GLU_definitions.h:451-455)
+  double cg_tol;      // CG_TOL (GLU_definitions.h:451-455)
 };
 
 // set or clear the done flag (used to run every kernel once as a no-op)
@@ -258,7 +257,10 @@ __device__ __forceinline__ void dir_at(const Ctx<R> &c, const cx<R> *in,
   }
 }
 
-template <typename R, bool DIR>
+// C is the arithmetic precision of the probes: the FP32 phase of the mixed
+// solver evaluates them in FP64 from its FP32 links and directions, because
+// per-site probe differences fall below FP32 rounding once theta < ~1e-6.
+template <typename R, bool DIR, typename C = R>
 __global__ void __launch_bounds__(kSiteThreads) k_dir_probe(Ctx<R> c) {
   if (c.st->done) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -280,20 +282,24 @@ __global__ void __launch_bounds__(kSiteThreads) k_dir_probe(Ctx<R> c) {
       int x[4], sd[4];
       coords(s, c.L, x);
       strides(c, sd);
-      cx<R> A1[9], A2[9], Bm[9], U[9];
-      set_gauge(A1, f[0], f[1], f[2], f[3], R(0.15));
-      set_gauge(A2, f[0], f[1], f[2], f[3], R(0.30));
-      R d1 = 0, d2 = 0;
+      auto up = [](cx<R> a) { return mk<C>((C)a.x, (C)a.y); };
+      cx<C> A1[9], A2[9], Bm[9], U[9];
+      set_gauge(A1, up(f[0]), up(f[1]), up(f[2]), up(f[3]), C(0.15));
+      set_gauge(A2, up(f[0]), up(f[1]), up(f[2]), up(f[3]), C(0.30));
+      C d1 = 0, d2 = 0;
 #pragma unroll 1
       for (int mu = 0; mu < 4; mu++) {
         const int y = fwd_site(s, mu, x, c.L, sd);
         cx<R> fy[4];
         dir_at<R, DIR>(c, in, so, beta, y, fy);
-        load_link(c.U, c.V, mu, s, U);
-        const R t0 = U[0].x + U[4].x + U[8].x;
-        set_gauge(Bm, fy[0], fy[1], fy[2], fy[3], R(0.15));
+        cx<R> u[9];
+        load_link(c.U, c.V, mu, s, u);
+#pragma unroll
+        for (int e = 0; e < 9; e++) U[e] = up(u[e]);
+        const C t0 = U[0].x + U[4].x + U[8].x;
+        set_gauge(Bm, up(fy[0]), up(fy[1]), up(fy[2]), up(fy[3]), C(0.15));
         d1 += re_tr_abc_dag(A1, U, Bm) - t0;
-        set_gauge(Bm, fy[0], fy[1], fy[2], fy[3], R(0.30));
+        set_gauge(Bm, up(fy[0]), up(fy[1]), up(fy[2]), up(fy[3]), C(0.30));
         d2 += re_tr_abc_dag(A2, U, Bm) - t0;
       }
       v[0] = d1;
