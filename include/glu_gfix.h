@@ -156,6 +156,22 @@ int gfix_profile_landau(const double *d_links, const size_t dims[4],
                         const gfix_params *p, int iters, double *ms,
                         double *bytes);
 
+/* theta_test_lin (src/Gfix/gftests.c:214-250) and the gauge functional
+ * (gftests.c:132-147) of the device links d_links (double[V][4][9][2] in
+ * HBM), written to the device array d_out[0..1].  No counterpart in the
+ * reference: it serves callers that cannot allocate device memory when they
+ * call in -- codes that give all of HBM to their own arena allocator, and
+ * stream-ordered pipelines in which cudaMalloc/cudaFree would synchronise
+ * the device.  It allocates nothing: its scratch is a fixed 1 MiB device
+ * array inside the library, so lattices above 16,777,216 sites are rejected.
+ * Calls that overlap on the GPU race on that array.  The first call on a
+ * device looks the array up; make it before any stream capture.  Launches on
+ * the legacy default stream; returns 0, or -1 with the reason in
+ * gfix_noalloc_error(). */
+int gfix_theta_functional_noalloc(const double *d_links, const size_t dims[4],
+                                  double *d_out);
+const char *gfix_noalloc_error(void);
+
 /* message of the last failed call (thread-local, never NULL) */
 const char *gfix_last_error(void);
 
