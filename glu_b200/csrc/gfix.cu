@@ -608,13 +608,13 @@ class Engine {
 
   // links: device AoS FP64 -> SoA R (and back)
   int from_aos(const double *aos) {
-    k_aos_to_soa<R><<<1184, 256, 0, s>>>(aos, d_U, V);
+    k_aos_to_soa<R><<<(V + kTrSites - 1) / kTrSites, 256, 0, s>>>(aos, d_U, V);
     LAUNCHED(1);
     CK(cudaGetLastError());
     return 0;
   }
   int to_aos(double *aos) {
-    k_soa_to_aos<R><<<1184, 256, 0, s>>>(d_U, aos, V);
+    k_soa_to_aos<R><<<(V + kTrSites - 1) / kTrSites, 256, 0, s>>>(d_U, aos, V);
     LAUNCHED(1);
     CK(cudaGetLastError());
     return 0;

@@ -477,26 +477,46 @@ __global__ void __launch_bounds__(kScalarThreads)
 // ---------------------------------------------------------------------
 // layout conversion: host AoS double[V][4][9][2] <-> device SoA cx<R>
 
+// One block moves kTrSites consecutive sites through shared memory so that
+// both the AoS side (36 contiguous complex numbers per site) and the SoA side
+// (kTrSites contiguous numbers per element row) are accessed coalesced.
+constexpr int kTrSites = 64;
+
 template <typename R>
-__global__ void k_aos_to_soa(const double *__restrict__ aos, cx<R> *U, int V) {
-  const size_t n = (size_t)V * 36;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const int s = (int)(i / 36), r = (int)(i % 36);  // r = mu*9 + e
-    const double2 v = reinterpret_cast<const double2 *>(aos)[i];
-    U[(size_t)r * V + s] = mk<R>((R)v.x, (R)v.y);
+__global__ void __launch_bounds__(256) k_aos_to_soa(const double *__restrict__ aos,
+                                                    cx<R> *U, int V) {
+  __shared__ double2 t[kTrSites * 36 + 1];
+  const size_t s0 = (size_t)blockIdx.x * kTrSites;
+  const int ns = (int)min((size_t)kTrSites, (size_t)V - s0);
+  const double2 *src = reinterpret_cast<const double2 *>(aos) + s0 * 36;
+  for (int i = threadIdx.x; i < ns * 36; i += blockDim.x) t[i] = src[i];
+  __syncthreads();
+  for (int i = threadIdx.x; i < 36 * kTrSites; i += blockDim.x) {
+    const int r = i / kTrSites, sl = i % kTrSites;
+    if (sl < ns) {
+      const double2 v = t[sl * 36 + r];
+      U[(size_t)r * V + s0 + sl] = mk<R>((R)v.x, (R)v.y);
+    }
   }
 }
 
 template <typename R>
-__global__ void k_soa_to_aos(const cx<R> *U, double *__restrict__ aos, int V) {
-  const size_t n = (size_t)V * 36;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const int s = (int)(i / 36), r = (int)(i % 36);
-    const cx<R> v = U[(size_t)r * V + s];
-    reinterpret_cast<double2 *>(aos)[i] = make_double2((double)v.x, (double)v.y);
+__global__ void __launch_bounds__(256) k_soa_to_aos(const cx<R> *U,
+                                                    double *__restrict__ aos,
+                                                    int V) {
+  __shared__ double2 t[kTrSites * 36 + 1];
+  const size_t s0 = (size_t)blockIdx.x * kTrSites;
+  const int ns = (int)min((size_t)kTrSites, (size_t)V - s0);
+  for (int i = threadIdx.x; i < 36 * kTrSites; i += blockDim.x) {
+    const int r = i / kTrSites, sl = i % kTrSites;
+    if (sl < ns) {
+      const cx<R> v = U[(size_t)r * V + s0 + sl];
+      t[sl * 36 + r] = make_double2((double)v.x, (double)v.y);
+    }
   }
+  __syncthreads();
+  double2 *dst = reinterpret_cast<double2 *>(aos) + s0 * 36;
+  for (int i = threadIdx.x; i < ns * 36; i += blockDim.x) dst[i] = t[i];
 }
 
 }  // namespace gfix
