@@ -1,0 +1,187 @@
+// Compile-time specialised FFT passes for the common lattice extents
+// (products of 2 and 3 up to 64).  Same algorithm, tiles and results as the
+// generic passes in fft_pass.cuh (in-place Stockham stages in shared memory,
+// radix 8/4/2/3, twiddles staged in shared memory), but every extent, stride
+// and pencil mapping is a template constant, so the per-butterfly index
+// arithmetic folds to shifts and multiply-adds and every loop unrolls.
+// Included by kernels.cuh inside namespace gfix, after fft_pass.cuh.
+
+// radix of the next stage for a remaining length m
+__host__ __device__ constexpr int ct_radix(int m) {
+  return (m % 8 == 0) ? 8 : (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2 : 3;
+}
+// can the extent be transformed by the compile-time stages?
+__host__ __device__ constexpr bool ct_ok(int n) {
+  while (n % 2 == 0) n /= 2;
+  while (n % 3 == 0) n /= 3;
+  return n == 1;
+}
+
+// Stockham stages for pencils of length N; pencil p starts at
+// (p / PIN) * PSHI + (p % PIN) * PSLO, elements are JS apart; BD threads.
+template <typename R, int N, int Ns, int NP, int PIN, int PSLO, int PSHI,
+          int JS, int BD>
+__device__ __forceinline__ void ct_stages(cx<R> *buf, const cx<R> *tw,
+                                          bool bwd) {
+  if constexpr (Ns < N) {
+    constexpr int RDX = ct_radix(N / Ns);
+    constexpr int NB = N / RDX;
+    constexpr int TOTAL = NP * NB;
+    constexpr int K = (TOTAL + BD - 1) / BD;
+    constexpr int STEP0 = N / (Ns * RDX);
+    cx<R> v[K][RDX];
+    int dst[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const int idx = threadIdx.x + k * BD;
+      dst[k] = -1;
+      if (TOTAL % BD == 0 || idx < TOTAL) {
+        const int p = idx / NB, j = idx % NB;
+        const int po = (p / PIN) * PSHI + (p % PIN) * PSLO;
+        const int jq = j / Ns, jm = j % Ns;
+#pragma unroll
+        for (int s = 0; s < RDX; s++) {
+          v[k][s] = buf[po + (j + s * NB) * JS];
+          if constexpr (Ns > 1)
+            if (s > 0) v[k][s] = cmul(v[k][s], twiddle(tw, s * jm * STEP0, bwd));
+        }
+        dft_reg<R, RDX>(v[k], tw, N, bwd);
+        dst[k] = po + (jq * Ns * RDX + jm) * JS;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (dst[k] >= 0) {
+#pragma unroll
+        for (int s = 0; s < RDX; s++) buf[dst[k] + s * Ns * JS] = v[k][s];
+      }
+    }
+    __syncthreads();
+    ct_stages<R, N, Ns * RDX, NP, PIN, PSLO, PSHI, JS, BD>(buf, tw, bwd);
+  }
+}
+
+__host__ __device__ constexpr int ct_threads(int n) { return n / 8 < 32 ? 32 : n / 8; }
+
+// xy-plane pass with compile-time extents (see k_fft_xy)
+template <typename R, int LX, int LY>
+__global__ void __launch_bounds__(ct_threads(LX *LY))
+    k_fft_xy_ct(Ctx<R> c, int bwd, int prsum) {
+  if (c.st->done) return;
+  constexpr int P = LX + 1, N = LX * LY, BD = ct_threads(N);
+  constexpr int EPT = (N + BD - 1) / BD;
+  extern __shared__ unsigned char smem_raw[];
+  cx<R> *A = reinterpret_cast<cx<R> *>(smem_raw);
+  cx<R> *twx = A + P * LY;
+  cx<R> *twy = twx + LX;
+  stage_twiddles(twx, c.tw + c.ax[0].tw_off, LX);
+  stage_twiddles(twy, c.tw + c.ax[1].tw_off, LY);
+  const int plane = blockIdx.x, field = blockIdx.y;
+  const int par = c.st->parity;
+  const size_t base = (size_t)field * c.V + (size_t)plane * N;
+  cx<R> *data = c.fb[par] + base;
+#pragma unroll
+  for (int k = 0; k < EPT; k++) {
+    const int e = threadIdx.x + k * BD;
+    if (N % BD == 0 || e < N) A[(e / LX) * P + e % LX] = data[e];
+  }
+  __syncthreads();
+  ct_stages<R, LX, 1, LY, 1, 0, P, 1, BD>(A, twx, bwd != 0);   // rows
+  ct_stages<R, LY, 1, LX, LX, 1, 0, P, BD>(A, twy, bwd != 0);  // columns
+  double v[2] = {0.0, 0.0};
+  const cx<R> *old = c.fb[par ^ 1] + base;
+#pragma unroll
+  for (int k = 0; k < EPT; k++) {
+    const int e = threadIdx.x + k * BD;
+    if (N % BD != 0 && e >= N) continue;
+    const cx<R> w = A[(e / LX) * P + e % LX];
+    data[e] = w;
+    if (prsum) {
+      const cx<R> od = old[e];
+      const double a = w.x, b = w.y;
+      const double tr = a - (double)od.x, ti = b - (double)od.y;
+      if (field == 0) {
+        v[0] += 2.0 * (a * a + b * b + a * b);
+        v[1] += 2.0 * (a * tr + b * ti) + (a * ti + b * tr);
+      } else {
+        v[0] += 2.0 * (a * a + b * b);
+        v[1] += 2.0 * (a * tr + b * ti);
+      }
+    }
+  }
+  if (prsum) {
+    block_sum_store<2>(v, c.part + 2 * (blockIdx.y * gridDim.x + blockIdx.x));
+    if (threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0)
+      c.st->nblocks = gridDim.x * gridDim.y;
+  }
+}
+
+// z(,t) pass with compile-time extents (see k_fft_zt).  NT = Lt for Landau
+// (z and t transformed); NT = 1 for Coulomb (z only, one slice per tile).
+template <typename R, int LZ, int NT, int B>
+__global__ void __launch_bounds__(ct_threads(B *LZ *NT))
+    k_fft_zt_ct(Ctx<R> c) {
+  if (c.st->done) return;
+  constexpr bool FOUR = NT > 1;
+  constexpr int TS = FOUR ? LZ * B + 1 : LZ * B;  // padded t-stride
+  constexpr int N = B * LZ * NT, BD = ct_threads(N);
+  constexpr int EPT = (N + BD - 1) / BD;
+  extern __shared__ unsigned char smem_raw[];
+  cx<R> *A = reinterpret_cast<cx<R> *>(smem_raw);
+  cx<R> *twz = A + TS * NT;
+  cx<R> *twt = twz + LZ;
+  stage_twiddles(twz, c.tw + c.ax[2].tw_off, LZ);
+  if constexpr (FOUR) stage_twiddles(twt, c.tw + c.ax[3].tw_off, NT);
+  const int Lx = c.L[0], Ly = c.L[1];
+  const int nxb = Lx / B;
+  int tile = blockIdx.x;
+  const int xb = tile % nxb;
+  tile /= nxb;
+  const int y = tile % Ly;
+  const int tslice = FOUR ? 0 : tile / Ly;
+  const int field = blockIdx.y;
+  cx<R> *data = c.fb[c.st->parity] + (size_t)field * c.V;
+  const int x0 = xb * B;
+  const size_t sz = (size_t)Lx * Ly;
+  const size_t base = (size_t)x0 + (size_t)Lx * y + sz * LZ * tslice;
+#pragma unroll
+  for (int k = 0; k < EPT; k++) {
+    const int e = threadIdx.x + k * BD;
+    if (N % BD == 0 || e < N) {
+      const int q = e / B, b = e % B, t = q / LZ, z = q % LZ;
+      A[b + B * z + TS * t] = data[base + b + sz * q];
+    }
+  }
+  __syncthreads();
+  ct_stages<R, LZ, 1, NT * B, B, 1, TS, B, BD>(A, twz, false);
+  if constexpr (FOUR) ct_stages<R, NT, 1, LZ * B, LZ * B, 1, 0, TS, BD>(A, twt, false);
+  const double D = FOUR ? 4.0 : 3.0;
+  const double cxy = c.cs[1 * c.cs_ld + y];
+#pragma unroll
+  for (int k = 0; k < EPT; k++) {
+    const int e = threadIdx.x + k * BD;
+    if (N % BD != 0 && e >= N) continue;
+    const int q = e / B, b = e % B, t = q / LZ, z = q % LZ;
+    double kcos = 0.0;
+    kcos += c.cs[x0 + b];
+    kcos += cxy;
+    kcos += c.cs[2 * c.cs_ld + z];
+    if constexpr (FOUR) kcos += c.cs[3 * c.cs_ld + t];
+    const double p2 = (kcos == D) ? 1.0 : 2.0 * (D - kcos);
+    const R ps = (R)(c.maxp * __drcp_rn(p2));
+    const int o = b + B * z + TS * t;
+    A[o] = mk<R>(A[o].x * ps, A[o].y * ps);
+  }
+  __syncthreads();
+  if constexpr (FOUR) ct_stages<R, NT, 1, LZ * B, LZ * B, 1, 0, TS, BD>(A, twt, true);
+  ct_stages<R, LZ, 1, NT * B, B, 1, TS, B, BD>(A, twz, true);
+#pragma unroll
+  for (int k = 0; k < EPT; k++) {
+    const int e = threadIdx.x + k * BD;
+    if (N % BD == 0 || e < N) {
+      const int q = e / B, b = e % B, t = q / LZ, z = q % LZ;
+      data[base + b + sz * q] = A[b + B * z + TS * t];
+    }
+  }
+}

@@ -83,6 +83,34 @@ static int factorize(int n, FftAxis &ax) {
   return 0;
 }
 
+// compile-time specialised FFT passes for the common extents; nullptr
+// where the generic passes serve
+template <typename R>
+using XyFn = void (*)(Ctx<R>, int, int);
+template <typename R>
+using ZtFn = void (*)(Ctx<R>);
+
+template <typename R>
+static XyFn<R> ct_xy(int lx, int ly) {
+#define GFIX_XY(n) \
+  if (lx == n && ly == n) return k_fft_xy_ct<R, n, n>;
+  GFIX_XY(4) GFIX_XY(8) GFIX_XY(16) GFIX_XY(24) GFIX_XY(32) GFIX_XY(48)
+  GFIX_XY(64)
+#undef GFIX_XY
+  return nullptr;
+}
+
+template <typename R>
+static ZtFn<R> ct_zt(int lz, int lt, int b) {
+#define GFIX_ZT(z, t, bb) \
+  if (lz == z && lt == t && b == bb) return k_fft_zt_ct<R, z, t, bb>;
+  GFIX_ZT(4, 4, 2) GFIX_ZT(4, 8, 2) GFIX_ZT(8, 8, 2) GFIX_ZT(8, 16, 2)
+  GFIX_ZT(16, 16, 2) GFIX_ZT(16, 32, 2) GFIX_ZT(24, 48, 2)
+  GFIX_ZT(32, 32, 2) GFIX_ZT(32, 64, 2)
+#undef GFIX_ZT
+  return nullptr;
+}
+
 struct Params {
   double gf_alpha = 0.08, acc = 1e-14;
   size_t max_iters = 1000;
@@ -108,6 +136,8 @@ class Engine {
   size_t sm_xy = 0, sm_zt = 0;
   int bd_xy = 256, bd_zt = 256, pt_xy = 8, pt_zt = 8;
   bool odd = false;
+  XyFn<R> xy_ct = nullptr;
+  ZtFn<R> zt_ct = nullptr;
   cudaGraphExec_t gx_cg = nullptr, gx_sd = nullptr;
   int gx_sd_fixed = -1;
   bool primed = false;
@@ -221,6 +251,19 @@ class Engine {
     // the dynamic shared-memory limit is an attribute of the function, not
     // of a launch: raise it once to the largest tile any engine can use
     if (set_smem_limits()) return -1;
+    // compile-time specialised passes where the extents have one
+    xy_ct = odd ? nullptr : ct_xy<R>(c.L[0], c.L[1]);
+    zt_ct = odd ? nullptr : ct_zt<R>(c.L[2], c.L[3], c.zt_b);
+    if (xy_ct) {
+      bd_xy = ct_threads(c.L[0] * c.L[1]);
+      CK(cudaFuncSetAttribute(xy_ct, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sm_xy));
+    }
+    if (zt_ct) {
+      bd_zt = ct_threads(c.zt_b * c.L[2] * c.L[3]);
+      CK(cudaFuncSetAttribute(zt_ct, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sm_zt));
+    }
     g_xy = dim3(V / (c.L[0] * c.L[1]), 4);
     g_zt = dim3((c.L[0] / c.zt_b) * c.L[1], 4);
     nb_site = (V + kSiteThreads - 1) / kSiteThreads;
@@ -285,7 +328,9 @@ class Engine {
     return 0;
   }
   void fft_xy(int bwd, int prsum) {
-    if (odd)
+    if (xy_ct)
+      xy_ct<<<g_xy, bd_xy, sm_xy, s>>>(c, bwd, prsum);
+    else if (odd)
       k_fft_xy<R, 16, true><<<g_xy, bd_xy, sm_xy, s>>>(c, bwd, prsum);
     else if (pt_xy == 8)
       k_fft_xy<R, 8, false><<<g_xy, bd_xy, sm_xy, s>>>(c, bwd, prsum);
@@ -294,7 +339,9 @@ class Engine {
     LAUNCHED(1);
   }
   void fft_zt() {
-    if (odd)
+    if (zt_ct)
+      zt_ct<<<g_zt, bd_zt, sm_zt, s>>>(c);
+    else if (odd)
       k_fft_zt<R, 16, true><<<g_zt, bd_zt, sm_zt, s>>>(c);
     else if (pt_zt == 8)
       k_fft_zt<R, 8, false><<<g_zt, bd_zt, sm_zt, s>>>(c);

@@ -231,6 +231,7 @@ __global__ void __launch_bounds__(kSiteThreads)
 // the 4D (or batched 3D) FFT with psq folded into the middle pass
 
 #include "fft_pass.cuh"
+#include "fft_ct.cuh"
 
 // ---------------------------------------------------------------------
 // K4: conjugate direction update fused with the line-search probes.
@@ -283,25 +284,28 @@ __global__ void __launch_bounds__(kSiteThreads) k_dir_probe(Ctx<R> c) {
       coords(s, c.L, x);
       strides(c, sd);
       auto up = [](cx<R> a) { return mk<C>((C)a.x, (C)a.y); };
-      cx<C> A1[9], A2[9], Bm[9], U[9];
-      set_gauge(A1, up(f[0]), up(f[1]), up(f[2]), up(f[3]), C(0.15));
-      set_gauge(A2, up(f[0]), up(f[1]), up(f[2]), up(f[3]), C(0.30));
-      C d1 = 0, d2 = 0;
+      // one probe at a time: a single matrix at x stays live
+      C d[2] = {0, 0};
 #pragma unroll 1
-      for (int mu = 0; mu < 4; mu++) {
-        const int y = fwd_site(s, mu, x, c.L, sd);
-        cx<R> fy[4];
-        dir_at<R, DIR>(c, in, so, beta, y, fy);
-        cx<R> u[9];
-        load_link(c.U, c.V, mu, s, u);
+      for (int k = 0; k < 2; k++) {
+        const C al = k == 0 ? C(0.15) : C(0.30);
+        cx<C> A[9], Bm[9], U[9];
+        set_gauge(A, up(f[0]), up(f[1]), up(f[2]), up(f[3]), al);
+#pragma unroll 1
+        for (int mu = 0; mu < 4; mu++) {
+          const int y = fwd_site(s, mu, x, c.L, sd);
+          cx<R> fy[4];
+          dir_at<R, DIR>(c, in, so, beta, y, fy);
+          cx<R> u[9];
+          load_link(c.U, c.V, mu, s, u);
 #pragma unroll
-        for (int e = 0; e < 9; e++) U[e] = up(u[e]);
-        const C t0 = U[0].x + U[4].x + U[8].x;
-        set_gauge(Bm, up(fy[0]), up(fy[1]), up(fy[2]), up(fy[3]), C(0.15));
-        d1 += re_tr_abc_dag(A1, U, Bm) - t0;
-        set_gauge(Bm, up(fy[0]), up(fy[1]), up(fy[2]), up(fy[3]), C(0.30));
-        d2 += re_tr_abc_dag(A2, U, Bm) - t0;
+          for (int e = 0; e < 9; e++) U[e] = up(u[e]);
+          const C t0 = U[0].x + U[4].x + U[8].x;
+          set_gauge(Bm, up(fy[0]), up(fy[1]), up(fy[2]), up(fy[3]), al);
+          d[k] += re_tr_abc_dag(A, U, Bm) - t0;
+        }
       }
+      const C d1 = d[0], d2 = d[1];
       v[0] = d1;
       v[1] = d2;
     }

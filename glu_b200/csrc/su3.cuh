@@ -67,12 +67,13 @@ __device__ __forceinline__ cx<R> cscale(cx<R> a, R s) {
 }
 
 // column Gram-Schmidt of columns 0 (u0,u3,u6) and 1 (u1,u4,u7); column 2
-// from their conjugate cross product
+// from their conjugate cross product.  The normalisations use rsqrt (within
+// an ulp of GLU's 1/sqrt, far cheaper than a division and a square root).
 template <typename R>
 __device__ __forceinline__ void gram_reunit(cx<R> *u) {
   R n = (u[0].x * u[0].x + u[3].x * u[3].x + u[6].x * u[6].x) +
         (u[0].y * u[0].y + u[3].y * u[3].y + u[6].y * u[6].y);
-  R s = R(1) / sqrt(n);
+  R s = rsqrt(n);
   u[0] = cscale(u[0], s);
   u[3] = cscale(u[3], s);
   u[6] = cscale(u[6], s);
@@ -82,7 +83,7 @@ __device__ __forceinline__ void gram_reunit(cx<R> *u) {
   u[7] = csub(u[7], cmul(p, u[6]));
   n = (u[1].x * u[1].x + u[4].x * u[4].x + u[7].x * u[7].x) +
       (u[1].y * u[1].y + u[4].y * u[4].y + u[7].y * u[7].y);
-  s = R(1) / sqrt(n);
+  s = rsqrt(n);
   u[1] = cscale(u[1], s);
   u[4] = cscale(u[4], s);
   u[7] = cscale(u[7], s);
