@@ -1,0 +1,453 @@
+// Coulomb gauge fixing of every time slice at once (GLU's Coulomb_FA,
+// src/Gfix/CFACG.c:531-636, solves the slices one after the other; they are
+// independent problems on the original spatial links, so here all of them
+// advance together, each with its own scalars, iteration count and end).
+//
+// Per slice t the unknown is the slice gauge field g_t(x) (SoA [9][V], the
+// slices side by side), the derivative is taken on the rotated links
+// g(x) U_i(x,t) g(x+i)^dag (steep_deriv_CG, CFACG.c:91-163), the FFT is the
+// 3D transform of each slice (FOURIER_ACCELERATE2) done by the Landau passes
+// with ndim = 3, and the update is g <- reunit(1 + a A) g
+// (exponentiate_gauge_CG, line_search.c:101-115).  Each step of a slice is
+// either an SD step (a run's first step, every FASD step) or a CG step.
+// A slice whose run ends is reunitarised and checked (adequate_solution,
+// CFACG.c:432-456), continued, or restarted from a random g (steep_fix,
+// CFACG.c:459-529); finished slices are masked out of every kernel.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace gfix {
+
+constexpr double kPrecTol = 3 * 1.0E-14;  // PREC_TOL, GLU_definitions.h:359-363
+constexpr int kCoulThreads = 128;
+
+enum SliceMode : int { SL_RUN = 0, SL_DONE = 1 };
+
+struct Slice {
+  double tr, inold, insum, sumconj, beta, alpha;
+  long long iter;     // steps of the current run (GLU's loc_iters)
+  long long tot;      // GLU's tot_iters of steep_fix
+  int sd;             // next step is an SD step
+  int use_ls;
+  int mode;           // SL_RUN / SL_DONE
+  int control;        // random restarts so far
+  int reunit;         // maintenance: reunitarise g_t and check it
+  int randomize;      // maintenance: random restart of g_t
+  int bad;            // set when the unitarity check fails
+  int trans;          // GLU's trans_flag: survives a continuation run
+  int traj_len;
+};
+
+struct CoulState {
+  double gf_alpha, acc, cg_tol;
+  long long max_iters;
+  int facg;           // 1 FACG, 0 FASD
+  int sd_fixed;       // GLU_GFIX_SD semantics
+  int active;         // slices still running
+  int nslices;
+  unsigned long long seed;
+  int traj_cap;       // per slice
+  double *traj;       // [nslices][traj_cap]
+};
+
+template <typename R>
+struct CCtx {
+  cx<R> *U;           // links SoA [4][9][V]
+  cx<R> *g;           // slice gauge fields SoA [9][V]
+  cx<R> *fb[2];       // in / in_old
+  cx<R> *sb[2];       // sn ping-pong
+  DevState *st;       // parities (shared with the FFT passes)
+  CoulState *cs;
+  Slice *sl;
+  double *part;       // [nslices][nbs][2]
+  int L[4];
+  int V, Lcu, nbs;
+};
+
+__device__ __forceinline__ void coul_coords(int i, const int *L, int *x) {
+  x[0] = i % L[0];
+  i /= L[0];
+  x[1] = i % L[1];
+  x[2] = i / L[1];
+}
+
+// in-slice forward / backward neighbour of slice site i in direction mu < 3
+__device__ __forceinline__ int sfwd(int i, int mu, const int *x, const int *L,
+                                    const int *sd) {
+  return x[mu] == L[mu] - 1 ? i - (L[mu] - 1) * sd[mu] : i + sd[mu];
+}
+__device__ __forceinline__ int sbck(int i, int mu, const int *x, const int *L,
+                                    const int *sd) {
+  return x[mu] == 0 ? i + (L[mu] - 1) * sd[mu] : i - sd[mu];
+}
+
+template <typename R>
+__device__ __forceinline__ void load9(const cx<R> *p, int V, int s, cx<R> *u) {
+#pragma unroll
+  for (int e = 0; e < 9; e++) u[e] = p[(size_t)e * V + s];
+}
+template <typename R>
+__device__ __forceinline__ void store9(cx<R> *p, int V, int s, const cx<R> *u) {
+#pragma unroll
+  for (int e = 0; e < 9; e++) p[(size_t)e * V + s] = u[e];
+}
+
+// rotated link g(a) U g(b)^dag of the reference's gtransform_local
+template <typename R>
+__device__ __forceinline__ void rotated(const CCtx<R> &c, int mu, int s_link,
+                                        int sa, int sb, cx<R> *C) {
+  cx<R> A[9], B[9];
+  load_link(c.U, c.V, mu, s_link, C);
+  load9(c.g, c.V, sa, A);
+  load9(c.g, c.V, sb, B);
+  gtransform(A, C, B);
+}
+
+// ---------------------------------------------------------------------
+// derivative on the rotated links, packed like the Landau fields
+// (steep_deriv_CG, src/Gfix/CFACG.c:91-163)
+template <typename R>
+__global__ void __launch_bounds__(kCoulThreads) k_cderiv(CCtx<R> c) {
+  const int t = blockIdx.y;
+  if (c.sl[t].mode == SL_DONE) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // in-slice site
+  if (i >= c.Lcu) return;
+  int x[3];
+  coul_coords(i, c.L, x);
+  const int sd[3] = {1, c.L[0], c.L[0] * c.L[1]};
+  const int off = t * c.Lcu;
+  R s0 = 0, s3 = 0;
+  cx<R> s1 = mk<R>(0, 0), s2 = mk<R>(0, 0), s4 = mk<R>(0, 0);
+#pragma unroll 1
+  for (int mu = 0; mu < 3; mu++) {
+    const int it = sfwd(i, mu, x, c.L, sd), bk = sbck(i, mu, x, c.L, sd);
+    cx<R> C[9], D[9];
+    rotated(c, mu, off + i, off + i, off + it, C);   // g(i) U(i) g(i+mu)^dag
+    rotated(c, mu, off + bk, off + bk, off + i, D);  // g(i-mu) U(i-mu) g(i)^dag
+    R b0, b3, a0, a3;
+    cx<R> b1, b2, b4, a1, a2, a4;
+    herm_short(C, b0, b1, b2, b3, b4);
+    herm_short(D, a0, a1, a2, a3, a4);
+    s0 += a0 - b0;
+    s1 = cadd(s1, csub(a1, b1));
+    s2 = cadd(s2, csub(a2, b2));
+    s3 += a3 - b3;
+    s4 = cadd(s4, csub(a4, b4));
+  }
+  // pack: in0 = i Re s0 - Re s3, in_k = i Re s_k - Im s_k (CFACG.c:144-150)
+  cx<R> *f = c.fb[c.st->parity];
+  const size_t V = c.V, s = off + i;
+  f[s] = mk<R>(-s3, s0);
+  f[V + s] = mk<R>(-s1.y, s1.x);
+  f[2 * V + s] = mk<R>(-s2.y, s2.x);
+  f[3 * V + s] = mk<R>(-s4.y, s4.x);
+}
+
+// sums of the accelerated field: insum (sum_PR / sum_DER2 form, both the
+// same 2 (r^2 + i^2 + r i) + 2 |.|^2 norm) and sum_conj
+// (src/Gfix/CFACG.c:165-258), per slice
+template <typename R>
+__global__ void __launch_bounds__(kCoulThreads) k_csums(CCtx<R> c) {
+  const int t = blockIdx.y;
+  double v[2] = {0.0, 0.0};
+  const bool live = c.sl[t].mode != SL_DONE;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (live && i < c.Lcu) {
+    const int par = c.st->parity;
+    const cx<R> *in = c.fb[par], *old = c.fb[par ^ 1];
+    const size_t V = c.V, s = (size_t)t * c.Lcu + i;
+    const bool cg = !c.sl[t].sd;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const double a = in[k * V + s].x, b = in[k * V + s].y;
+      double l1 = a * a + b * b, l2 = 0.0;
+      if (k == 0) l1 += a * b;
+      if (cg) {
+        const double tr = a - (double)old[k * V + s].x,
+                     ti = b - (double)old[k * V + s].y;
+        l2 = 2.0 * (a * tr + b * ti);
+        if (k == 0) l2 += a * ti + b * tr;
+      }
+      v[0] += 2.0 * l1;
+      v[1] += l2;
+    }
+  }
+  block_sum_store<2>(v, c.part + 2 * ((size_t)t * c.nbs + blockIdx.x));
+}
+
+// sn = in + beta sn_old at site s (the same fma form as the Landau kernels);
+// an SD step takes sn = in without reading sn_old
+template <typename R>
+__device__ __forceinline__ void cdir(const cx<R> *in, const cx<R> *so, R beta,
+                                     bool sd, size_t s, size_t V, cx<R> *f) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const cx<R> a = in[k * V + s];
+    if (sd) {
+      f[k] = a;
+    } else {
+      const cx<R> b = so[k * V + s];
+      f[k] = mk<R>(fma(beta, b.x, a.x), fma(beta, b.y, a.y));
+    }
+  }
+}
+
+// direction sn = in + beta_t sn_old (beta_t = 0 on SD steps, so sn = in),
+// written for every live slice, and the line-search probes of
+// line_search_Coulomb (src/Gfix/line_search.c:141-271) at 0.17 and 0.34 as
+// differences to the alpha = 0 value; each link counted once (forward links
+// of every site, the same set the reference's draughtboard visits)
+template <typename R>
+__global__ void __launch_bounds__(kCoulThreads) k_cprobe(CCtx<R> c) {
+  const int t = blockIdx.y;
+  double v[2] = {0.0, 0.0};
+  const Slice &S = c.sl[t];
+  const bool live = S.mode != SL_DONE;
+  const bool probes = live && S.use_ls;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (live && i < c.Lcu) {
+    const int par = c.st->parity, spar = c.st->sparity;
+    const cx<R> *in = c.fb[par], *so = c.sb[spar];
+    cx<R> *sn = c.sb[spar ^ 1];
+    const R beta = (R)S.beta;
+    const bool sdstep = S.sd != 0;
+    const int off = t * c.Lcu;
+    cx<R> f[4];
+    cdir(in, so, beta, sdstep, (size_t)off + i, (size_t)c.V, f);
+#pragma unroll
+    for (int k = 0; k < 4; k++) sn[(size_t)k * c.V + off + i] = f[k];
+    if (probes) {
+      int x[3];
+      coul_coords(i, c.L, x);
+      const int sd[3] = {1, c.L[0], c.L[0] * c.L[1]};
+      auto up = [](cx<R> a) { return mk<double>((double)a.x, (double)a.y); };
+      double d[2] = {0.0, 0.0};
+#pragma unroll 1
+      for (int k = 0; k < 2; k++) {
+        const double al = k == 0 ? 0.17 : 0.34;
+        cx<double> A[9], Bm[9], Cd[9];
+        set_gauge(A, up(f[0]), up(f[1]), up(f[2]), up(f[3]), al);
+#pragma unroll 1
+        for (int mu = 0; mu < 3; mu++) {
+          const int it = sfwd(i, mu, x, c.L, sd);
+          cx<R> C[9], fy[4];
+          rotated(c, mu, off + i, off + i, off + it, C);
+          cdir(in, so, beta, sdstep, (size_t)off + it, (size_t)c.V, fy);
+#pragma unroll
+          for (int e = 0; e < 9; e++) Cd[e] = up(C[e]);
+          const double t0 = Cd[0].x + Cd[4].x + Cd[8].x;
+          set_gauge(Bm, up(fy[0]), up(fy[1]), up(fy[2]), up(fy[3]), al);
+          d[k] += re_tr_abc_dag(A, Cd, Bm) - t0;
+        }
+      }
+      v[0] = d[0];
+      v[1] = d[1];
+    }
+  }
+  if (probes) block_sum_store<2>(v, c.part + 2 * ((size_t)t * c.nbs + blockIdx.x));
+}
+
+// g(x) <- reunit(1 + alpha_t sn(x)) g(x) (exponentiate_gauge_CG,
+// src/Gfix/line_search.c:101-115)
+template <typename R>
+__global__ void __launch_bounds__(kCoulThreads) k_cupdate(CCtx<R> c) {
+  const int t = blockIdx.y;
+  const Slice &S = c.sl[t];
+  if (S.mode == SL_DONE) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.Lcu) return;
+  const size_t V = c.V, s = (size_t)t * c.Lcu + i;
+  const cx<R> *d = c.sb[c.st->sparity ^ 1];
+  cx<R> A[9], G[9], r[9];
+  set_gauge(A, d[s], d[V + s], d[2 * V + s], d[3 * V + s], (R)S.alpha);
+  load9(c.g, c.V, (int)s, G);
+  multab(r, A, G);
+  store9(c.g, c.V, (int)s, r);
+}
+
+// per-slice housekeeping at the end of a run: reunitarise g_t and check its
+// norm (adequate_solution, src/Gfix/CFACG.c:432-456), or replace g_t by
+// random SU(3) matrices for a restart (steep_fix, CFACG.c:507-522; our own
+// generator, not GLU's RNG stream)
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kCoulThreads) k_cmaint(CCtx<R> c, int what) {
+  const int t = blockIdx.y;
+  Slice &S = c.sl[t];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.Lcu || S.mode == SL_DONE) return;
+  const int s = t * c.Lcu + i;
+  if (what == 0 && S.reunit) {
+    cx<R> G[9];
+    load9(c.g, c.V, s, G);
+    gram_reunit(G);
+    store9(c.g, c.V, s, G);
+    double sum = 0.0;
+#pragma unroll
+    for (int e = 0; e < 9; e++) sum += (double)G[e].x * G[e].x + (double)G[e].y * G[e].y;
+    const double lim = (double)(S.iter > 0 ? S.iter : 1) * kPrecTol;
+    if (fabs(sum - 3.0) > lim) atomicOr(&S.bad, 1);
+  } else if (what == 1 && S.randomize) {
+    cx<R> G[9];
+    unsigned long long h = mix64(c.cs->seed ^ mix64(((unsigned long long)t << 40) ^
+                                                    ((unsigned long long)S.control << 32) ^
+                                                    (unsigned long long)i));
+#pragma unroll
+    for (int e = 0; e < 9; e++) {
+      h = mix64(h);
+      const double u1 = ((h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+      h = mix64(h);
+      const double u2 = ((h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+      const double rad = sqrt(-2.0 * log(u1));
+      G[e] = mk<R>((R)(rad * cospi(2.0 * u2)), (R)(rad * sinpi(2.0 * u2)));
+    }
+    gram_reunit(G);
+    store9(c.g, c.V, s, G);
+  }
+}
+
+enum CoulOp : int { C_SUMS = 0, C_PROBES = 1, C_END1 = 2, C_END2 = 3 };
+
+// one thread per slice: fixed-order sums of the slice's partials and GLU's
+// control flow of steep_step_FACG / _FASD and steep_fix
+// (src/Gfix/CFACG.c:285-529)
+__global__ void k_cscalar(CoulState *cs, Slice *sl, const double *part,
+                          int nbs, int op, double Lcu, DevState *st) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < cs->nslices) {
+    Slice &S = sl[t];
+    if (S.mode != SL_DONE) {
+      double a0 = 0.0, a1 = 0.0;
+      if (op == C_SUMS || op == C_PROBES) {
+        for (int b = 0; b < nbs; b++) {
+          a0 += part[2 * ((size_t)t * nbs + b)];
+          a1 += part[2 * ((size_t)t * nbs + b) + 1];
+        }
+      }
+      switch (op) {
+        case C_SUMS: {
+          S.insum = a0;
+          S.sumconj = a1;
+          S.tr = a0 / (3.0 * Lcu);  // GFNORM_COULOMB
+          if (S.sd) {
+            S.inold = a0;
+            S.beta = 0.0;
+            // FACG's SD start always searches (CFACG.c:318); FASD steps
+            // search unless GLU_GFIX_SD (CFACG.c:270-280)
+            S.use_ls = cs->facg ? 1 : !cs->sd_fixed;
+          } else {
+            const double b = S.sumconj / S.inold;
+            double beta = (b < 0.0) ? 0.0 : b;
+            if (S.tr < cs->cg_tol) beta = S.insum / S.inold;
+            S.beta = beta;
+            S.inold = S.insum;
+            S.use_ls = S.tr > cs->cg_tol;
+          }
+          if (cs->traj && S.traj_len < cs->traj_cap)
+            cs->traj[(size_t)t * cs->traj_cap + S.traj_len++] = S.tr;
+          break;
+        }
+        case C_PROBES: {
+          if (S.use_ls) {
+            const double al[3] = {0.0, 0.17, 0.34};
+            const double f[3] = {0.0, -a0, -a1};
+            S.alpha = approx_minimum(al, f);
+          } else {
+            S.alpha = cs->gf_alpha;
+          }
+          break;
+        }
+        case C_END1: {
+          S.reunit = 0;
+          S.bad = 0;
+          S.randomize = 0;
+          if (cs->facg && S.sd) {
+            S.sd = 0;  // the SD start is not counted
+            break;
+          }
+          S.iter++;
+          if ((S.tr > cs->acc) && (S.iter < cs->max_iters)) break;
+          S.reunit = S.tr < cs->acc;  // run ended: adequate_solution first
+          S.sd = -1;                  // marks "ended" for C_END2
+          break;
+        }
+        case C_END2: {
+          if (S.sd != -1) break;
+          const long long loc = S.iter;
+          const bool fin = isfinite(S.tr);
+          if (S.bad) S.trans = 1;
+          S.sd = 1;
+          S.iter = 0;
+          if (loc >= cs->max_iters) {
+            if (S.tr < 1E4 * cs->acc && fin) {  // continuation run
+              S.tot += loc;
+              break;
+            }
+            if (S.tr > cs->acc || !fin) S.trans = 1;
+          }
+          if (S.control < 8 && S.trans) {  // random restart
+            S.randomize = 1;
+            S.trans = 0;
+            S.tot += loc;
+            S.control++;
+            break;
+          }
+          S.tot += loc;
+          S.iter = loc;
+          S.mode = SL_DONE;
+          // the slice that ends last stops the whole sequence
+          if (atomicSub(&cs->active, 1) == 1) st->done = 1;
+          break;
+        }
+      }
+    }
+  }
+}
+
+// the slice transforms of Coulomb_FA (gtransform_slice, src/Gfix/gtrans.c:
+// 214-238): U_i(x,t) <- g_t(x) U_i(x,t) g_t(x+i)^dag for i < 3 and
+// U_t(x,t) <- g_t(x) U_t(x,t) g_{t+1}(x)^dag, periodic in t
+template <typename R>
+__global__ void __launch_bounds__(kCoulThreads) k_cslice_transform(CCtx<R> c) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= c.V) return;
+  const int t = s / c.Lcu, i = s - t * c.Lcu;
+  int x[3];
+  coul_coords(i, c.L, x);
+  const int sd[3] = {1, c.L[0], c.L[0] * c.L[1]};
+  cx<R> A[9], B[9], U[9];
+  load9(c.g, c.V, s, A);
+  for (int mu = 0; mu < 4; mu++) {
+    const int nb = mu < 3 ? t * c.Lcu + sfwd(i, mu, x, c.L, sd)
+                          : ((t + 1) % c.L[3]) * c.Lcu + i;
+    load9(c.g, c.V, nb, B);
+    load_link(c.U, c.V, mu, s, U);
+    gtransform(A, U, B);
+    store_link(c.U, c.V, mu, s, U);
+  }
+}
+
+// in / in_old and sn ping-pong after every step of every live slice
+__global__ void k_cflip(DevState *st) {
+  if (st->done) return;
+  st->parity ^= 1;
+  st->sparity ^= 1;
+}
+
+template <typename R>
+__global__ void k_cinit(CCtx<R> c) {
+  const size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (s >= (size_t)c.V) return;
+  cx<R> G[9];
+  set_identity(G);
+  store9(c.g, c.V, (int)s, G);
+}
+
+}  // namespace gfix

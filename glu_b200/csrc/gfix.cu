@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "../../include/glu_gfix.h"
+#include "coulomb.cuh"
 #include "extra_kernels.cuh"
 #include "kernels.cuh"
 
@@ -107,6 +108,8 @@ static ZtFn<R> ct_zt(int lz, int lt, int b) {
   GFIX_ZT(4, 4, 2) GFIX_ZT(4, 8, 2) GFIX_ZT(8, 8, 2) GFIX_ZT(8, 16, 2)
   GFIX_ZT(16, 16, 2) GFIX_ZT(16, 32, 2) GFIX_ZT(24, 48, 2)
   GFIX_ZT(32, 32, 2) GFIX_ZT(32, 64, 2)
+  GFIX_ZT(4, 1, 8) GFIX_ZT(8, 1, 8) GFIX_ZT(16, 1, 8) GFIX_ZT(24, 1, 8)
+  GFIX_ZT(32, 1, 8) GFIX_ZT(48, 1, 8) GFIX_ZT(64, 1, 8)
 #undef GFIX_ZT
   return nullptr;
 }
@@ -136,6 +139,8 @@ class Engine {
   size_t sm_xy = 0, sm_zt = 0;
   int bd_xy = 256, bd_zt = 256, pt_xy = 8, pt_zt = 8;
   bool odd = false;
+  bool coul = false;
+  int Lcu = 0;
   XyFn<R> xy_ct = nullptr;
   ZtFn<R> zt_ct = nullptr;
   cudaGraphExec_t gx_cg = nullptr, gx_sd = nullptr;
@@ -149,7 +154,15 @@ class Engine {
   void release() {
     if (gx_cg) cudaGraphExecDestroy(gx_cg);
     if (gx_sd) cudaGraphExecDestroy(gx_sd);
-    gx_cg = gx_sd = nullptr;
+    if (gx_coul) cudaGraphExecDestroy(gx_coul);
+    gx_cg = gx_sd = gx_coul = nullptr;
+    cudaFree(d_cst);
+    cudaFreeHost(h_cst);
+    cudaFree(d_sl);
+    cudaFreeHost(h_sl);
+    cudaFree(d_ctraj);
+    d_cst = nullptr;
+    d_sl = nullptr;
     cudaFree(d_st);
     cudaFreeHost(h_st);
     cudaFree(d_part);
@@ -168,7 +181,9 @@ class Engine {
     s = nullptr;
   }
 
-  int init(const size_t *d, bool with_G, bool with_staging) {
+  int init(const size_t *d, bool with_G, bool with_staging,
+           bool coulomb = false) {
+    coul = coulomb;
     for (int i = 0; i < 4; i++) dims[i] = d[i];
     const size_t Vs = d[0] * d[1] * d[2] * d[3];
     if (Vs == 0 || Vs > (size_t)INT32_MAX / 4)
@@ -183,8 +198,11 @@ class Engine {
         return fail("extent %d has a prime factor above %d", c.L[i], kMaxRadix);
     }
     c.V = V;
-    c.ndim = 4;
-    c.maxp = 4.0 * 4 / (double)V;  // MAX_LANDAU
+    Lcu = (int)(d[0] * d[1] * d[2]);
+    c.ndim = coul ? 3 : 4;
+    // MAX_LANDAU = 4 ND / V, MAX_COULOMB = 4 (ND - 1) / LCU
+    // (GLU_definitions.h:414, 420)
+    c.maxp = coul ? 4.0 * 3 / (double)Lcu : 4.0 * 4 / (double)V;
     // twiddle pool: one table per axis
     std::vector<cx<R>> tw;
     for (int a = 0; a < 4; a++) {
@@ -214,7 +232,10 @@ class Engine {
     c.cs_ld = ld;
     // tiles
     c.xy_pitch = c.L[0] + 1;
-    const int want_b = 2;
+    // x columns per zt tile: 2 (32-byte rows in FP64) for Landau's big
+    // (z, t) tiles; Coulomb tiles hold one slice's z pencils only
+    const int want_b = coul ? 8 : 2;
+    const int nt = coul ? 1 : c.L[3];
     c.zt_b = 1;
     for (int b = want_b; b >= 1; b--)
       if (c.L[0] % b == 0) {
@@ -229,11 +250,11 @@ class Engine {
       t = std::max<size_t>(128, (t + 31) / 32 * 32);
       return t;
     };
-    while (c.zt_b > 1 && (size_t)c.zt_b * c.L[2] * c.L[3] > 512u * pt_small)
+    while (c.zt_b > 1 && (size_t)c.zt_b * c.L[2] * nt > 512u * pt_small)
       c.zt_b /= 2;
     while (c.zt_b > 1 && c.L[0] % c.zt_b) c.zt_b /= 2;
     const size_t n_xy = (size_t)c.L[0] * c.L[1];
-    const size_t n_zt = (size_t)c.zt_b * c.L[2] * c.L[3];
+    const size_t n_zt = (size_t)c.zt_b * c.L[2] * nt;
     if (n_xy > 8192 || n_zt > 8192)
       return fail("FFT tile of %zu / %zu elements exceeds 8192", n_xy, n_zt);
     odd = false;
@@ -246,26 +267,27 @@ class Engine {
     bd_zt = (int)threads_for(n_zt, pt_zt);
     // tile (padded) plus the twiddle tables of its two axes
     sm_xy = ((size_t)c.xy_pitch * c.L[1] + c.L[0] + c.L[1]) * sizeof(cx<R>);
-    sm_zt = ((size_t)(c.zt_b * c.L[2] + 1) * c.L[3] + c.L[2] + c.L[3]) *
-            sizeof(cx<R>);
+    sm_zt = coul ? ((size_t)c.zt_b * c.L[2] + c.L[2]) * sizeof(cx<R>)
+                 : ((size_t)(c.zt_b * c.L[2] + 1) * c.L[3] + c.L[2] + c.L[3]) *
+                       sizeof(cx<R>);
     // the dynamic shared-memory limit is an attribute of the function, not
     // of a launch: raise it once to the largest tile any engine can use
     if (set_smem_limits()) return -1;
     // compile-time specialised passes where the extents have one
     xy_ct = odd ? nullptr : ct_xy<R>(c.L[0], c.L[1]);
-    zt_ct = odd ? nullptr : ct_zt<R>(c.L[2], c.L[3], c.zt_b);
+    zt_ct = odd ? nullptr : ct_zt<R>(c.L[2], nt, c.zt_b);
     if (xy_ct) {
       bd_xy = ct_threads(c.L[0] * c.L[1]);
       CK(cudaFuncSetAttribute(xy_ct, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)sm_xy));
     }
     if (zt_ct) {
-      bd_zt = ct_threads(c.zt_b * c.L[2] * c.L[3]);
+      bd_zt = ct_threads(c.zt_b * c.L[2] * nt);
       CK(cudaFuncSetAttribute(zt_ct, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)sm_zt));
     }
     g_xy = dim3(V / (c.L[0] * c.L[1]), 4);
-    g_zt = dim3((c.L[0] / c.zt_b) * c.L[1], 4);
+    g_zt = dim3((c.L[0] / c.zt_b) * c.L[1] * (coul ? c.L[3] : 1), 4);
     nb_site = (V + kSiteThreads - 1) / kSiteThreads;
     const size_t nparts =
         std::max<size_t>((size_t)nb_site, (size_t)g_xy.x * g_xy.y) + 1024;
@@ -653,6 +675,188 @@ class Engine {
     return 0;
   }
 
+  // ------------------------------------------------------------------
+  // Coulomb: all slices as independent 3D problems (coulomb.cuh)
+  CCtx<R> cc{};
+  CoulState *d_cst = nullptr, *h_cst = nullptr;
+  Slice *d_sl = nullptr, *h_sl = nullptr;
+  double *d_ctraj = nullptr;
+  size_t ctraj_alloc = 0;
+  int nbs = 0;
+  cudaGraphExec_t gx_coul = nullptr;
+
+  int cinit() {
+    if (d_cst) return 0;
+    const int T = c.L[3];
+    nbs = (Lcu + kCoulThreads - 1) / kCoulThreads;
+    CK(cudaMalloc(&d_cst, sizeof(CoulState)));
+    CK(cudaMallocHost(&h_cst, sizeof(CoulState)));
+    CK(cudaMalloc(&d_sl, sizeof(Slice) * T));
+    CK(cudaMallocHost(&h_sl, sizeof(Slice) * T));
+    // per-slice partials: [T][nbs] pairs, next to the engine's own uses
+    const size_t need = (size_t)T * nbs;
+    const size_t have =
+        std::max<size_t>((size_t)nb_site, (size_t)g_xy.x * g_xy.y) + 1024;
+    if (need > have) {
+      cudaFree(d_part);
+      CK(cudaMalloc(&d_part, (need + 1024) * 2 * sizeof(double)));
+      c.part = d_part;
+    }
+    cc.U = d_U;
+    cc.g = d_G;
+    cc.fb[0] = c.fb[0];
+    cc.fb[1] = c.fb[1];
+    cc.sb[0] = c.sb[0];
+    cc.sb[1] = c.sb[1];
+    cc.st = d_st;
+    cc.cs = d_cst;
+    cc.sl = d_sl;
+    cc.part = d_part;
+    for (int i = 0; i < 4; i++) cc.L[i] = c.L[i];
+    cc.V = V;
+    cc.Lcu = Lcu;
+    cc.nbs = nbs;
+    return 0;
+  }
+
+  void cscalar(int op) {
+    const int T = c.L[3];
+    k_cscalar<<<(T + 127) / 128, 128, 0, s>>>(
+        d_cst, d_sl, d_part, nbs, op, (double)Lcu, d_st);
+    LAUNCHED(1);
+  }
+
+  void capture_coul() {
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+      cudaGetLastError();
+      graph_ok = false;
+      return;
+    }
+    const unsigned long long before = g_launches.load();
+    citer();
+    g_launches.store(before);
+    if (cudaStreamEndCapture(s, &g) != cudaSuccess ||
+        cudaGraphInstantiate(&gx_coul, g, 0) != cudaSuccess) {
+      cudaGetLastError();
+      gx_coul = nullptr;
+      graph_ok = false;
+    }
+    if (g) cudaGraphDestroy(g);
+  }
+
+  // one step of every live slice
+  void citer() {
+    const dim3 gs(nbs, c.L[3]);
+    k_cderiv<R><<<gs, kCoulThreads, 0, s>>>(cc);
+    fft_xy(0, 0);
+    fft_zt();
+    fft_xy(1, 0);
+    k_csums<R><<<gs, kCoulThreads, 0, s>>>(cc);
+    cscalar(C_SUMS);
+    k_cprobe<R><<<gs, kCoulThreads, 0, s>>>(cc);
+    cscalar(C_PROBES);
+    k_cupdate<R><<<gs, kCoulThreads, 0, s>>>(cc);
+    cscalar(C_END1);
+    k_cmaint<R><<<gs, kCoulThreads, 0, s>>>(cc, 0);
+    cscalar(C_END2);
+    k_cmaint<R><<<gs, kCoulThreads, 0, s>>>(cc, 1);
+    k_cflip<<<1, 1, 0, s>>>(d_st);
+    LAUNCHED(7);
+  }
+
+  // GLU's Coulomb_FA (src/Gfix/CFACG.c:531-636) on the resident links
+  int csolve(const Params &p, size_t *iters, double *slice_theta,
+             size_t *slice_iters, size_t *traj_len) {
+    if (cinit()) return -1;
+    const int T = c.L[3];
+    const size_t per = p.traj_cap ? p.traj_cap / T : 0;
+    if (per && per * T > ctraj_alloc) {
+      cudaFree(d_ctraj);
+      CK(cudaMalloc(&d_ctraj, per * T * sizeof(double)));
+      ctraj_alloc = per * T;
+    }
+    CoulState cst;
+    memset(&cst, 0, sizeof cst);
+    cst.gf_alpha = p.gf_alpha;
+    cst.acc = p.acc;
+    cst.cg_tol = 5E-11;
+    cst.max_iters = (long long)p.max_iters;
+    cst.facg = p.algo == GFIX_CG;
+    cst.sd_fixed = p.sd_fixed;
+    cst.active = T;
+    cst.nslices = T;
+    cst.seed = 0x5DEECE66Dull;
+    cst.traj_cap = (int)per;
+    cst.traj = per ? d_ctraj : nullptr;
+    CK(cudaMemcpyAsync(d_cst, &cst, sizeof cst, cudaMemcpyHostToDevice, s));
+    std::vector<Slice> sl(T);
+    memset(sl.data(), 0, sizeof(Slice) * T);
+    for (auto &x : sl) {
+      x.sd = 1;
+      x.mode = SL_RUN;
+    }
+    CK(cudaMemcpyAsync(d_sl, sl.data(), sizeof(Slice) * T,
+                       cudaMemcpyHostToDevice, s));
+    DevState st;
+    memset(&st, 0, sizeof st);
+    CK(cudaMemcpyAsync(d_st, &st, sizeof st, cudaMemcpyHostToDevice, s));
+    // sn starts at zero: SD steps use beta = 0 against it
+    CK(cudaMemsetAsync(c.sb[0], 0, (size_t)V * 8 * sizeof(cx<R>), s));
+    k_cinit<R><<<(V + 255) / 256, 256, 0, s>>>(cc);
+    LAUNCHED(1);
+    const unsigned long long per_iter = 14;  // launches in citer()
+    int batch = 2;
+    size_t guard = 0;
+    const size_t limit = (p.max_iters + 2) * 9 * 64 + 1024;
+    for (;;) {
+      // the first steps run as direct launches (they load every kernel of
+      // the sequence), the rest as replays of one captured step
+      if (guard > 0 && !gx_coul && graph_ok) capture_coul();
+      for (int k = 0; k < batch; k++) {
+        if (gx_coul) {
+          CK(cudaGraphLaunch(gx_coul, s));
+          LAUNCHED(per_iter);
+        } else {
+          citer();
+        }
+      }
+      CK(cudaGetLastError());
+      if (read_state()) return -1;
+      if (h_st->done) break;
+      guard += batch;
+      if (guard > limit)
+        return fail("Coulomb solve did not stop after %zu steps", guard);
+      batch = std::min(batch * 2, 32);
+    }
+    k_cslice_transform<R><<<(V + kCoulThreads - 1) / kCoulThreads,
+                            kCoulThreads, 0, s>>>(cc);
+    LAUNCHED(1);
+    CK(cudaMemcpyAsync(h_sl, d_sl, sizeof(Slice) * T, cudaMemcpyDeviceToHost,
+                       s));
+    CK(cudaStreamSynchronize(s));
+    size_t tot = 0;
+    for (int t = 0; t < T; t++) {
+      tot += (size_t)h_sl[t].tot;
+      if (slice_theta) slice_theta[t] = h_sl[t].tr;
+      if (slice_iters) slice_iters[t] = (size_t)h_sl[t].tot;
+    }
+    *iters = tot;
+    if (traj_len) *traj_len = 0;
+    if (per && p.traj_theta) {
+      // slice-major, stride per = traj_cap / Lt; unused entries are NaN
+      std::vector<double> h(per * T);
+      CK(cudaMemcpy(h.data(), d_ctraj, h.size() * sizeof(double),
+                    cudaMemcpyDeviceToHost));
+      for (int t = 0; t < T; t++)
+        for (size_t k = 0; k < per; k++)
+          p.traj_theta[t * per + k] =
+              (int)k < h_sl[t].traj_len ? h[t * per + k] : NAN;
+      if (traj_len) *traj_len = per * T;
+    }
+    return 0;
+  }
+
   // links: device AoS FP64 -> SoA R (and back)
   int from_aos(const double *aos) {
     k_aos_to_soa<R><<<(V + kTrSites - 1) / kTrSites, 256, 0, s>>>(aos, d_U, V);
@@ -713,6 +917,25 @@ static Engine<float> *engine32(const size_t *d) {
   if (e->init(d, true, false)) return nullptr;
   Engine<float> *p = e.get();
   g_e32[k] = std::move(e);
+  return p;
+}
+
+// Coulomb engines: FP64, with the slice gauge fields in d_G
+static std::map<Key, std::unique_ptr<Engine<double>>> g_ec;
+
+static Engine<double> *engine_coul(const size_t *d) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    fail("no CUDA device");
+    return nullptr;
+  }
+  Key k{dev, {d[0], d[1], d[2], d[3]}, 64};
+  auto it = g_ec.find(k);
+  if (it != g_ec.end()) return it->second.get();
+  auto e = std::make_unique<Engine<double>>();
+  if (e->init(d, true, true, true)) return nullptr;
+  Engine<double> *p = e.get();
+  g_ec[k] = std::move(e);
   return p;
 }
 
@@ -823,6 +1046,7 @@ unsigned long long gfix_kernel_launches(void) { return g_launches.load(); }
 void gfix_release(void) {
   g_e64.clear();
   g_e32.clear();
+  g_ec.clear();
 }
 
 static int check_params(const size_t *dims, const gfix_params *p) {
@@ -950,17 +1174,70 @@ int gfix_profile_landau(const double *d_links, const size_t dims[4],
   return e->profile_cg(q, iters, ms, bytes);
 }
 
+// the staged links of `e` (AoS FP64 in e->d_aos) Coulomb-fixed in place
+static int coulomb_staged(Engine<double> *e, const gfix_params *gp,
+                          gfix_result *r, double *slice_theta,
+                          size_t *slice_iters) {
+  const Params p = to_params(gp);
+  const int T = e->c.L[3];
+  std::vector<double> th(T);
+  std::vector<size_t> it(T);
+  gfix_result res;
+  memset(&res, 0, sizeof res);
+  CK(cudaEventRecord(e->ev0, e->s));
+  if (e->from_aos(e->d_aos)) return -1;
+  size_t iters = 0, tl = 0;
+  if (e->csolve(p, &iters, th.data(), it.data(), &tl)) return -1;
+  CK(cudaEventRecord(e->ev1, e->s));
+  if (e->to_aos(e->d_aos)) return -1;
+  CK(cudaStreamSynchronize(e->s));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+  double worst = 0.0;
+  int restarts = 0;
+  for (int t = 0; t < T; t++) {
+    worst = std::isnan(th[t]) || th[t] > worst ? th[t] : worst;
+    restarts += e->h_sl[t].control;
+    if (slice_theta) slice_theta[t] = th[t];
+    if (slice_iters) slice_iters[t] = it[t];
+  }
+  res.iters = iters;
+  res.theta = worst;
+  res.traj_len = tl;
+  res.gpu_ms = ms;
+  res.restarts = restarts;
+  if (r) *r = res;
+  return 0;
+}
+
 int gfix_coulomb(double *links, const size_t dims[4], const gfix_params *p,
                  gfix_result *r, double *slice_theta, size_t *slice_iters) {
-  (void)links; (void)dims; (void)p; (void)r; (void)slice_theta;
-  (void)slice_iters;
-  return fail("Coulomb gauge fixing is not built yet");
+  if (check_params(dims, p)) return -1;
+  if (!links) return fail("null links");
+  Engine<double> *e = engine_coul(dims);
+  if (!e) return -1;
+  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
+  if (coulomb_staged(e, p, r, slice_theta, slice_iters)) return -1;
+  CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
+  CK(cudaStreamSynchronize(e->s));
+  return 0;
 }
 
 int gfix_coulomb_device(double *d_links, const size_t dims[4],
                         const gfix_params *p, gfix_result *r,
                         double *slice_theta, size_t *slice_iters) {
-  return gfix_coulomb(d_links, dims, p, r, slice_theta, slice_iters);
+  if (check_params(dims, p)) return -1;
+  if (!d_links) return fail("null links");
+  Engine<double> *e = engine_coul(dims);
+  if (!e) return -1;
+  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpyAsync(e->d_aos, d_links, bytes, cudaMemcpyDeviceToDevice, e->s));
+  if (coulomb_staged(e, p, r, slice_theta, slice_iters)) return -1;
+  CK(cudaMemcpyAsync(d_links, e->d_aos, bytes, cudaMemcpyDeviceToDevice, e->s));
+  CK(cudaStreamSynchronize(e->s));
+  return 0;
 }
 
 }  // extern "C"

@@ -41,6 +41,7 @@ class FixResult:
     traj_func: np.ndarray = field(default_factory=lambda: np.zeros(0))
     slice_theta: np.ndarray | None = None
     slice_iters: np.ndarray | None = None
+    restarts: int = 0
 
 
 def _dims(dims):
@@ -94,22 +95,44 @@ def landau_fix(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
 def coulomb_fix(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
                 algo="FACG", sd_fixed_step=False, precision="FP64",
                 switch_theta=1e-9, traj_cap=0) -> FixResult:
-    """Coulomb FA gauge fixing of all slices (GLU's Coulomb_FA)."""
-    lib = _lib.load()
+    """Coulomb FA gauge fixing of all slices (GLU's Coulomb_FA) of a copy of
+    `links`.  traj_theta is slice-major: traj_cap // Lt entries per slice,
+    NaN past the slice's last FFT round."""
     cd, d = _dims(dims)
     U = _links(links, d)
+    r = _coulomb(U.ctypes.data, cd, d, gf_alpha, accuracy, max_iters, algo,
+                 sd_fixed_step, precision, switch_theta, traj_cap, False)
+    r.links = U
+    return r
+
+
+def coulomb_fix_device(d_links, dims, gf_alpha=0.08, accuracy=1e-14,
+                       max_iters=1000, algo="FACG", sd_fixed_step=False,
+                       precision="FP64", switch_theta=1e-9,
+                       traj_cap=0) -> FixResult:
+    """As coulomb_fix on links already in HBM: `d_links` is a device pointer
+    (e.g. ``tensor.data_ptr()``) to double[V][4][9][2], fixed in place."""
+    cd, d = _dims(dims)
+    return _coulomb(int(d_links), cd, d, gf_alpha, accuracy, max_iters, algo,
+                    sd_fixed_step, precision, switch_theta, traj_cap, True)
+
+
+def _coulomb(ptr, cd, d, gf_alpha, accuracy, max_iters, algo, sd_fixed_step,
+             precision, switch_theta, traj_cap, device) -> FixResult:
+    lib = _lib.load()
     p, tt, tf = _params(gf_alpha, accuracy, max_iters, algo, sd_fixed_step,
                         precision, switch_theta, traj_cap)
     r = GfixResult()
     sth = np.zeros(d[3])
     sit = np.zeros(d[3], dtype=np.uintp)
-    check(lib.gfix_coulomb(U.ctypes.data, cd, C.byref(p), C.byref(r),
-                           sth.ctypes.data_as(C.POINTER(C.c_double)),
-                           sit.ctypes.data_as(C.POINTER(C.c_size_t))))
+    fn = lib.gfix_coulomb_device if device else lib.gfix_coulomb
+    check(fn(ptr, cd, C.byref(p), C.byref(r),
+             sth.ctypes.data_as(C.POINTER(C.c_double)),
+             sit.ctypes.data_as(C.POINTER(C.c_size_t))))
     n = r.traj_len
-    return FixResult(U, int(r.iters), float(r.theta), int(r.iters_fp32),
+    return FixResult(None, int(r.iters), float(r.theta), int(r.iters_fp32),
                      float(r.gpu_ms), tt[:n].copy(), tf[:n].copy(), sth,
-                     sit.astype(np.int64))
+                     sit.astype(np.int64), int(r.restarts))
 
 
 # --- GLU-named entry points -------------------------------------------------
