@@ -53,7 +53,12 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--dims", default="32,32,32,64")
+    ap.add_argument("--workload", default="landau", choices=["landau", "coulomb"],
+                    help="landau: 32^3x64 Landau FACG (the headline); coulomb: "
+                         "64^3x128 Coulomb FACG, all slices batched")
+    ap.add_argument("--dims", default=None,
+                    help="lattice extents; default 32,32,32,64 (landau) or "
+                         "64,64,64,128 (coulomb)")
     ap.add_argument("--profile-iters", type=int, default=20)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -433,10 +438,277 @@ def profile_only(args, dims):
                       for k in range(7)}})
 
 
+# ---------------------------------------------------------------------------
+# Coulomb workload: every time slice of a 64^3x128 configuration fixed to
+# theta < 1e-14 (GLU's Coulomb_FA, FACG), all slices in one batched launch
+# sequence.  FP64.
+
+C_METRIC = "Coulomb-gauge-fixed configs/hour (64^3x128 FACG, theta<1e-14 per slice)"
+C_ALPHA = 0.08
+C_KERNELS = ["k_cderiv", "k_fft_xy_fwd_c", "k_fft_z_c", "k_fft_xy_bwd_sums_c",
+             "k_cprobe", "k_cupdate", "k_cscalar"]
+
+
+def _cparams():
+    p = _params("fp64")
+    p.gf_alpha = C_ALPHA
+    return p
+
+
+def coulomb_steps_record(dims):
+    """Slice steps (iterations + one SD start per slice) of a full Coulomb
+    fix of this workload, recorded from a GPU run (the per-slice iteration
+    counts of the GPU path follow the reference's within a few)."""
+    f = ROOT / "profiles" / "coulomb_full_fix.json"
+    if f.exists():
+        for e in json.loads(f.read_text()):
+            if tuple(e["dims"]) == tuple(dims):
+                return int(e["slice_steps"]), e
+    return None, None
+
+
+def coulomb_cpu_sample(U2, dims, nthreads, k=3):
+    """Seconds per slice step of GLU's Coulomb_FA (oracle/_ref) on the
+    host cores: a 2-slice lattice of the same spatial extent, k iterations
+    per run at an unreachable accuracy, so each slice runs 1 + 8 restarts of
+    (1 SD start + k CG steps)."""
+    from oracle.oracle import REF_SO, Reference
+    if not REF_SO.exists():
+        raise RuntimeError("oracle/_ref (the reference build) is not present")
+    d2 = (dims[0], dims[1], dims[2], 2)
+    R = Reference()
+    R.setup(d2, nthreads, C_ALPHA)
+    R.put_links(U2)
+    t = time.perf_counter()
+    it = R.coulomb_fa(1e-30, k, "FACG")["iters"]
+    el = time.perf_counter() - t
+    steps = it + 2 * 9  # + one SD start per run
+    return dict(kind="reference", cores=nthreads, s_step=el / steps,
+                steps=steps, seconds=el)
+
+
+def coulomb_gpu(args, dims, rank, world, local):
+    import ctypes as C
+    import torch
+    torch.cuda.set_device(local)
+    from glu_b200 import _lib
+    from glu_b200._lib import GfixResult, check
+    from glu_b200.workload import tiled_config_device
+    lib = _lib.load()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    U = tiled_config_device(dims, seed=4 + rank)
+    dpristine = torch.view_as_real(U).reshape(-1).contiguous()
+    del U
+    dwork = torch.empty_like(dpristine)
+    hwork = torch.empty(dpristine.shape, dtype=torch.float64, pin_memory=True)
+    cd = (C.c_size_t * 4)(*dims)
+    V = int(np.prod(dims))
+    T = dims[3]
+    sth = np.zeros(T)
+    sit = np.zeros(T, dtype=np.uintp)
+
+    def fix(ptr, device):
+        r = GfixResult()
+        p = _cparams()
+        fn = lib.gfix_coulomb_device if device else lib.gfix_coulomb
+        check(fn(ptr, cd, C.byref(p), C.byref(r),
+                 sth.ctypes.data_as(C.POINTER(C.c_double)),
+                 sit.ctypes.data_as(C.POINTER(C.c_size_t))))
+        return r
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    with Clocks(local) as clk:
+        for _ in range(args.warmup):
+            dwork.copy_(dpristine)
+            fix(dwork.data_ptr(), True)
+        ms = 0.0
+        launches0 = lib.gfix_kernel_launches()
+        iters = []
+        for _ in range(args.steps):
+            # the pristine copy is refreshed outside the timed region
+            dwork.copy_(dpristine)
+            barrier()
+            a, b = ev(), ev()
+            a.record()
+            r = fix(dwork.data_ptr(), True)
+            b.record()
+            barrier()
+            ms += a.elapsed_time(b)
+            iters.append(int(r.iters))
+        launches = lib.gfix_kernel_launches() - launches0
+        ms = max_over_ranks(ms)
+        e_ms = 0.0
+        for _ in range(args.steps):
+            hwork.copy_(dpristine)
+            barrier()
+            a, b = ev(), ev()
+            a.record()
+            fix(hwork.data_ptr(), False)
+            b.record()
+            torch.cuda.synchronize()
+            e_ms += a.elapsed_time(b)
+        e_ms = max_over_ranks(e_ms)
+    slice_iters = sit.astype(np.int64).copy()
+    pm = np.zeros(7)
+    pb = np.zeros(7)
+    check(lib.gfix_profile_coulomb(dpristine.data_ptr(), cd, C.byref(_cparams()),
+                                   args.profile_iters,
+                                   pm.ctypes.data_as(C.POINTER(C.c_double)),
+                                   pb.ctypes.data_as(C.POINTER(C.c_double))))
+    U2 = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the first two slices of the input, for the host sample
+        U2 = torch.view_as_complex(
+            dpristine[: 2 * V // T * 72].reshape(-1, 2)).reshape(-1, 4, 3, 3).cpu().numpy()
+    if dist is not None:
+        dist.destroy_process_group()
+    return dict(ms=ms, e2e_ms=e_ms, iters=iters, theta=float(np.max(sth)),
+                slice_iters=slice_iters, launches=launches,
+                clocks=clk.summary(), prof=(pm, pb), V=V), U2
+
+
+def coulomb_line(args, dims, world, res, cpu):
+    steps = args.steps
+    peak, peak_src = peaks()
+    pm, pb = res["prof"]
+    k = int(np.argmax(pm[:6]))
+    achieved = pb[k] / (pm[k] * 1e-3) / 1e9
+    traffic = traffic_from_profiles(C_KERNELS[k], "fp64", dims)
+    V = res["V"]
+    return {
+        "metric": C_METRIC, "value": world * steps * 3600e3 / res["ms"],
+        "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": res["ms"] / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled + seeded random gauge transform, on device)",
+        "config": {"workload": "Coulomb FACG theta<1e-14 per slice, %s" % "x".join(map(str, dims)),
+                   "dims": list(dims), "gf_alpha": C_ALPHA, "accuracy": ACC,
+                   "precision": "fp64", "iters": res["iters"][-1],
+                   "slice_iters_min_max": [int(res["slice_iters"].min()),
+                                           int(res["slice_iters"].max())],
+                   "slice_steps": int(res["slice_iters"].sum() + dims[3]),
+                   "final_theta_max": res["theta"],
+                   "l2": "inputs (%.2f GB of links) larger than the 126 MB L2" % (V * 576 / 1e9),
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "e2e": {"value": world * steps * 3600e3 / res["e2e_ms"], "unit": UNIT,
+                "h2d_bytes_per_step": V * 576, "d2h_bytes_per_step": V * 576},
+        "roofline": {"bound": "hbm", "kernel": C_KERNELS[k] + " (fp64)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src,
+                     "traffic": traffic, "algorithmic_bytes": pb[k],
+                     "per_kernel": {C_KERNELS[j]: {"ms": round(pm[j], 5),
+                                                   "GB/s": round(pb[j] / (pm[j] * 1e-3) / 1e9, 1) if pb[j] else None}
+                                    for j in range(7)}},
+        "gpu_launches": res["launches"],
+        "clocks": res["clocks"],
+        **({"cpu_baseline": cpu} if cpu else {}),
+    }
+
+
+def coulomb_profile_only(args, dims):
+    import ctypes as C
+    import torch
+    from glu_b200 import _lib
+    from glu_b200._lib import check
+    from glu_b200.workload import tiled_config_device
+    lib = _lib.load()
+    d = torch.view_as_real(tiled_config_device(dims, seed=4)).reshape(-1).contiguous()
+    cd = (C.c_size_t * 4)(*dims)
+    ms = np.zeros(7)
+    by = np.zeros(7)
+    check(lib.gfix_profile_coulomb(d.data_ptr(), cd, C.byref(_cparams()),
+                                   args.profile_iters,
+                                   ms.ctypes.data_as(C.POINTER(C.c_double)),
+                                   by.ctypes.data_as(C.POINTER(C.c_double))))
+    emit({"profile": "coulomb fp64", "dims": list(dims), "iters": args.profile_iters,
+          "kernels": {C_KERNELS[k]: {"ms": ms[k], "bytes": by[k],
+                                     "GB/s": by[k] / (ms[k] * 1e-3) / 1e9 if ms[k] else None}
+                      for k in range(7)}})
+
+
+def coulomb_main(args, dims, rank, world, local):
+    if args.profile_only:
+        coulomb_profile_only(args, dims)
+        return
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        n_steps, _ = coulomb_steps_record(dims)
+        if n_steps is None:
+            emit({"impl": "reference", "unavailable":
+                  "no recorded slice-step count of a full Coulomb fix for dims %s" % (dims,)})
+            return
+        from glu_b200.workload import tiled_config_device
+        U = tiled_config_device((dims[0], dims[1], dims[2], 8), seed=4, device="cpu")
+        U2 = U[: 2 * dims[0] * dims[1] * dims[2]].numpy()
+        cores = os.cpu_count() or 1
+        samples = [coulomb_cpu_sample(U2, dims, cores) for _ in range(max(args.steps, 1))]
+        s_step = statistics.median(x["s_step"] for x in samples)
+        t_fix = s_step * n_steps
+        value = 3600.0 / t_fix
+        emit({"metric": C_METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+              "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_fix * 1e3,
+              "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+              "dtype": "f64", "data": "synthetic (8^4 GLU heatbath tiled + random gauge)",
+              "config": {"workload": "Coulomb FACG theta<1e-14 per slice, %s" % "x".join(map(str, dims)),
+                         "dims": list(dims), "slice_steps": n_steps,
+                         "parallelism": "host OpenMP"},
+              "impl": "reference",
+              "cpu_baseline": {"value": value, "unit": UNIT, "cores": samples[0]["cores"],
+                               "kind": "reference",
+                               "sample": "%d x %d slice steps of a 2-slice %dx%dx%d lattice; "
+                                         "%.3f s/slice step x %d slice steps"
+                                         % (len(samples), samples[0]["steps"], dims[0], dims[1],
+                                            dims[2], s_step, n_steps)},
+              "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                      "d2h_bytes_per_step": 0}})
+        return
+    res, U2 = coulomb_gpu(args, dims, rank, world, local)
+    cpu = None
+    if U2 is not None:
+        try:
+            s = coulomb_cpu_sample(U2, dims, os.cpu_count() or 1)
+            n_steps = int(res["slice_iters"].sum() + dims[3])
+            t_fix = s["s_step"] * n_steps
+            cpu = {"value": 3600.0 / t_fix, "unit": UNIT, "cores": s["cores"],
+                   "kind": s["kind"],
+                   "sample": "%d slice steps of a 2-slice %dx%dx%d lattice (%.1f s); "
+                             "%.3f s/slice step x %d slice steps of the full fix"
+                             % (s["steps"], dims[0], dims[1], dims[2], s["seconds"],
+                                s["s_step"], n_steps)}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "kind": "unavailable", "sample": str(e)}
+    if rank == 0:
+        emit(coulomb_line(args, dims, world, res, cpu))
+
+
 def main():
     args = parse()
+    if args.dims is None:
+        args.dims = "32,32,32,64" if args.workload == "landau" else "64,64,64,128"
     dims = tuple(int(x) for x in args.dims.split(","))
     rank, world, local = dist_env()
+    if args.workload == "coulomb":
+        coulomb_main(args, dims, rank, world, local)
+        return
     if args.profile_only:
         profile_only(args, dims)
         return

@@ -34,7 +34,8 @@ EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
            "Coulomb_FA", "FOURIER_ACCELERATE2", "gfix_landau",
            "gfix_landau_device", "gfix_coulomb", "gfix_coulomb_device",
            "gfix_observables", "gfix_reunit", "gfix_fourier_accelerate",
-           "gfix_profile_landau", "gfix_theta_functional_noalloc",
+           "gfix_profile_landau", "gfix_profile_coulomb",
+           "gfix_theta_functional_noalloc",
            "gfix_noalloc_error",
            "gfix_last_error", "gfix_release", "gfix_kernel_launches")
 
@@ -71,6 +72,9 @@ def load(path: Path | str | None = None):
     lib.gfix_reunit.argtypes = [C.c_void_p, _szp]
     lib.gfix_fourier_accelerate.restype = C.c_int
     lib.gfix_fourier_accelerate.argtypes = [C.c_void_p, _szp, C.c_int]
+    lib.gfix_profile_coulomb.restype = C.c_int
+    lib.gfix_profile_coulomb.argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
+                                         C.c_int, _dp, _dp]
     lib.gfix_profile_landau.restype = C.c_int
     lib.gfix_profile_landau.argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
                                         C.c_int, _dp, _dp]

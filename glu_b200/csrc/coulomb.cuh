@@ -49,6 +49,7 @@ struct CoulState {
   unsigned long long seed;
   int traj_cap;       // per slice
   double *traj;       // [nslices][traj_cap]
+  int *done_mask;     // [nslices], 1 once a slice has finished (FFT passes skip it)
 };
 
 template <typename R>
@@ -65,21 +66,43 @@ struct CCtx {
   int V, Lcu, nbs;
 };
 
-__device__ __forceinline__ void coul_coords(int i, const int *L, int *x) {
-  x[0] = i % L[0];
-  i /= L[0];
-  x[1] = i % L[1];
-  x[2] = i / L[1];
+// slice-site coordinates and the in-slice neighbours of site i in direction
+// MU (compile-time, so no index array lands in local memory)
+struct SliceSite {
+  int i, x[3];
+};
+__device__ __forceinline__ SliceSite slice_site(int i, const int *L) {
+  SliceSite q;
+  q.i = i;
+  q.x[0] = i % L[0];
+  const int r = i / L[0];
+  q.x[1] = r % L[1];
+  q.x[2] = r / L[1];
+  return q;
+}
+template <int MU>
+__device__ __forceinline__ int sfwd(const SliceSite &q, const int *L) {
+  const int sd = MU == 0 ? 1 : MU == 1 ? L[0] : L[0] * L[1];
+  return q.x[MU] == L[MU] - 1 ? q.i - (L[MU] - 1) * sd : q.i + sd;
+}
+// the same with a run-time direction, by selects
+__device__ __forceinline__ int sfwd_rt(const SliceSite &q, const int *L, int mu) {
+  const int xm = mu == 0 ? q.x[0] : mu == 1 ? q.x[1] : q.x[2];
+  const int lm = mu == 0 ? L[0] : mu == 1 ? L[1] : L[2];
+  const int sd = mu == 0 ? 1 : mu == 1 ? L[0] : L[0] * L[1];
+  return xm == lm - 1 ? q.i - (lm - 1) * sd : q.i + sd;
+}
+template <int MU>
+__device__ __forceinline__ int sbck(const SliceSite &q, const int *L) {
+  const int sd = MU == 0 ? 1 : MU == 1 ? L[0] : L[0] * L[1];
+  return q.x[MU] == 0 ? q.i + (L[MU] - 1) * sd : q.i - sd;
 }
 
-// in-slice forward / backward neighbour of slice site i in direction mu < 3
-__device__ __forceinline__ int sfwd(int i, int mu, const int *x, const int *L,
-                                    const int *sd) {
-  return x[mu] == L[mu] - 1 ? i - (L[mu] - 1) * sd[mu] : i + sd[mu];
-}
-__device__ __forceinline__ int sbck(int i, int mu, const int *x, const int *L,
-                                    const int *sd) {
-  return x[mu] == 0 ? i + (L[mu] - 1) * sd[mu] : i - sd[mu];
+// buffer of a ping-pong pair by parity, as a select (a runtime index into
+// the by-value kernel parameter would copy it to local memory)
+template <typename T>
+__device__ __forceinline__ T *pick(T *const (&b)[2], int p) {
+  return p ? b[1] : b[0];
 }
 
 template <typename R>
@@ -104,39 +127,55 @@ __device__ __forceinline__ void rotated(const CCtx<R> &c, int mu, int s_link,
   gtransform(A, C, B);
 }
 
+// Hermitian short form of the rotated link (5 entries)
+template <typename R>
+struct HShort {
+  R h0, h3;
+  cx<R> h1, h2, h4;
+};
+template <typename R>
+__device__ __forceinline__ HShort<R> rotated_herm(const CCtx<R> &c, int mu,
+                                                  int s_link, int sa, int sb) {
+  cx<R> C[9];
+  rotated(c, mu, s_link, sa, sb, C);
+  HShort<R> h;
+  herm_short(C, h.h0, h.h1, h.h2, h.h3, h.h4);
+  return h;
+}
+
 // ---------------------------------------------------------------------
 // derivative on the rotated links, packed like the Landau fields
 // (steep_deriv_CG, src/Gfix/CFACG.c:91-163)
+template <typename R, int MU>
+__device__ __forceinline__ void cderiv_dir(const CCtx<R> &c, const SliceSite &q,
+                                           int off, R &s0, cx<R> &s1, cx<R> &s2,
+                                           R &s3, cx<R> &s4) {
+  const int it = sfwd<MU>(q, c.L), bk = sbck<MU>(q, c.L);
+  // g(i) U(i) g(i+mu)^dag and g(i-mu) U(i-mu) g(i)^dag
+  const HShort<R> b = rotated_herm(c, MU, off + q.i, off + q.i, off + it);
+  const HShort<R> a = rotated_herm(c, MU, off + bk, off + bk, off + q.i);
+  s0 += a.h0 - b.h0;
+  s1 = cadd(s1, csub(a.h1, b.h1));
+  s2 = cadd(s2, csub(a.h2, b.h2));
+  s3 += a.h3 - b.h3;
+  s4 = cadd(s4, csub(a.h4, b.h4));
+}
+
 template <typename R>
-__global__ void __launch_bounds__(kCoulThreads) k_cderiv(CCtx<R> c) {
+__global__ void __launch_bounds__(kCoulThreads, 4) k_cderiv(CCtx<R> c) {
   const int t = blockIdx.y;
   if (c.sl[t].mode == SL_DONE) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;  // in-slice site
   if (i >= c.Lcu) return;
-  int x[3];
-  coul_coords(i, c.L, x);
-  const int sd[3] = {1, c.L[0], c.L[0] * c.L[1]};
+  const SliceSite q = slice_site(i, c.L);
   const int off = t * c.Lcu;
   R s0 = 0, s3 = 0;
   cx<R> s1 = mk<R>(0, 0), s2 = mk<R>(0, 0), s4 = mk<R>(0, 0);
-#pragma unroll 1
-  for (int mu = 0; mu < 3; mu++) {
-    const int it = sfwd(i, mu, x, c.L, sd), bk = sbck(i, mu, x, c.L, sd);
-    cx<R> C[9], D[9];
-    rotated(c, mu, off + i, off + i, off + it, C);   // g(i) U(i) g(i+mu)^dag
-    rotated(c, mu, off + bk, off + bk, off + i, D);  // g(i-mu) U(i-mu) g(i)^dag
-    R b0, b3, a0, a3;
-    cx<R> b1, b2, b4, a1, a2, a4;
-    herm_short(C, b0, b1, b2, b3, b4);
-    herm_short(D, a0, a1, a2, a3, a4);
-    s0 += a0 - b0;
-    s1 = cadd(s1, csub(a1, b1));
-    s2 = cadd(s2, csub(a2, b2));
-    s3 += a3 - b3;
-    s4 = cadd(s4, csub(a4, b4));
-  }
+  cderiv_dir<R, 0>(c, q, off, s0, s1, s2, s3, s4);
+  cderiv_dir<R, 1>(c, q, off, s0, s1, s2, s3, s4);
+  cderiv_dir<R, 2>(c, q, off, s0, s1, s2, s3, s4);
   // pack: in0 = i Re s0 - Re s3, in_k = i Re s_k - Im s_k (CFACG.c:144-150)
-  cx<R> *f = c.fb[c.st->parity];
+  cx<R> *f = pick(c.fb, c.st->parity);
   const size_t V = c.V, s = off + i;
   f[s] = mk<R>(-s3, s0);
   f[V + s] = mk<R>(-s1.y, s1.x);
@@ -144,37 +183,10 @@ __global__ void __launch_bounds__(kCoulThreads) k_cderiv(CCtx<R> c) {
   f[3 * V + s] = mk<R>(-s4.y, s4.x);
 }
 
-// sums of the accelerated field: insum (sum_PR / sum_DER2 form, both the
-// same 2 (r^2 + i^2 + r i) + 2 |.|^2 norm) and sum_conj
-// (src/Gfix/CFACG.c:165-258), per slice
-template <typename R>
-__global__ void __launch_bounds__(kCoulThreads) k_csums(CCtx<R> c) {
-  const int t = blockIdx.y;
-  double v[2] = {0.0, 0.0};
-  const bool live = c.sl[t].mode != SL_DONE;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (live && i < c.Lcu) {
-    const int par = c.st->parity;
-    const cx<R> *in = c.fb[par], *old = c.fb[par ^ 1];
-    const size_t V = c.V, s = (size_t)t * c.Lcu + i;
-    const bool cg = !c.sl[t].sd;
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const double a = in[k * V + s].x, b = in[k * V + s].y;
-      double l1 = a * a + b * b, l2 = 0.0;
-      if (k == 0) l1 += a * b;
-      if (cg) {
-        const double tr = a - (double)old[k * V + s].x,
-                     ti = b - (double)old[k * V + s].y;
-        l2 = 2.0 * (a * tr + b * ti);
-        if (k == 0) l2 += a * ti + b * tr;
-      }
-      v[0] += 2.0 * l1;
-      v[1] += l2;
-    }
-  }
-  block_sum_store<2>(v, c.part + 2 * ((size_t)t * c.nbs + blockIdx.x));
-}
+// The sums of the accelerated field, insum (sum_DER2 / sum_PR, one norm) and
+// sum_conj (src/Gfix/CFACG.c:165-258), come from the inverse xy FFT pass
+// (prsum = 1): its per-plane partials of slice t are the planes
+// t Lz .. t Lz + Lz - 1 of each of the 4 fields.
 
 // sn = in + beta sn_old at site s (the same fma form as the Landau kernels);
 // an SD step takes sn = in without reading sn_old
@@ -193,13 +205,35 @@ __device__ __forceinline__ void cdir(const cx<R> *in, const cx<R> *so, R beta,
   }
 }
 
-// direction sn = in + beta_t sn_old (beta_t = 0 on SD steps, so sn = in),
-// written for every live slice, and the line-search probes of
-// line_search_Coulomb (src/Gfix/line_search.c:141-271) at 0.17 and 0.34 as
-// differences to the alpha = 0 value; each link counted once (forward links
-// of every site, the same set the reference's draughtboard visits)
+// one link of the line-search probes: Re tr(A C B^dag) - Re tr C with C the
+// rotated link and B the probe gauge matrix at the forward neighbour
 template <typename R>
-__global__ void __launch_bounds__(kCoulThreads) k_cprobe(CCtx<R> c) {
+__device__ __forceinline__ double cprobe_dir(const CCtx<R> &c, const SliceSite &q,
+                                             int mu, int off, const cx<R> *in,
+                                             const cx<R> *so, R beta, bool sdstep,
+                                             const cx<double> *A, double al) {
+  auto up = [](cx<R> a) { return mk<double>((double)a.x, (double)a.y); };
+  const int it = sfwd_rt(q, c.L, mu);
+  cx<double> Cd[9], Bm[9];
+  {
+    cx<R> C[9];
+    rotated(c, mu, off + q.i, off + q.i, off + it, C);
+#pragma unroll
+    for (int e = 0; e < 9; e++) Cd[e] = up(C[e]);
+  }
+  cx<R> fy[4];
+  cdir(in, so, beta, sdstep, (size_t)off + it, (size_t)c.V, fy);
+  set_gauge(Bm, up(fy[0]), up(fy[1]), up(fy[2]), up(fy[3]), al);
+  return re_tr_abc_dag(A, Cd, Bm) - (Cd[0].x + Cd[4].x + Cd[8].x);
+}
+
+// direction sn = in + beta_t sn_old (an SD step takes sn = in), written for
+// every live slice, and the line-search probes of line_search_Coulomb
+// (src/Gfix/line_search.c:141-271) at 0.17 and 0.34 as differences to the
+// alpha = 0 value; each link counted once (the forward links of every site,
+// the same set the reference's draughtboard visits)
+template <typename R>
+__global__ void __launch_bounds__(kCoulThreads, 3) k_cprobe(CCtx<R> c) {
   const int t = blockIdx.y;
   double v[2] = {0.0, 0.0};
   const Slice &S = c.sl[t];
@@ -208,8 +242,8 @@ __global__ void __launch_bounds__(kCoulThreads) k_cprobe(CCtx<R> c) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (live && i < c.Lcu) {
     const int par = c.st->parity, spar = c.st->sparity;
-    const cx<R> *in = c.fb[par], *so = c.sb[spar];
-    cx<R> *sn = c.sb[spar ^ 1];
+    const cx<R> *in = pick(c.fb, par), *so = pick(c.sb, spar);
+    cx<R> *sn = pick(c.sb, spar ^ 1);
     const R beta = (R)S.beta;
     const bool sdstep = S.sd != 0;
     const int off = t * c.Lcu;
@@ -218,31 +252,19 @@ __global__ void __launch_bounds__(kCoulThreads) k_cprobe(CCtx<R> c) {
 #pragma unroll
     for (int k = 0; k < 4; k++) sn[(size_t)k * c.V + off + i] = f[k];
     if (probes) {
-      int x[3];
-      coul_coords(i, c.L, x);
-      const int sd[3] = {1, c.L[0], c.L[0] * c.L[1]};
+      const SliceSite q = slice_site(i, c.L);
       auto up = [](cx<R> a) { return mk<double>((double)a.x, (double)a.y); };
-      double d[2] = {0.0, 0.0};
 #pragma unroll 1
       for (int k = 0; k < 2; k++) {
         const double al = k == 0 ? 0.17 : 0.34;
-        cx<double> A[9], Bm[9], Cd[9];
+        cx<double> A[9];
         set_gauge(A, up(f[0]), up(f[1]), up(f[2]), up(f[3]), al);
+        double d = 0.0;
 #pragma unroll 1
-        for (int mu = 0; mu < 3; mu++) {
-          const int it = sfwd(i, mu, x, c.L, sd);
-          cx<R> C[9], fy[4];
-          rotated(c, mu, off + i, off + i, off + it, C);
-          cdir(in, so, beta, sdstep, (size_t)off + it, (size_t)c.V, fy);
-#pragma unroll
-          for (int e = 0; e < 9; e++) Cd[e] = up(C[e]);
-          const double t0 = Cd[0].x + Cd[4].x + Cd[8].x;
-          set_gauge(Bm, up(fy[0]), up(fy[1]), up(fy[2]), up(fy[3]), al);
-          d[k] += re_tr_abc_dag(A, Cd, Bm) - t0;
-        }
+        for (int mu = 0; mu < 3; mu++)
+          d += cprobe_dir<R>(c, q, mu, off, in, so, beta, sdstep, A, al);
+        v[k] = d;
       }
-      v[0] = d[0];
-      v[1] = d[1];
     }
   }
   if (probes) block_sum_store<2>(v, c.part + 2 * ((size_t)t * c.nbs + blockIdx.x));
@@ -258,7 +280,7 @@ __global__ void __launch_bounds__(kCoulThreads) k_cupdate(CCtx<R> c) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.Lcu) return;
   const size_t V = c.V, s = (size_t)t * c.Lcu + i;
-  const cx<R> *d = c.sb[c.st->sparity ^ 1];
+  const cx<R> *d = pick(c.sb, c.st->sparity ^ 1);
   cx<R> A[9], G[9], r[9];
   set_gauge(A, d[s], d[V + s], d[2 * V + s], d[3 * V + s], (R)S.alpha);
   load9(c.g, c.V, (int)s, G);
@@ -318,14 +340,25 @@ enum CoulOp : int { C_SUMS = 0, C_PROBES = 1, C_END1 = 2, C_END2 = 3 };
 // one thread per slice: fixed-order sums of the slice's partials and GLU's
 // control flow of steep_step_FACG / _FASD and steep_fix
 // (src/Gfix/CFACG.c:285-529)
+// Partials: C_SUMS reads the inverse xy FFT pass's per-plane pairs (plane
+// index field * nplanes + t * lz + z), C_PROBES the probe kernel's per-block
+// pairs (t * nbs + block).
 __global__ void k_cscalar(CoulState *cs, Slice *sl, const double *part,
-                          int nbs, int op, double Lcu, DevState *st) {
+                          int nbs, int lz, int nplanes, int op, double Lcu,
+                          DevState *st) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t < cs->nslices) {
     Slice &S = sl[t];
     if (S.mode != SL_DONE) {
       double a0 = 0.0, a1 = 0.0;
-      if (op == C_SUMS || op == C_PROBES) {
+      if (op == C_SUMS) {
+        for (int f = 0; f < 4; f++)
+          for (int z = 0; z < lz; z++) {
+            const size_t b = (size_t)f * nplanes + (size_t)t * lz + z;
+            a0 += part[2 * b];
+            a1 += part[2 * b + 1];
+          }
+      } else if (op == C_PROBES) {
         for (int b = 0; b < nbs; b++) {
           a0 += part[2 * ((size_t)t * nbs + b)];
           a1 += part[2 * ((size_t)t * nbs + b) + 1];
@@ -402,6 +435,7 @@ __global__ void k_cscalar(CoulState *cs, Slice *sl, const double *part,
           S.tot += loc;
           S.iter = loc;
           S.mode = SL_DONE;
+          cs->done_mask[t] = 1;
           // the slice that ends last stops the whole sequence
           if (atomicSub(&cs->active, 1) == 1) st->done = 1;
           break;
@@ -414,24 +448,30 @@ __global__ void k_cscalar(CoulState *cs, Slice *sl, const double *part,
 // the slice transforms of Coulomb_FA (gtransform_slice, src/Gfix/gtrans.c:
 // 214-238): U_i(x,t) <- g_t(x) U_i(x,t) g_t(x+i)^dag for i < 3 and
 // U_t(x,t) <- g_t(x) U_t(x,t) g_{t+1}(x)^dag, periodic in t
+template <typename R, int MU>
+__device__ __forceinline__ void cslice_link(const CCtx<R> &c, const SliceSite &q,
+                                            int s, int t, const cx<R> *A) {
+  const int nb = MU < 3 ? t * c.Lcu + sfwd<(MU < 3 ? MU : 0)>(q, c.L)
+                        : ((t + 1) % c.L[3]) * c.Lcu + q.i;
+  cx<R> B[9], U[9];
+  load9(c.g, c.V, nb, B);
+  load_link(c.U, c.V, MU, s, U);
+  gtransform(A, U, B);
+  store_link(c.U, c.V, MU, s, U);
+}
+
 template <typename R>
 __global__ void __launch_bounds__(kCoulThreads) k_cslice_transform(CCtx<R> c) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= c.V) return;
-  const int t = s / c.Lcu, i = s - t * c.Lcu;
-  int x[3];
-  coul_coords(i, c.L, x);
-  const int sd[3] = {1, c.L[0], c.L[0] * c.L[1]};
-  cx<R> A[9], B[9], U[9];
+  const int t = s / c.Lcu;
+  const SliceSite q = slice_site(s - t * c.Lcu, c.L);
+  cx<R> A[9];
   load9(c.g, c.V, s, A);
-  for (int mu = 0; mu < 4; mu++) {
-    const int nb = mu < 3 ? t * c.Lcu + sfwd(i, mu, x, c.L, sd)
-                          : ((t + 1) % c.L[3]) * c.Lcu + i;
-    load9(c.g, c.V, nb, B);
-    load_link(c.U, c.V, mu, s, U);
-    gtransform(A, U, B);
-    store_link(c.U, c.V, mu, s, U);
-  }
+  cslice_link<R, 0>(c, q, s, t, A);
+  cslice_link<R, 1>(c, q, s, t, A);
+  cslice_link<R, 2>(c, q, s, t, A);
+  cslice_link<R, 3>(c, q, s, t, A);
 }
 
 // in / in_old and sn ping-pong after every step of every live slice

@@ -19,6 +19,9 @@ __host__ __device__ constexpr bool ct_ok(int n) {
 
 // Stockham stages for pencils of length N; pencil p starts at
 // (p / PIN) * PSHI + (p % PIN) * PSLO, elements are JS apart; BD threads.
+// Consecutive threads take consecutive pencils at the same butterfly index:
+// their elements are neighbours in shared memory (no bank conflicts for the
+// tile layouts below) and they share one twiddle factor (a broadcast).
 template <typename R, int N, int Ns, int NP, int PIN, int PSLO, int PSHI,
           int JS, int BD>
 __device__ __forceinline__ void ct_stages(cx<R> *buf, const cx<R> *tw,
@@ -36,7 +39,7 @@ __device__ __forceinline__ void ct_stages(cx<R> *buf, const cx<R> *tw,
       const int idx = threadIdx.x + k * BD;
       dst[k] = -1;
       if (TOTAL % BD == 0 || idx < TOTAL) {
-        const int p = idx / NB, j = idx % NB;
+        const int p = idx % NP, j = idx / NP;
         const int po = (p / PIN) * PSHI + (p % PIN) * PSLO;
         const int jq = j / Ns, jm = j % Ns;
 #pragma unroll
@@ -63,12 +66,21 @@ __device__ __forceinline__ void ct_stages(cx<R> *buf, const cx<R> *tw,
 }
 
 __host__ __device__ constexpr int ct_threads(int n) { return n / 8 < 32 ? 32 : n / 8; }
+// resident blocks asked of the compiler: 1024 threads per SM at least
+__host__ __device__ constexpr int ct_minb(int n) {
+  return 1024 / ct_threads(n) < 1 ? 1 : 1024 / ct_threads(n);
+}
+// padding of the t-stride of a zt tile of B x columns: t-planes start B
+// elements apart modulo 8, so the z-stage pencils of 8 (FP64) or 16 (FP32)
+// consecutive threads fall in distinct banks
+__host__ __device__ constexpr int zt_pad(int b) { return b < 16 ? b : 0; }
 
 // xy-plane pass with compile-time extents (see k_fft_xy)
 template <typename R, int LX, int LY>
-__global__ void __launch_bounds__(ct_threads(LX *LY))
+__global__ void __launch_bounds__(ct_threads(LX *LY), ct_minb(LX *LY))
     k_fft_xy_ct(Ctx<R> c, int bwd, int prsum) {
   if (c.st->done) return;
+  if (c.skip && c.skip[blockIdx.x / c.L[2]]) return;  // finished slice
   constexpr int P = LX + 1, N = LX * LY, BD = ct_threads(N);
   constexpr int EPT = (N + BD - 1) / BD;
   extern __shared__ unsigned char smem_raw[];
@@ -120,11 +132,13 @@ __global__ void __launch_bounds__(ct_threads(LX *LY))
 // z(,t) pass with compile-time extents (see k_fft_zt).  NT = Lt for Landau
 // (z and t transformed); NT = 1 for Coulomb (z only, one slice per tile).
 template <typename R, int LZ, int NT, int B>
-__global__ void __launch_bounds__(ct_threads(B *LZ *NT))
+__global__ void __launch_bounds__(ct_threads(B *LZ *NT), ct_minb(B *LZ *NT))
     k_fft_zt_ct(Ctx<R> c) {
   if (c.st->done) return;
+  if constexpr (NT == 1)
+    if (c.skip && c.skip[blockIdx.x / ((c.L[0] / B) * c.L[1])]) return;
   constexpr bool FOUR = NT > 1;
-  constexpr int TS = FOUR ? LZ * B + 1 : LZ * B;  // padded t-stride
+  constexpr int TS = FOUR ? LZ * B + zt_pad(B) : LZ * B;  // padded t-stride
   constexpr int N = B * LZ * NT, BD = ct_threads(N);
   constexpr int EPT = (N + BD - 1) / BD;
   extern __shared__ unsigned char smem_raw[];

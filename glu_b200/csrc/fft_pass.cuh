@@ -20,6 +20,7 @@ __device__ __forceinline__ void stage_twiddles(cx<R> *dst, const cx<R> *src,
 template <typename R, int PT, bool ODD>
 __global__ void __launch_bounds__(512, 2) k_fft_xy(Ctx<R> c, int bwd, int prsum) {
   if (c.st->done) return;
+  if (c.skip && c.skip[blockIdx.x / c.L[2]]) return;  // finished slice
   extern __shared__ unsigned char smem_raw[];
   __shared__ FftAxis s_ax[2];
   const int Lx = c.L[0], Ly = c.L[1], P = c.xy_pitch;
@@ -83,6 +84,7 @@ __global__ void __launch_bounds__(512, 2) k_fft_xy(Ctx<R> c, int bwd, int prsum)
 template <typename R, int PT, bool ODD>
 __global__ void __launch_bounds__(512, 2) k_fft_zt(Ctx<R> c) {
   if (c.st->done) return;
+  if (c.skip && c.skip[blockIdx.x / ((c.L[0] / c.zt_b) * c.L[1])]) return;
   extern __shared__ unsigned char smem_raw[];
   __shared__ FftAxis s_ax[2];
   const int Lx = c.L[0], Ly = c.L[1], Lz = c.L[2], Lt = c.L[3];

@@ -110,6 +110,8 @@ static ZtFn<R> ct_zt(int lz, int lt, int b) {
   GFIX_ZT(32, 32, 2) GFIX_ZT(32, 64, 2)
   GFIX_ZT(4, 1, 8) GFIX_ZT(8, 1, 8) GFIX_ZT(16, 1, 8) GFIX_ZT(24, 1, 8)
   GFIX_ZT(32, 1, 8) GFIX_ZT(48, 1, 8) GFIX_ZT(64, 1, 8)
+  GFIX_ZT(8, 1, 16) GFIX_ZT(16, 1, 16) GFIX_ZT(24, 1, 16) GFIX_ZT(32, 1, 16)
+  GFIX_ZT(48, 1, 16) GFIX_ZT(64, 1, 16)
 #undef GFIX_ZT
   return nullptr;
 }
@@ -161,6 +163,8 @@ class Engine {
     cudaFree(d_sl);
     cudaFreeHost(h_sl);
     cudaFree(d_ctraj);
+    cudaFree(d_cmask);
+    d_cmask = nullptr;
     d_cst = nullptr;
     d_sl = nullptr;
     cudaFree(d_st);
@@ -234,7 +238,7 @@ class Engine {
     c.xy_pitch = c.L[0] + 1;
     // x columns per zt tile: 2 (32-byte rows in FP64) for Landau's big
     // (z, t) tiles; Coulomb tiles hold one slice's z pencils only
-    const int want_b = coul ? 8 : 2;
+    const int want_b = coul ? 16 : 2;
     const int nt = coul ? 1 : c.L[3];
     c.zt_b = 1;
     for (int b = want_b; b >= 1; b--)
@@ -267,24 +271,31 @@ class Engine {
     bd_zt = (int)threads_for(n_zt, pt_zt);
     // tile (padded) plus the twiddle tables of its two axes
     sm_xy = ((size_t)c.xy_pitch * c.L[1] + c.L[0] + c.L[1]) * sizeof(cx<R>);
+    // (the t-stride padding covers the generic pass's 1 and zt_pad)
     sm_zt = coul ? ((size_t)c.zt_b * c.L[2] + c.L[2]) * sizeof(cx<R>)
-                 : ((size_t)(c.zt_b * c.L[2] + 1) * c.L[3] + c.L[2] + c.L[3]) *
-                       sizeof(cx<R>);
+                 : ((size_t)(c.zt_b * c.L[2] + std::max(1, zt_pad(c.zt_b))) *
+                        c.L[3] + c.L[2] + c.L[3]) * sizeof(cx<R>);
     // the dynamic shared-memory limit is an attribute of the function, not
     // of a launch: raise it once to the largest tile any engine can use
     if (set_smem_limits()) return -1;
     // compile-time specialised passes where the extents have one
     xy_ct = odd ? nullptr : ct_xy<R>(c.L[0], c.L[1]);
     zt_ct = odd ? nullptr : ct_zt<R>(c.L[2], nt, c.zt_b);
+    // the FFT passes live in shared memory: ask for the largest carveout so
+    // that several tiles are resident per SM
     if (xy_ct) {
       bd_xy = ct_threads(c.L[0] * c.L[1]);
       CK(cudaFuncSetAttribute(xy_ct, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)sm_xy));
+      CK(cudaFuncSetAttribute(xy_ct, cudaFuncAttributePreferredSharedMemoryCarveout,
+                              (int)cudaSharedmemCarveoutMaxShared));
     }
     if (zt_ct) {
       bd_zt = ct_threads(c.zt_b * c.L[2] * nt);
       CK(cudaFuncSetAttribute(zt_ct, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)sm_zt));
+      CK(cudaFuncSetAttribute(zt_ct, cudaFuncAttributePreferredSharedMemoryCarveout,
+                              (int)cudaSharedmemCarveoutMaxShared));
     }
     g_xy = dim3(V / (c.L[0] * c.L[1]), 4);
     g_zt = dim3((c.L[0] / c.zt_b) * c.L[1] * (coul ? c.L[3] : 1), 4);
@@ -334,18 +345,15 @@ class Engine {
     static bool done = false;
     if (done) return 0;
     const int lim = (8192 + 8192 / 8 + 1024) * (int)sizeof(cx<R>);
-    CK(cudaFuncSetAttribute(k_fft_xy<R, 8, false>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    CK(cudaFuncSetAttribute(k_fft_xy<R, 16, false>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    CK(cudaFuncSetAttribute(k_fft_xy<R, 16, true>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    CK(cudaFuncSetAttribute(k_fft_zt<R, 8, false>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    CK(cudaFuncSetAttribute(k_fft_zt<R, 16, false>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-    CK(cudaFuncSetAttribute(k_fft_zt<R, 16, true>,
-                            cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+    const void *fns[] = {
+        (const void *)k_fft_xy<R, 8, false>, (const void *)k_fft_xy<R, 16, false>,
+        (const void *)k_fft_xy<R, 16, true>, (const void *)k_fft_zt<R, 8, false>,
+        (const void *)k_fft_zt<R, 16, false>, (const void *)k_fft_zt<R, 16, true>};
+    for (const void *f : fns) {
+      CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+      CK(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                              (int)cudaSharedmemCarveoutMaxShared));
+    }
     done = true;
     return 0;
   }
@@ -681,6 +689,7 @@ class Engine {
   CoulState *d_cst = nullptr, *h_cst = nullptr;
   Slice *d_sl = nullptr, *h_sl = nullptr;
   double *d_ctraj = nullptr;
+  int *d_cmask = nullptr;
   size_t ctraj_alloc = 0;
   int nbs = 0;
   cudaGraphExec_t gx_coul = nullptr;
@@ -692,6 +701,8 @@ class Engine {
     CK(cudaMalloc(&d_cst, sizeof(CoulState)));
     CK(cudaMallocHost(&h_cst, sizeof(CoulState)));
     CK(cudaMalloc(&d_sl, sizeof(Slice) * T));
+    CK(cudaMalloc(&d_cmask, sizeof(int) * T));
+    c.skip = d_cmask;
     CK(cudaMallocHost(&h_sl, sizeof(Slice) * T));
     // per-slice partials: [T][nbs] pairs, next to the engine's own uses
     const size_t need = (size_t)T * nbs;
@@ -721,8 +732,8 @@ class Engine {
 
   void cscalar(int op) {
     const int T = c.L[3];
-    k_cscalar<<<(T + 127) / 128, 128, 0, s>>>(
-        d_cst, d_sl, d_part, nbs, op, (double)Lcu, d_st);
+    k_cscalar<<<(T + 127) / 128, 128, 0, s>>>(d_cst, d_sl, d_part, nbs, c.L[2],
+                                              c.L[2] * T, op, (double)Lcu, d_st);
     LAUNCHED(1);
   }
 
@@ -751,8 +762,7 @@ class Engine {
     k_cderiv<R><<<gs, kCoulThreads, 0, s>>>(cc);
     fft_xy(0, 0);
     fft_zt();
-    fft_xy(1, 0);
-    k_csums<R><<<gs, kCoulThreads, 0, s>>>(cc);
+    fft_xy(1, 1);  // with the per-plane sums of the accelerated field
     cscalar(C_SUMS);
     k_cprobe<R><<<gs, kCoulThreads, 0, s>>>(cc);
     cscalar(C_PROBES);
@@ -762,12 +772,12 @@ class Engine {
     cscalar(C_END2);
     k_cmaint<R><<<gs, kCoulThreads, 0, s>>>(cc, 1);
     k_cflip<<<1, 1, 0, s>>>(d_st);
-    LAUNCHED(7);
+    LAUNCHED(6);
   }
 
   // GLU's Coulomb_FA (src/Gfix/CFACG.c:531-636) on the resident links
-  int csolve(const Params &p, size_t *iters, double *slice_theta,
-             size_t *slice_iters, size_t *traj_len) {
+  // state of a new solve: every slice live, g = 1, fields zero
+  int cstart(const Params &p) {
     if (cinit()) return -1;
     const int T = c.L[3];
     const size_t per = p.traj_cap ? p.traj_cap / T : 0;
@@ -789,6 +799,8 @@ class Engine {
     cst.seed = 0x5DEECE66Dull;
     cst.traj_cap = (int)per;
     cst.traj = per ? d_ctraj : nullptr;
+    cst.done_mask = d_cmask;
+    CK(cudaMemsetAsync(d_cmask, 0, sizeof(int) * T, s));
     CK(cudaMemcpyAsync(d_cst, &cst, sizeof cst, cudaMemcpyHostToDevice, s));
     std::vector<Slice> sl(T);
     memset(sl.data(), 0, sizeof(Slice) * T);
@@ -801,11 +813,19 @@ class Engine {
     DevState st;
     memset(&st, 0, sizeof st);
     CK(cudaMemcpyAsync(d_st, &st, sizeof st, cudaMemcpyHostToDevice, s));
-    // sn starts at zero: SD steps use beta = 0 against it
-    CK(cudaMemsetAsync(c.sb[0], 0, (size_t)V * 8 * sizeof(cx<R>), s));
+    // in_old and sn start at zero (SD steps do not read them)
+    CK(cudaMemsetAsync(c.fb[0], 0, (size_t)V * 16 * sizeof(cx<R>), s));
     k_cinit<R><<<(V + 255) / 256, 256, 0, s>>>(cc);
     LAUNCHED(1);
-    const unsigned long long per_iter = 14;  // launches in citer()
+    return 0;
+  }
+
+  int csolve(const Params &p, size_t *iters, double *slice_theta,
+             size_t *slice_iters, size_t *traj_len) {
+    if (cstart(p)) return -1;
+    const int T = c.L[3];
+    const size_t per = p.traj_cap ? p.traj_cap / T : 0;
+    const unsigned long long per_iter = 13;  // launches in citer()
     int batch = 2;
     size_t guard = 0;
     const size_t limit = (p.max_iters + 2) * 9 * 64 + 1024;
@@ -853,6 +873,72 @@ class Engine {
           p.traj_theta[t * per + k] =
               (int)k < h_sl[t].traj_len ? h[t * per + k] : NAN;
       if (traj_len) *traj_len = per * T;
+    }
+    return 0;
+  }
+
+  // Measurement aid: n steps of every slice (none may finish: accuracy 0)
+  // with CUDA events between the launches; ms[k] = mean time of launch k:
+  // 0 derivative, 1 xy FFT forward, 2 z FFT with psq, 3 xy FFT inverse +
+  // sums, 4 direction + probes, 5 g update, 6 the scalar, housekeeping and
+  // parity launches of a step; bytes[k] = its algorithmic HBM bytes.
+  int profile_coul(const Params &p, int n, double *ms, double *bytes) {
+    Params q = p;
+    q.acc = 0.0;
+    q.max_iters = (size_t)n + 16;
+    q.traj_cap = 0;
+    if (cstart(q)) return -1;
+    const dim3 gs(nbs, c.L[3]);
+    std::vector<cudaEvent_t> ev(10);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int it = 0; it < n; it++) {
+      CK(cudaEventRecord(ev[0], s));
+      k_cderiv<R><<<gs, kCoulThreads, 0, s>>>(cc);
+      CK(cudaEventRecord(ev[1], s));
+      fft_xy(0, 0);
+      CK(cudaEventRecord(ev[2], s));
+      fft_zt();
+      CK(cudaEventRecord(ev[3], s));
+      fft_xy(1, 1);
+      CK(cudaEventRecord(ev[4], s));
+      cscalar(C_SUMS);
+      CK(cudaEventRecord(ev[5], s));
+      k_cprobe<R><<<gs, kCoulThreads, 0, s>>>(cc);
+      CK(cudaEventRecord(ev[6], s));
+      cscalar(C_PROBES);
+      CK(cudaEventRecord(ev[7], s));
+      k_cupdate<R><<<gs, kCoulThreads, 0, s>>>(cc);
+      CK(cudaEventRecord(ev[8], s));
+      cscalar(C_END1);
+      k_cmaint<R><<<gs, kCoulThreads, 0, s>>>(cc, 0);
+      cscalar(C_END2);
+      k_cmaint<R><<<gs, kCoulThreads, 0, s>>>(cc, 1);
+      k_cflip<<<1, 1, 0, s>>>(d_st);
+      CK(cudaEventRecord(ev[9], s));
+      LAUNCHED(6);
+      CK(cudaStreamSynchronize(s));
+      float t[9];
+      for (int k = 0; k < 9; k++) CK(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
+      acc[0] += t[0];
+      acc[1] += t[1];
+      acc[2] += t[2];
+      acc[3] += t[3];
+      acc[4] += t[5];
+      acc[5] += t[7];
+      acc[6] += t[4] + t[6] + t[8];
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    CK(cudaGetLastError());
+    const double B = sizeof(cx<R>) * (double)V;  // one complex per site
+    // derivative: 3 links, g, 4 fields out; FFT passes: 4 fields in and out
+    // (+ in_old for the sums); probes: in, sn_old, sn out, 3 links, g;
+    // update: sn, g in and out
+    const double b[7] = {(27 + 9 + 4) * B, 8 * B, 8 * B, 12 * B,
+                         (4 + 4 + 4 + 27 + 9) * B, (4 + 9 + 9) * B, 0.0};
+    for (int k = 0; k < 7; k++) {
+      ms[k] = acc[k] / n;
+      if (bytes) bytes[k] = b[k];
     }
     return 0;
   }
@@ -1222,6 +1308,20 @@ int gfix_coulomb(double *links, const size_t dims[4], const gfix_params *p,
   CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
   CK(cudaStreamSynchronize(e->s));
   return 0;
+}
+
+int gfix_profile_coulomb(const double *d_links, const size_t dims[4],
+                         const gfix_params *p, int iters, double *ms,
+                         double *bytes) {
+  if (check_params(dims, p)) return -1;
+  if (!d_links || !ms || iters < 1) return fail("bad profile arguments");
+  Engine<double> *e = engine_coul(dims);
+  if (!e) return -1;
+  const size_t n = (size_t)e->V * 36 * sizeof(double2);
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpyAsync(e->d_aos, d_links, n, cudaMemcpyDeviceToDevice, e->s));
+  if (e->from_aos(e->d_aos)) return -1;
+  return e->profile_coul(to_params(p), iters, ms, bytes);
 }
 
 int gfix_coulomb_device(double *d_links, const size_t dims[4],

@@ -96,6 +96,7 @@ struct Ctx {
   int xy_pitch;       // padded row pitch of the xy tile
   double maxp;        // MAX_LANDAU = 4 ND / V or MAX_COULOMB = 4 (ND-1)/Lcu
   FftAxis ax[4];
+  const int *skip;    // ndim 3: per-slice flags, set slices are not transformed
 };
 
 // ---------------------------------------------------------------------

@@ -57,3 +57,41 @@ def tiled_config(dims, seed: int = 2, transform: bool = True) -> np.ndarray:
         gfwd = np.roll(gd, -1, axis=axis[mu])
         out[..., mu, :, :] = np.matmul(np.matmul(g, Ug[..., mu, :, :]), gfwd)
     return np.ascontiguousarray(out.reshape(-1, 4, 3, 3))
+
+
+def _random_su3_torch(n: int, gen, device):
+    """random_su3 on the device (torch), same construction."""
+    import torch
+    z = torch.randn((n, 3, 2), dtype=torch.complex128, generator=gen,
+                    device=device)
+    c0 = z[:, :, 0] / torch.linalg.vector_norm(z[:, :, 0], dim=1, keepdim=True)
+    c1 = z[:, :, 1] - torch.sum(torch.conj(c0) * z[:, :, 1], dim=1,
+                                keepdim=True) * c0
+    c1 = c1 / torch.linalg.vector_norm(c1, dim=1, keepdim=True)
+    c2 = torch.conj(torch.linalg.cross(c0, c1, dim=1))
+    return torch.stack([c0, c1, c2], dim=2)
+
+
+def tiled_config_device(dims, seed: int = 4, device="cuda"):
+    """tiled_config built on the device (torch complex128, shape (V, 4, 3,
+    3)), for lattices whose host-side construction would need tens of GB of
+    host memory (64^3x128: 19.3 GB of links).  Seeded by a device generator:
+    reproducible on the same GPU model, not bit-equal to the host version."""
+    import torch
+    base, bd = base_config()
+    Lx, Ly, Lz, Lt = (int(d) for d in dims)
+    if any(L % b for L, b in zip((Lx, Ly, Lz, Lt), bd)):
+        raise ValueError(f"extents {dims} must be multiples of {bd}")
+    b = torch.from_numpy(base.reshape(bd[3], bd[2], bd[1], bd[0], 4, 3, 3)).to(device)
+    U = b.repeat(Lt // bd[3], Lz // bd[2], Ly // bd[1], Lx // bd[0], 1, 1, 1)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    V = Lx * Ly * Lz * Lt
+    g = _random_su3_torch(V, gen, device).reshape(Lt, Lz, Ly, Lx, 3, 3)
+    axis = {0: 3, 1: 2, 2: 1, 3: 0}
+    for mu in range(4):
+        gf = torch.roll(g, -1, dims=axis[mu]).conj().transpose(-1, -2)
+        U[..., mu, :, :] = torch.matmul(torch.matmul(g, U[..., mu, :, :]), gf)
+        del gf
+    del g
+    return U.reshape(V, 4, 3, 3)

@@ -156,6 +156,17 @@ int gfix_profile_landau(const double *d_links, const size_t dims[4],
                         const gfix_params *p, int iters, double *ms,
                         double *bytes);
 
+/* Measurement aid for Coulomb: `iters` steps of every slice from the device
+ * links `d_links` (not modified), accuracy forced to 0 so no slice stops,
+ * with CUDA events between the launches.  ms[k] / bytes[k] as for
+ * gfix_profile_landau, for k = 0 derivative, 1 xy FFT forward, 2 z FFT with
+ * psq, 3 xy FFT inverse + the per-slice sums, 4 direction + line-search
+ * probes, 5 update of the slice gauge fields, 6 the scalar, housekeeping and
+ * parity launches of one step. */
+int gfix_profile_coulomb(const double *d_links, const size_t dims[4],
+                         const gfix_params *p, int iters, double *ms,
+                         double *bytes);
+
 /* theta_test_lin (src/Gfix/gftests.c:214-250) and the gauge functional
  * (gftests.c:132-147) of the device links d_links (double[V][4][9][2] in
  * HBM), written to the device array d_out[0..1].  No counterpart in the
