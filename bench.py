@@ -449,8 +449,8 @@ C_KERNELS = ["k_cderiv", "k_fft_xy_fwd_c", "k_fft_z_c", "k_fft_xy_bwd_sums_c",
              "k_cprobe", "k_cupdate", "k_cscalar"]
 
 
-def _cparams():
-    p = _params("fp64")
+def _cparams(prec: str = "fp64"):
+    p = _params(prec)
     p.gf_alpha = C_ALPHA
     return p
 
@@ -525,9 +525,9 @@ def coulomb_gpu(args, dims, rank, world, local):
     sth = np.zeros(T)
     sit = np.zeros(T, dtype=np.uintp)
 
-    def fix(ptr, device):
+    def fix(ptr, device, prec):
         r = GfixResult()
-        p = _cparams()
+        p = _cparams(prec)
         fn = lib.gfix_coulomb_device if device else lib.gfix_coulomb
         check(fn(ptr, cd, C.byref(p), C.byref(r),
                  sth.ctypes.data_as(C.POINTER(C.c_double)),
@@ -535,44 +535,54 @@ def coulomb_gpu(args, dims, rank, world, local):
         return r
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    out = {}
     with Clocks(local) as clk:
-        for _ in range(args.warmup):
-            dwork.copy_(dpristine)
-            fix(dwork.data_ptr(), True)
-        ms = 0.0
-        launches0 = lib.gfix_kernel_launches()
-        iters = []
-        for _ in range(args.steps):
-            # the pristine copy is refreshed outside the timed region
-            dwork.copy_(dpristine)
-            barrier()
-            a, b = ev(), ev()
-            a.record()
-            r = fix(dwork.data_ptr(), True)
-            b.record()
-            barrier()
-            ms += a.elapsed_time(b)
-            iters.append(int(r.iters))
-        launches = lib.gfix_kernel_launches() - launches0
-        ms = max_over_ranks(ms)
-        e_ms = 0.0
-        for _ in range(args.steps):
-            hwork.copy_(dpristine)
-            barrier()
-            a, b = ev(), ev()
-            a.record()
-            fix(hwork.data_ptr(), False)
-            b.record()
-            torch.cuda.synchronize()
-            e_ms += a.elapsed_time(b)
-        e_ms = max_over_ranks(e_ms)
-    slice_iters = sit.astype(np.int64).copy()
-    pm = np.zeros(7)
-    pb = np.zeros(7)
-    check(lib.gfix_profile_coulomb(dpristine.data_ptr(), cd, C.byref(_cparams()),
-                                   args.profile_iters,
-                                   pm.ctypes.data_as(C.POINTER(C.c_double)),
-                                   pb.ctypes.data_as(C.POINTER(C.c_double))))
+        for prec in ([args.precision, "fp64"] if args.precision == "mixed"
+                     else ["fp64"]):
+            for _ in range(args.warmup):
+                dwork.copy_(dpristine)
+                fix(dwork.data_ptr(), True, prec)
+            ms = 0.0
+            launches0 = lib.gfix_kernel_launches()
+            iters = []
+            for _ in range(args.steps):
+                # the pristine copy is refreshed outside the timed region
+                dwork.copy_(dpristine)
+                barrier()
+                a, b = ev(), ev()
+                a.record()
+                r = fix(dwork.data_ptr(), True, prec)
+                b.record()
+                barrier()
+                ms += a.elapsed_time(b)
+                iters.append(int(r.iters))
+            launches = lib.gfix_kernel_launches() - launches0
+            ms = max_over_ranks(ms)
+            theta = float(np.max(sth))
+            slice_iters = sit.astype(np.int64).copy()
+            e_ms = 0.0
+            for _ in range(args.steps):
+                hwork.copy_(dpristine)
+                barrier()
+                a, b = ev(), ev()
+                a.record()
+                fix(hwork.data_ptr(), False, prec)
+                b.record()
+                torch.cuda.synchronize()
+                e_ms += a.elapsed_time(b)
+            e_ms = max_over_ranks(e_ms)
+            out[prec] = dict(ms=ms, e2e_ms=e_ms, iters=iters, theta=theta,
+                             iters_fp32=int(r.iters_fp32),
+                             slice_iters=slice_iters, launches=launches)
+    prof = {}
+    for prec in ("fp64", "mixed") if args.precision == "mixed" else ("fp64",):
+        pm = np.zeros(7)
+        pb = np.zeros(7)
+        check(lib.gfix_profile_coulomb(dpristine.data_ptr(), cd,
+                                       C.byref(_cparams(prec)), args.profile_iters,
+                                       pm.ctypes.data_as(C.POINTER(C.c_double)),
+                                       pb.ctypes.data_as(C.POINTER(C.c_double))))
+        prof["fp32" if prec == "mixed" else "fp64"] = (pm, pb)
     U2 = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # the first two slices of the input, for the host sample
@@ -580,28 +590,41 @@ def coulomb_gpu(args, dims, rank, world, local):
             dpristine[: 2 * V // T * 72].reshape(-1, 2)).reshape(-1, 4, 3, 3).cpu().numpy()
     if dist is not None:
         dist.destroy_process_group()
-    return dict(ms=ms, e2e_ms=e_ms, iters=iters, theta=float(np.max(sth)),
-                slice_iters=slice_iters, launches=launches,
-                clocks=clk.summary(), prof=(pm, pb), V=V), U2
+    res = dict(out[args.precision])
+    res.update(clocks=clk.summary(), prof=prof, V=V, out=out)
+    return res, U2
 
 
 def coulomb_line(args, dims, world, res, cpu):
     steps = args.steps
     peak, peak_src = peaks()
-    pm, pb = res["prof"]
-    k = int(np.argmax(pm[:6]))
+    # dominant kernel over a fix: per-step time x slice steps in its precision
+    n32 = res["iters_fp32"] if args.precision == "mixed" else 0
+    n64 = res["iters"][-1] - n32
+    cand = [(res["prof"][tag][0][j] * n, tag, j)
+            for tag, n in (("fp32", n32), ("fp64", n64)) if tag in res["prof"]
+            for j in range(6)]
+    _, tag, k = max(cand)
+    pm, pb = res["prof"][tag]
     achieved = pb[k] / (pm[k] * 1e-3) / 1e9
-    traffic = traffic_from_profiles(C_KERNELS[k], "fp64", dims)
+    traffic = traffic_from_profiles(C_KERNELS[k], tag, dims)
     V = res["V"]
     return {
         "metric": C_METRIC, "value": world * steps * 3600e3 / res["ms"],
         "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
         "ms_per_step": res["ms"] / steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if args.precision == "mixed" else "f64",
         "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled + seeded random gauge transform, on device)",
         "config": {"workload": "Coulomb FACG theta<1e-14 per slice, %s" % "x".join(map(str, dims)),
                    "dims": list(dims), "gf_alpha": C_ALPHA, "accuracy": ACC,
-                   "precision": "fp64", "iters": res["iters"][-1],
+                   "precision": args.precision, "iters": res["iters"][-1],
+                   "iters_fp32": res["iters_fp32"],
+                   "switch_theta": 1e-9 if args.precision == "mixed" else None,
+                   "fp64_only": {"value": world * steps * 3600e3 / res["out"]["fp64"]["ms"],
+                                 "ms_per_step": res["out"]["fp64"]["ms"] / steps,
+                                 "iters": res["out"]["fp64"]["iters"][-1],
+                                 "e2e": world * steps * 3600e3 / res["out"]["fp64"]["e2e_ms"]},
                    "slice_iters_min_max": [int(res["slice_iters"].min()),
                                            int(res["slice_iters"].max())],
                    "slice_steps": int(res["slice_iters"].sum() + dims[3]),
@@ -610,13 +633,15 @@ def coulomb_line(args, dims, world, res, cpu):
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "e2e": {"value": world * steps * 3600e3 / res["e2e_ms"], "unit": UNIT,
                 "h2d_bytes_per_step": V * 576, "d2h_bytes_per_step": V * 576},
-        "roofline": {"bound": "hbm", "kernel": C_KERNELS[k] + " (fp64)",
+        "roofline": {"bound": "hbm", "kernel": "%s (%s)" % (C_KERNELS[k], tag),
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src,
                      "traffic": traffic, "algorithmic_bytes": pb[k],
-                     "per_kernel": {C_KERNELS[j]: {"ms": round(pm[j], 5),
-                                                   "GB/s": round(pb[j] / (pm[j] * 1e-3) / 1e9, 1) if pb[j] else None}
-                                    for j in range(7)}},
+                     "per_kernel": {"%s:%s" % (C_KERNELS[j], t):
+                                    {"ms": round(res["prof"][t][0][j], 5),
+                                     "GB/s": round(res["prof"][t][1][j] / (res["prof"][t][0][j] * 1e-3) / 1e9, 1)
+                                     if res["prof"][t][1][j] else None}
+                                    for t in res["prof"] for j in range(7)}},
         "gpu_launches": res["launches"],
         "clocks": res["clocks"],
         **({"cpu_baseline": cpu} if cpu else {}),
@@ -634,11 +659,12 @@ def coulomb_profile_only(args, dims):
     cd = (C.c_size_t * 4)(*dims)
     ms = np.zeros(7)
     by = np.zeros(7)
-    check(lib.gfix_profile_coulomb(d.data_ptr(), cd, C.byref(_cparams()),
+    check(lib.gfix_profile_coulomb(d.data_ptr(), cd, C.byref(_cparams(args.precision)),
                                    args.profile_iters,
                                    ms.ctypes.data_as(C.POINTER(C.c_double)),
                                    by.ctypes.data_as(C.POINTER(C.c_double))))
-    emit({"profile": "coulomb fp64", "dims": list(dims), "iters": args.profile_iters,
+    emit({"profile": "coulomb " + ("fp32" if args.precision == "mixed" else "fp64"),
+          "dims": list(dims), "iters": args.profile_iters,
           "kernels": {C_KERNELS[k]: {"ms": ms[k], "bytes": by[k],
                                      "GB/s": by[k] / (ms[k] * 1e-3) / 1e9 if ms[k] else None}
                       for k in range(7)}})
@@ -686,7 +712,7 @@ def coulomb_main(args, dims, rank, world, local):
     if U2 is not None:
         try:
             s = coulomb_cpu_sample(U2, dims, os.cpu_count() or 1)
-            n_steps = int(res["slice_iters"].sum() + dims[3])
+            n_steps = int(res["out"]["fp64"]["slice_iters"].sum() + dims[3])
             t_fix = s["s_step"] * n_steps
             cpu = {"value": 3600.0 / t_fix, "unit": UNIT, "cores": s["cores"],
                    "kind": s["kind"],

@@ -19,7 +19,10 @@
 
 namespace gfix {
 
-constexpr double kPrecTol = 3 * 1.0E-14;  // PREC_TOL, GLU_definitions.h:359-363
+// PREC_TOL (GLU_definitions.h:359-363): NC 1e-14 in double, NC 1e-6 in
+// single precision builds
+constexpr double kPrecTol = 3 * 1.0E-14;
+constexpr double kPrecTolSingle = 3 * 1.0E-6;
 constexpr int kCoulThreads = 128;
 
 enum SliceMode : int { SL_RUN = 0, SL_DONE = 1 };
@@ -50,6 +53,8 @@ struct CoulState {
   int traj_cap;       // per slice
   double *traj;       // [nslices][traj_cap]
   int *done_mask;     // [nslices], 1 once a slice has finished (FFT passes skip it)
+  double prec_tol;    // PREC_TOL of the unitarity check
+  double hp_below;    // FP32 storage: FP64 arithmetic for slices below this theta
 };
 
 template <typename R>
@@ -127,18 +132,40 @@ __device__ __forceinline__ void rotated(const CCtx<R> &c, int mu, int s_link,
   gtransform(A, C, B);
 }
 
-// Hermitian short form of the rotated link (5 entries)
+// Hermitian short form of the rotated link (5 entries), formed in the
+// arithmetic type CT from links and g stored in R
 template <typename R>
 struct HShort {
   R h0, h3;
   cx<R> h1, h2, h4;
 };
-template <typename R>
-__device__ __forceinline__ HShort<R> rotated_herm(const CCtx<R> &c, int mu,
-                                                  int s_link, int sa, int sb) {
-  cx<R> C[9];
-  rotated(c, mu, s_link, sa, sb, C);
-  HShort<R> h;
+// rotated link g(a) U g(b)^dag in the arithmetic type CT
+template <typename R, typename CT>
+__device__ __forceinline__ void rotated_ct(const CCtx<R> &c, int mu, int s_link,
+                                           int sa, int sb, cx<CT> *C) {
+  auto up = [](cx<R> a) { return mk<CT>((CT)a.x, (CT)a.y); };
+  cx<CT> A[9], B[9];
+  {
+    cx<R> t[9];
+    load_link(c.U, c.V, mu, s_link, t);
+#pragma unroll
+    for (int e = 0; e < 9; e++) C[e] = up(t[e]);
+    load9(c.g, c.V, sa, t);
+#pragma unroll
+    for (int e = 0; e < 9; e++) A[e] = up(t[e]);
+    load9(c.g, c.V, sb, t);
+#pragma unroll
+    for (int e = 0; e < 9; e++) B[e] = up(t[e]);
+  }
+  gtransform(A, C, B);
+}
+
+template <typename R, typename CT>
+__device__ __forceinline__ HShort<CT> rotated_herm(const CCtx<R> &c, int mu,
+                                                   int s_link, int sa, int sb) {
+  cx<CT> C[9];
+  rotated_ct<R, CT>(c, mu, s_link, sa, sb, C);
+  HShort<CT> h;
   herm_short(C, h.h0, h.h1, h.h2, h.h3, h.h4);
   return h;
 }
@@ -146,14 +173,14 @@ __device__ __forceinline__ HShort<R> rotated_herm(const CCtx<R> &c, int mu,
 // ---------------------------------------------------------------------
 // derivative on the rotated links, packed like the Landau fields
 // (steep_deriv_CG, src/Gfix/CFACG.c:91-163)
-template <typename R, int MU>
+template <typename R, typename CT, int MU>
 __device__ __forceinline__ void cderiv_dir(const CCtx<R> &c, const SliceSite &q,
-                                           int off, R &s0, cx<R> &s1, cx<R> &s2,
-                                           R &s3, cx<R> &s4) {
+                                           int off, CT &s0, cx<CT> &s1,
+                                           cx<CT> &s2, CT &s3, cx<CT> &s4) {
   const int it = sfwd<MU>(q, c.L), bk = sbck<MU>(q, c.L);
   // g(i) U(i) g(i+mu)^dag and g(i-mu) U(i-mu) g(i)^dag
-  const HShort<R> b = rotated_herm(c, MU, off + q.i, off + q.i, off + it);
-  const HShort<R> a = rotated_herm(c, MU, off + bk, off + bk, off + q.i);
+  const HShort<CT> b = rotated_herm<R, CT>(c, MU, off + q.i, off + q.i, off + it);
+  const HShort<CT> a = rotated_herm<R, CT>(c, MU, off + bk, off + bk, off + q.i);
   s0 += a.h0 - b.h0;
   s1 = cadd(s1, csub(a.h1, b.h1));
   s2 = cadd(s2, csub(a.h2, b.h2));
@@ -161,26 +188,31 @@ __device__ __forceinline__ void cderiv_dir(const CCtx<R> &c, const SliceSite &q,
   s4 = cadd(s4, csub(a.h4, b.h4));
 }
 
-template <typename R>
-__global__ void __launch_bounds__(kCoulThreads, 4) k_cderiv(CCtx<R> c) {
+// CT: arithmetic type.  With FP32 storage a slice below theta = hp_below is
+// worked in FP64 arithmetic: the rotated links g U g^dag of FP32 products
+// carry a per-step rounding noise that stalls the FP32 phase near
+// theta ~ 1e-8.  `sel` picks the slices of this variant (ArithSel).
+template <typename R, typename CT = R>
+__global__ void __launch_bounds__(kCoulThreads, 4) k_cderiv(CCtx<R> c, int sel) {
   const int t = blockIdx.y;
-  if (c.sl[t].mode == SL_DONE) return;
+  if (c.sl[t].mode == SL_DONE || arith_skip(sel, c.sl[t].tr, c.cs->hp_below))
+    return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;  // in-slice site
   if (i >= c.Lcu) return;
   const SliceSite q = slice_site(i, c.L);
   const int off = t * c.Lcu;
-  R s0 = 0, s3 = 0;
-  cx<R> s1 = mk<R>(0, 0), s2 = mk<R>(0, 0), s4 = mk<R>(0, 0);
-  cderiv_dir<R, 0>(c, q, off, s0, s1, s2, s3, s4);
-  cderiv_dir<R, 1>(c, q, off, s0, s1, s2, s3, s4);
-  cderiv_dir<R, 2>(c, q, off, s0, s1, s2, s3, s4);
+  CT s0 = 0, s3 = 0;
+  cx<CT> s1 = mk<CT>(0, 0), s2 = mk<CT>(0, 0), s4 = mk<CT>(0, 0);
+  cderiv_dir<R, CT, 0>(c, q, off, s0, s1, s2, s3, s4);
+  cderiv_dir<R, CT, 1>(c, q, off, s0, s1, s2, s3, s4);
+  cderiv_dir<R, CT, 2>(c, q, off, s0, s1, s2, s3, s4);
   // pack: in0 = i Re s0 - Re s3, in_k = i Re s_k - Im s_k (CFACG.c:144-150)
   cx<R> *f = pick(c.fb, c.st->parity);
   const size_t V = c.V, s = off + i;
-  f[s] = mk<R>(-s3, s0);
-  f[V + s] = mk<R>(-s1.y, s1.x);
-  f[2 * V + s] = mk<R>(-s2.y, s2.x);
-  f[3 * V + s] = mk<R>(-s4.y, s4.x);
+  f[s] = mk<R>((R)-s3, (R)s0);
+  f[V + s] = mk<R>((R)-s1.y, (R)s1.x);
+  f[2 * V + s] = mk<R>((R)-s2.y, (R)s2.x);
+  f[3 * V + s] = mk<R>((R)-s4.y, (R)s4.x);
 }
 
 // The sums of the accelerated field, insum (sum_DER2 / sum_PR, one norm) and
@@ -205,36 +237,20 @@ __device__ __forceinline__ void cdir(const cx<R> *in, const cx<R> *so, R beta,
   }
 }
 
-// one link of the line-search probes: Re tr(A C B^dag) - Re tr C with C the
-// rotated link and B the probe gauge matrix at the forward neighbour
-template <typename R>
-__device__ __forceinline__ double cprobe_dir(const CCtx<R> &c, const SliceSite &q,
-                                             int mu, int off, const cx<R> *in,
-                                             const cx<R> *so, R beta, bool sdstep,
-                                             const cx<double> *A, double al) {
-  auto up = [](cx<R> a) { return mk<double>((double)a.x, (double)a.y); };
-  const int it = sfwd_rt(q, c.L, mu);
-  cx<double> Cd[9], Bm[9];
-  {
-    cx<R> C[9];
-    rotated(c, mu, off + q.i, off + q.i, off + it, C);
-#pragma unroll
-    for (int e = 0; e < 9; e++) Cd[e] = up(C[e]);
-  }
-  cx<R> fy[4];
-  cdir(in, so, beta, sdstep, (size_t)off + it, (size_t)c.V, fy);
-  set_gauge(Bm, up(fy[0]), up(fy[1]), up(fy[2]), up(fy[3]), al);
-  return re_tr_abc_dag(A, Cd, Bm) - (Cd[0].x + Cd[4].x + Cd[8].x);
-}
-
 // direction sn = in + beta_t sn_old (an SD step takes sn = in), written for
 // every live slice, and the line-search probes of line_search_Coulomb
 // (src/Gfix/line_search.c:141-271) at 0.17 and 0.34 as differences to the
 // alpha = 0 value; each link counted once (the forward links of every site,
-// the same set the reference's draughtboard visits)
-template <typename R>
-__global__ void __launch_bounds__(kCoulThreads, 3) k_cprobe(CCtx<R> c) {
+// the same set the reference's draughtboard visits).  Per link the rotated
+// link C = g(x) U g(x+mu)^dag is formed once and serves both probes; the
+// probe gauge matrices of the site itself wait in shared memory.
+// CT: arithmetic type of the probes (FP64 for FP32 storage below hp_below,
+// as in k_cderiv); `sel` picks the slices of this variant.
+template <typename R, typename CT = R>
+__global__ void __launch_bounds__(kCoulThreads, 3) k_cprobe(CCtx<R> c, int sel) {
+  __shared__ cx<CT> sA[2][9][kCoulThreads];
   const int t = blockIdx.y;
+  if (arith_skip(sel, c.sl[t].tr, c.cs->hp_below)) return;
   double v[2] = {0.0, 0.0};
   const Slice &S = c.sl[t];
   const bool live = S.mode != SL_DONE;
@@ -252,19 +268,36 @@ __global__ void __launch_bounds__(kCoulThreads, 3) k_cprobe(CCtx<R> c) {
 #pragma unroll
     for (int k = 0; k < 4; k++) sn[(size_t)k * c.V + off + i] = f[k];
     if (probes) {
-      const SliceSite q = slice_site(i, c.L);
-      auto up = [](cx<R> a) { return mk<double>((double)a.x, (double)a.y); };
+      auto up = [](cx<R> a) { return mk<CT>((CT)a.x, (CT)a.y); };
+      const CT al0 = CT(0.17), al1 = CT(0.34);
 #pragma unroll 1
       for (int k = 0; k < 2; k++) {
-        const double al = k == 0 ? 0.17 : 0.34;
-        cx<double> A[9];
-        set_gauge(A, up(f[0]), up(f[1]), up(f[2]), up(f[3]), al);
-        double d = 0.0;
-#pragma unroll 1
-        for (int mu = 0; mu < 3; mu++)
-          d += cprobe_dir<R>(c, q, mu, off, in, so, beta, sdstep, A, al);
-        v[k] = d;
+        cx<CT> A[9];
+        set_gauge(A, up(f[0]), up(f[1]), up(f[2]), up(f[3]), k ? al1 : al0);
+#pragma unroll
+        for (int e = 0; e < 9; e++) sA[k][e][threadIdx.x] = A[e];
       }
+      const SliceSite q = slice_site(i, c.L);
+      CT d[2] = {0, 0};
+#pragma unroll 1
+      for (int mu = 0; mu < 3; mu++) {
+        const int it = sfwd_rt(q, c.L, mu);
+        cx<CT> Cd[9];
+        rotated_ct<R, CT>(c, mu, off + i, off + i, off + it, Cd);
+        const CT t0 = Cd[0].x + Cd[4].x + Cd[8].x;
+        cx<R> fy[4];
+        cdir(in, so, beta, sdstep, (size_t)off + it, (size_t)c.V, fy);
+#pragma unroll 1
+        for (int k = 0; k < 2; k++) {
+          cx<CT> A[9], Bm[9];
+#pragma unroll
+          for (int e = 0; e < 9; e++) A[e] = sA[k][e][threadIdx.x];
+          set_gauge(Bm, up(fy[0]), up(fy[1]), up(fy[2]), up(fy[3]), k ? al1 : al0);
+          d[k] += re_tr_abc_dag(A, Cd, Bm) - t0;
+        }
+      }
+      v[0] = d[0];
+      v[1] = d[1];
     }
   }
   if (probes) block_sum_store<2>(v, c.part + 2 * ((size_t)t * c.nbs + blockIdx.x));
@@ -285,6 +318,10 @@ __global__ void __launch_bounds__(kCoulThreads) k_cupdate(CCtx<R> c) {
   set_gauge(A, d[s], d[V + s], d[2 * V + s], d[3 * V + s], (R)S.alpha);
   load9(c.g, c.V, (int)s, G);
   multab(r, A, G);
+  // FP32: the product of many rounded SU(3) factors drifts off the group
+  // (~1e-7 a step) and the derivative assumes a unitary g; FP64 keeps GLU's
+  // plain product
+  if constexpr (sizeof(R) == 4) gram_reunit(r);
   store9(c.g, c.V, (int)s, r);
 }
 
@@ -314,7 +351,7 @@ __global__ void __launch_bounds__(kCoulThreads) k_cmaint(CCtx<R> c, int what) {
     double sum = 0.0;
 #pragma unroll
     for (int e = 0; e < 9; e++) sum += (double)G[e].x * G[e].x + (double)G[e].y * G[e].y;
-    const double lim = (double)(S.iter > 0 ? S.iter : 1) * kPrecTol;
+    const double lim = (double)(S.iter > 0 ? S.iter : 1) * c.cs->prec_tol;
     if (fabs(sum - 3.0) > lim) atomicOr(&S.bad, 1);
   } else if (what == 1 && S.randomize) {
     cx<R> G[9];

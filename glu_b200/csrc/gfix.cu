@@ -379,6 +379,18 @@ class Engine {
       k_fft_zt<R, 16, false><<<g_zt, bd_zt, sm_zt, s>>>(c);
     LAUNCHED(1);
   }
+  // direction + probes: FP64 storage one kernel; FP32 storage the FP32- and
+  // the FP64-arithmetic variants, of which the device state picks one
+  template <bool DIR>
+  void probe() {
+    if (sizeof(R) == 8) {
+      k_dir_probe<R, DIR, double><<<nb_site, kSiteThreads, 0, s>>>(c, SEL_ALWAYS);
+    } else {
+      k_dir_probe<R, DIR, R><<<nb_site, kSiteThreads, 0, s>>>(c, SEL_LOW);
+      k_dir_probe<R, DIR, double><<<nb_site, kSiteThreads, 0, s>>>(c, SEL_HIGH);
+      LAUNCHED(1);
+    }
+  }
   void fft(bool prsum) {
     fft_xy(0, 0);
     fft_zt();
@@ -392,7 +404,7 @@ class Engine {
     if (sd_fixed) {
       scalar(OP_ALPHA_FIXED, 0);
     } else {
-      k_dir_probe<R, false, double><<<nb_site, kSiteThreads, 0, s>>>(c);
+      probe<false>();
       LAUNCHED(1);
       scalar(OP_PROBES, 2);
     }
@@ -405,7 +417,7 @@ class Engine {
     theta(OP_THETA_MAIN);
     fft(true);
     scalar(OP_PR, 2);
-    k_dir_probe<R, true, double><<<nb_site, kSiteThreads, 0, s>>>(c);
+    probe<true>();
     LAUNCHED(1);
     scalar(OP_PROBES, 2);
     k_update<R, true><<<nb_site, kSiteThreads, 0, s>>>(c);
@@ -450,8 +462,10 @@ class Engine {
 
   unsigned long long per_iter_launches(bool cg, bool sd_fixed) const {
     // k_deriv + scalar + 3 fft + ...
-    if (cg) return 2 + 3 + 1 + 2 + 1 + 1;
-    return 2 + 3 + (sd_fixed ? 1 : 2) + 1 + 1;
+    // (FP32 storage launches two probe variants)
+    const unsigned long long two = sizeof(R) == 4 ? 1 : 0;
+    if (cg) return 2 + 3 + 1 + 2 + 1 + 1 + two;
+    return 2 + 3 + (sd_fixed ? 1 : 2 + two) + 1 + 1;
   }
 
   int read_state() {
@@ -519,6 +533,7 @@ class Engine {
     // GLU's CG_TOL (5e-11) in both phases: with FP64 probe arithmetic the
     // FP32 phase keeps its line search down to the precision switch
     st.cg_tol = 5E-11;
+    st.hp_below = 1E-5;
     st.traj_cap = p.traj_cap ? (long long)p.traj_cap : 0;
     st.traj_theta = p.traj_cap ? d_traj : nullptr;
     st.traj_func = p.traj_cap ? d_traj + p.traj_cap : nullptr;
@@ -648,7 +663,7 @@ class Engine {
       CK(cudaEventRecord(ev[5], s));
       scalar(OP_PR, 2);
       CK(cudaEventRecord(ev[6], s));
-      k_dir_probe<R, true, double><<<nb_site, kSiteThreads, 0, s>>>(c);
+      probe<true>();
       CK(cudaEventRecord(ev[7], s));
       CK(cudaStreamSynchronize(s));
       float t[7];
@@ -756,15 +771,36 @@ class Engine {
     if (g) cudaGraphDestroy(g);
   }
 
+  // derivative and probes: FP64 storage one kernel each; FP32 storage an
+  // FP32- and an FP64-arithmetic variant, each taking its own slices
+  void cderiv(dim3 gs) {
+    if (sizeof(R) == 8) {
+      k_cderiv<R, double><<<gs, kCoulThreads, 0, s>>>(cc, SEL_ALWAYS);
+    } else {
+      k_cderiv<R, R><<<gs, kCoulThreads, 0, s>>>(cc, SEL_LOW);
+      k_cderiv<R, double><<<gs, kCoulThreads, 0, s>>>(cc, SEL_HIGH);
+      LAUNCHED(1);
+    }
+  }
+  void cprobe(dim3 gs) {
+    if (sizeof(R) == 8) {
+      k_cprobe<R, double><<<gs, kCoulThreads, 0, s>>>(cc, SEL_ALWAYS);
+    } else {
+      k_cprobe<R, R><<<gs, kCoulThreads, 0, s>>>(cc, SEL_LOW);
+      k_cprobe<R, double><<<gs, kCoulThreads, 0, s>>>(cc, SEL_HIGH);
+      LAUNCHED(1);
+    }
+  }
+
   // one step of every live slice
   void citer() {
     const dim3 gs(nbs, c.L[3]);
-    k_cderiv<R><<<gs, kCoulThreads, 0, s>>>(cc);
+    cderiv(gs);
     fft_xy(0, 0);
     fft_zt();
     fft_xy(1, 1);  // with the per-plane sums of the accelerated field
     cscalar(C_SUMS);
-    k_cprobe<R><<<gs, kCoulThreads, 0, s>>>(cc);
+    cprobe(gs);
     cscalar(C_PROBES);
     k_cupdate<R><<<gs, kCoulThreads, 0, s>>>(cc);
     cscalar(C_END1);
@@ -776,8 +812,9 @@ class Engine {
   }
 
   // GLU's Coulomb_FA (src/Gfix/CFACG.c:531-636) on the resident links
-  // state of a new solve: every slice live, g = 1, fields zero
-  int cstart(const Params &p) {
+  // state of a new solve: every slice live, fields zero, g = 1 (or the g
+  // left in place by an earlier phase)
+  int cstart(const Params &p, bool identity = true) {
     if (cinit()) return -1;
     const int T = c.L[3];
     const size_t per = p.traj_cap ? p.traj_cap / T : 0;
@@ -800,6 +837,11 @@ class Engine {
     cst.traj_cap = (int)per;
     cst.traj = per ? d_ctraj : nullptr;
     cst.done_mask = d_cmask;
+    cst.prec_tol = sizeof(R) == 4 ? kPrecTolSingle : kPrecTol;
+    // FP32 storage: FP32 arithmetic only while theta >= 1e-2 -- below it the
+    // rounding of FP32 rotated links slows the slices' convergence (measured
+    // on 32^3x64 and 64^3x128 slices), unlike the Landau probes (1e-5)
+    cst.hp_below = 1E-2;
     CK(cudaMemsetAsync(d_cmask, 0, sizeof(int) * T, s));
     CK(cudaMemcpyAsync(d_cst, &cst, sizeof cst, cudaMemcpyHostToDevice, s));
     std::vector<Slice> sl(T);
@@ -815,17 +857,22 @@ class Engine {
     CK(cudaMemcpyAsync(d_st, &st, sizeof st, cudaMemcpyHostToDevice, s));
     // in_old and sn start at zero (SD steps do not read them)
     CK(cudaMemsetAsync(c.fb[0], 0, (size_t)V * 16 * sizeof(cx<R>), s));
-    k_cinit<R><<<(V + 255) / 256, 256, 0, s>>>(cc);
-    LAUNCHED(1);
+    if (identity) {
+      k_cinit<R><<<(V + 255) / 256, 256, 0, s>>>(cc);
+      LAUNCHED(1);
+    }
     return 0;
   }
 
+  // transform = false leaves the links untouched (a mixed-precision phase)
   int csolve(const Params &p, size_t *iters, double *slice_theta,
-             size_t *slice_iters, size_t *traj_len) {
-    if (cstart(p)) return -1;
+             size_t *slice_iters, size_t *traj_len, bool identity = true,
+             bool transform = true) {
+    if (cstart(p, identity)) return -1;
     const int T = c.L[3];
     const size_t per = p.traj_cap ? p.traj_cap / T : 0;
-    const unsigned long long per_iter = 13;  // launches in citer()
+    // launches in citer() (FP32 storage: two variants of two kernels)
+    const unsigned long long per_iter = sizeof(R) == 4 ? 15 : 13;
     int batch = 2;
     size_t guard = 0;
     const size_t limit = (p.max_iters + 2) * 9 * 64 + 1024;
@@ -849,9 +896,11 @@ class Engine {
         return fail("Coulomb solve did not stop after %zu steps", guard);
       batch = std::min(batch * 2, 32);
     }
-    k_cslice_transform<R><<<(V + kCoulThreads - 1) / kCoulThreads,
-                            kCoulThreads, 0, s>>>(cc);
-    LAUNCHED(1);
+    if (transform) {
+      k_cslice_transform<R><<<(V + kCoulThreads - 1) / kCoulThreads,
+                              kCoulThreads, 0, s>>>(cc);
+      LAUNCHED(1);
+    }
     CK(cudaMemcpyAsync(h_sl, d_sl, sizeof(Slice) * T, cudaMemcpyDeviceToHost,
                        s));
     CK(cudaStreamSynchronize(s));
@@ -894,7 +943,7 @@ class Engine {
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     for (int it = 0; it < n; it++) {
       CK(cudaEventRecord(ev[0], s));
-      k_cderiv<R><<<gs, kCoulThreads, 0, s>>>(cc);
+      cderiv(gs);
       CK(cudaEventRecord(ev[1], s));
       fft_xy(0, 0);
       CK(cudaEventRecord(ev[2], s));
@@ -904,7 +953,7 @@ class Engine {
       CK(cudaEventRecord(ev[4], s));
       cscalar(C_SUMS);
       CK(cudaEventRecord(ev[5], s));
-      k_cprobe<R><<<gs, kCoulThreads, 0, s>>>(cc);
+      cprobe(gs);
       CK(cudaEventRecord(ev[6], s));
       cscalar(C_PROBES);
       CK(cudaEventRecord(ev[7], s));
@@ -1025,6 +1074,24 @@ static Engine<double> *engine_coul(const size_t *d) {
   return p;
 }
 
+static std::map<Key, std::unique_ptr<Engine<float>>> g_ec32;
+
+static Engine<float> *engine_coul32(const size_t *d) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    fail("no CUDA device");
+    return nullptr;
+  }
+  Key k{dev, {d[0], d[1], d[2], d[3]}, 32};
+  auto it = g_ec32.find(k);
+  if (it != g_ec32.end()) return it->second.get();
+  auto e = std::make_unique<Engine<float>>();
+  if (e->init(d, true, false, true)) return nullptr;
+  Engine<float> *p = e.get();
+  g_ec32[k] = std::move(e);
+  return p;
+}
+
 static Params to_params(const gfix_params *p) {
   Params q;
   q.gf_alpha = p->gf_alpha;
@@ -1133,6 +1200,7 @@ void gfix_release(void) {
   g_e64.clear();
   g_e32.clear();
   g_ec.clear();
+  g_ec32.clear();
 }
 
 static int check_params(const size_t *dims, const gfix_params *p) {
@@ -1260,34 +1328,71 @@ int gfix_profile_landau(const double *d_links, const size_t dims[4],
   return e->profile_cg(q, iters, ms, bytes);
 }
 
-// the staged links of `e` (AoS FP64 in e->d_aos) Coulomb-fixed in place
+// the staged links of `e` (AoS FP64 in e->d_aos) Coulomb-fixed in place.
+// GFIX_MIXED: every slice first runs in FP32 (links, g, fields; probes and
+// reductions in FP64 arithmetic) to theta < switch_theta, then g is
+// widened, reunitarised in FP64 and the FP64 solve continues from it to the
+// requested accuracy; a non-finite FP32 phase hands over nothing (FP64 from
+// g = 1).  Trajectories then hold the FP64 phase.
 static int coulomb_staged(Engine<double> *e, const gfix_params *gp,
                           gfix_result *r, double *slice_theta,
                           size_t *slice_iters) {
   const Params p = to_params(gp);
   const int T = e->c.L[3];
-  std::vector<double> th(T);
-  std::vector<size_t> it(T);
+  std::vector<double> th(T), th32(T);
+  std::vector<size_t> it(T), it32(T, 0);
   gfix_result res;
   memset(&res, 0, sizeof res);
   CK(cudaEventRecord(e->ev0, e->s));
   if (e->from_aos(e->d_aos)) return -1;
-  size_t iters = 0, tl = 0;
-  if (e->csolve(p, &iters, th.data(), it.data(), &tl)) return -1;
+  size_t iters = 0, tl = 0, n32 = 0;
+  bool from_g = false;
+  if (gp->precision == GFIX_MIXED) {
+    Engine<float> *f = engine_coul32(e->dims);
+    if (!f) return -1;
+    CK(cudaStreamSynchronize(e->s));
+    k_convert<double, float><<<1184, 256, 0, f->s>>>(e->d_U, f->d_U,
+                                                     (size_t)e->V * 36);
+    LAUNCHED(1);
+    Params p32 = p;
+    p32.acc = gp->switch_theta;
+    p32.traj_cap = 0;
+    p32.traj_theta = p32.traj_func = nullptr;
+    if (f->csolve(p32, &n32, th32.data(), it32.data(), nullptr, true, false))
+      return -1;
+    bool finite = true;
+    for (int t = 0; t < T; t++) finite &= std::isfinite(th32[t]) != 0;
+    if (finite) {
+      k_convert<float, double><<<1184, 256, 0, f->s>>>(f->d_G, e->d_G,
+                                                       (size_t)e->V * 9);
+      LAUNCHED(1);
+      CK(cudaStreamSynchronize(f->s));
+      k_reunit_links<double><<<(e->V + 255) / 256, 256, 0, e->s>>>(
+          e->d_G, (size_t)e->V, (size_t)e->V);
+      LAUNCHED(1);
+      from_g = true;
+    } else {
+      std::fill(it32.begin(), it32.end(), 0);
+      n32 = 0;
+      res.restarts++;
+    }
+  }
+  if (e->csolve(p, &iters, th.data(), it.data(), &tl, !from_g, true)) return -1;
   CK(cudaEventRecord(e->ev1, e->s));
   if (e->to_aos(e->d_aos)) return -1;
   CK(cudaStreamSynchronize(e->s));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
   double worst = 0.0;
-  int restarts = 0;
+  int restarts = res.restarts;
   for (int t = 0; t < T; t++) {
     worst = std::isnan(th[t]) || th[t] > worst ? th[t] : worst;
     restarts += e->h_sl[t].control;
     if (slice_theta) slice_theta[t] = th[t];
-    if (slice_iters) slice_iters[t] = it[t];
+    if (slice_iters) slice_iters[t] = it[t] + it32[t];
   }
-  res.iters = iters;
+  res.iters = iters + n32;
+  res.iters_fp32 = n32;
   res.theta = worst;
   res.traj_len = tl;
   res.gpu_ms = ms;
@@ -1321,6 +1426,15 @@ int gfix_profile_coulomb(const double *d_links, const size_t dims[4],
   CK(cudaDeviceSynchronize());
   CK(cudaMemcpyAsync(e->d_aos, d_links, n, cudaMemcpyDeviceToDevice, e->s));
   if (e->from_aos(e->d_aos)) return -1;
+  if (p->precision == GFIX_MIXED) {
+    Engine<float> *f = engine_coul32(dims);
+    if (!f) return -1;
+    CK(cudaStreamSynchronize(e->s));
+    k_convert<double, float><<<1184, 256, 0, f->s>>>(e->d_U, f->d_U,
+                                                     (size_t)e->V * 36);
+    LAUNCHED(1);
+    return f->profile_coul(to_params(p), iters, ms, bytes);
+  }
   return e->profile_coul(to_params(p), iters, ms, bytes);
 }
 

@@ -65,7 +65,17 @@ struct DevState {
   int nblocks;        // partials written by the last reduction kernel
   int sd_fixed;       // GLU_GFIX_SD: fixed step gf_alpha in SD steps
   double cg_tol;      // CG_TOL (GLU_definitions.h:451-455)
+  double hp_below;    // FP32 storage: probes in FP64 arithmetic once tr < this
 };
+
+// which arithmetic variant of a kernel runs this step (FP32 storage: FP32
+// arithmetic while theta >= hp_below, FP64 arithmetic below; a NaN theta
+// takes the FP32 variant)
+enum ArithSel : int { SEL_ALWAYS = 0, SEL_LOW = 1, SEL_HIGH = 2 };
+__device__ __forceinline__ bool arith_skip(int sel, double tr, double below) {
+  const bool high = tr < below;
+  return (sel == SEL_LOW && high) || (sel == SEL_HIGH && !high);
+}
 
 // set or clear the done flag (used to run every kernel once as a no-op)
 __global__ void k_set_done(DevState *st, int v) { st->done = v; }
@@ -260,11 +270,13 @@ __device__ __forceinline__ void dir_at(const Ctx<R> &c, const cx<R> *in,
 }
 
 // C is the arithmetic precision of the probes: the FP32 phase of the mixed
-// solver evaluates them in FP64 from its FP32 links and directions, because
-// per-site probe differences fall below FP32 rounding once theta < ~1e-6.
+// solver evaluates them in FP64 from its FP32 links and directions once
+// theta < hp_below (1e-5), because per-site probe differences fall below
+// FP32 rounding once theta < ~1e-6; above it FP32 arithmetic serves.  Both
+// variants are launched, `sel` lets the one that fits the step run.
 template <typename R, bool DIR, typename C = R>
-__global__ void __launch_bounds__(kSiteThreads) k_dir_probe(Ctx<R> c) {
-  if (c.st->done) return;
+__global__ void __launch_bounds__(kSiteThreads) k_dir_probe(Ctx<R> c, int sel) {
+  if (c.st->done || arith_skip(sel, c.st->tr, c.st->hp_below)) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int par = c.st->parity, spar = c.st->sparity;
   const cx<R> *in = c.fb[par];

@@ -162,7 +162,8 @@ int gfix_profile_landau(const double *d_links, const size_t dims[4],
  * gfix_profile_landau, for k = 0 derivative, 1 xy FFT forward, 2 z FFT with
  * psq, 3 xy FFT inverse + the per-slice sums, 4 direction + line-search
  * probes, 5 update of the slice gauge fields, 6 the scalar, housekeeping and
- * parity launches of one step. */
+ * parity launches of one step.  precision GFIX_MIXED profiles the FP32
+ * kernels. */
 int gfix_profile_coulomb(const double *d_links, const size_t dims[4],
                          const gfix_params *p, int iters, double *ms,
                          double *bytes);

@@ -179,3 +179,31 @@ def test_glu_named_coulomb_reunitarises(lat400):
     M = U.reshape(-1, 3, 3)
     err = np.abs(M @ np.conj(np.swapaxes(M, -1, -2)) - np.eye(3)).max()
     assert err < 1e-14
+
+
+@pytest.mark.parametrize("case", ["lat400", "hb8"])
+def test_mixed_precision_reaches_fp64_accuracy(case, request):
+    """FP32 phase to theta < 1e-9 per slice, FP64 polish to 1e-14: the same
+    accuracy, the links on the same gauge orbit, and the FP64 fix's gauge."""
+    g = request.getfixturevalue(case)
+    d = _dims(g)
+    alpha = 0.09 if case == "lat400" else 0.08
+    r64 = gfix.coulomb_fix(g["links"], d, alpha, ACC, 2000, "FACG")
+    r = gfix.coulomb_fix(g["links"], d, alpha, ACC, 2000, "FACG",
+                         precision="MIXED", switch_theta=1e-9)
+    assert np.all(r.slice_theta < ACC)
+    assert 0 < r.iters_fp32 < r.iters
+    assert np.all(r.slice_iters > 0)
+    _, _, p0 = gfix.observables(g["links"], d)
+    _, _, p1 = gfix.observables(r.links, d)
+    assert abs(p1 - p0) < 1e-13
+    # Coulomb gauge leaves one global SU(3) rotation per slice free, and the
+    # FP32 rounding of the derivative's zero mode moves it (~1e-4 here); the
+    # traces of the spatial links are blind to it and pin the local gauge to
+    # the distance theta < 1e-14 leaves open
+    # (a small Faddeev-Popov eigenvalue can stretch that to ~1e-6); the
+    # spatial functional, second order at the solution, agrees to 1e-13
+    tr = lambda U: np.trace(U[:, :3], axis1=-2, axis2=-1)  # noqa: E731
+    assert np.abs(tr(r.links) - tr(r64.links)).max() < 1e-5
+    fs = lambda U: 1.0 - tr(U).real.sum() / (9.0 * U.shape[0])  # noqa: E731
+    assert abs(fs(r.links) - fs(r64.links)) < 1e-13
