@@ -39,7 +39,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "gauge-fixed configs/hour (32^3x64 Landau FACG, theta<1e-14)"
+def metric_name(dims) -> str:
+    return "gauge-fixed configs/hour (%dx%dx%dx%d Landau FACG, theta<1e-14)" % tuple(dims)
 UNIT = "configs/hour"
 ACC = 1e-14
 ALPHA = 0.08
@@ -340,7 +341,7 @@ def reference_arm(args, dims, rank, world):
     t_fix = fixed + s_iter * n_ref
     value = 3600.0 / t_fix
     s0 = samples[0]
-    emit({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+    emit({"metric": metric_name(dims), "value": value, "unit": UNIT, "n_gpus": world,
           "steps": args.steps, "warmup": args.warmup,
           "ms_per_step": t_fix * 1e3, "higher_is_better": True,
           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -384,7 +385,7 @@ def gpu_line(args, dims, world, res, cpu):
                   for t in ("fp32", "fp64") if (t != "fp32" or prec == "mixed")
                   for j, (m, b) in enumerate(zip(*res["prof"][t])) if j < 6}
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "metric": metric_name(dims), "value": value, "unit": UNIT, "n_gpus": world,
         "steps": steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if prec == "mixed" else "f64",
@@ -443,7 +444,9 @@ def profile_only(args, dims):
 # theta < 1e-14 (GLU's Coulomb_FA, FACG), all slices in one batched launch
 # sequence.  FP64.
 
-C_METRIC = "Coulomb-gauge-fixed configs/hour (64^3x128 FACG, theta<1e-14 per slice)"
+def c_metric_name(dims) -> str:
+    return ("Coulomb-gauge-fixed configs/hour (%dx%dx%dx%d FACG, theta<1e-14 per slice)"
+            % tuple(dims))
 C_ALPHA = 0.08
 C_KERNELS = ["k_cderiv", "k_fft_xy_fwd_c", "k_fft_z_c", "k_fft_xy_bwd_sums_c",
              "k_cprobe", "k_cupdate", "k_cscalar"]
@@ -610,7 +613,7 @@ def coulomb_line(args, dims, world, res, cpu):
     traffic = traffic_from_profiles(C_KERNELS[k], tag, dims)
     V = res["V"]
     return {
-        "metric": C_METRIC, "value": world * steps * 3600e3 / res["ms"],
+        "metric": c_metric_name(dims), "value": world * steps * 3600e3 / res["ms"],
         "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
         "ms_per_step": res["ms"] / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
@@ -690,7 +693,7 @@ def coulomb_main(args, dims, rank, world, local):
         s_step = statistics.median(x["s_step"] for x in samples)
         t_fix = s_step * n_steps
         value = 3600.0 / t_fix
-        emit({"metric": C_METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        emit({"metric": c_metric_name(dims), "value": value, "unit": UNIT, "n_gpus": world,
               "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_fix * 1e3,
               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
               "dtype": "f64", "data": "synthetic (8^4 GLU heatbath tiled + random gauge)",

@@ -65,7 +65,11 @@ __device__ __forceinline__ void ct_stages(cx<R> *buf, const cx<R> *tw,
   }
 }
 
-__host__ __device__ constexpr int ct_threads(int n) { return n / 8 < 32 ? 32 : n / 8; }
+// threads of a tile of n elements: one radix-8 butterfly each (32..1024
+// threads), two for tiles above 8192 elements
+__host__ __device__ constexpr int ct_threads(int n) {
+  return n / 8 < 32 ? 32 : (n / 8 <= 1024 ? n / 8 : n / 16);
+}
 // resident blocks asked of the compiler: 1024 threads per SM at least
 __host__ __device__ constexpr int ct_minb(int n) {
   return 1024 / ct_threads(n) < 1 ? 1 : 1024 / ct_threads(n);

@@ -107,7 +107,7 @@ static ZtFn<R> ct_zt(int lz, int lt, int b) {
   if (lz == z && lt == t && b == bb) return k_fft_zt_ct<R, z, t, bb>;
   GFIX_ZT(4, 4, 2) GFIX_ZT(4, 8, 2) GFIX_ZT(8, 8, 2) GFIX_ZT(8, 16, 2)
   GFIX_ZT(16, 16, 2) GFIX_ZT(16, 32, 2) GFIX_ZT(24, 48, 2)
-  GFIX_ZT(32, 32, 2) GFIX_ZT(32, 64, 2)
+  GFIX_ZT(32, 32, 2) GFIX_ZT(32, 64, 2) GFIX_ZT(48, 96, 2)
   GFIX_ZT(4, 1, 8) GFIX_ZT(8, 1, 8) GFIX_ZT(16, 1, 8) GFIX_ZT(24, 1, 8)
   GFIX_ZT(32, 1, 8) GFIX_ZT(48, 1, 8) GFIX_ZT(64, 1, 8)
   GFIX_ZT(8, 1, 16) GFIX_ZT(16, 1, 16) GFIX_ZT(24, 1, 16) GFIX_ZT(32, 1, 16)
@@ -246,25 +246,35 @@ class Engine {
         c.zt_b = b;
         break;
       }
-    // tiles are transformed in place, one element per thread and stage for
-    // kPerThread elements: at most 512 threads, so tiles up to 8192
+    odd = false;
+    for (int a = 0; a < 4; a++)
+      for (int k = 0; k < c.ax[a].nstages; k++)
+        odd |= (c.ax[a].st[k].r == 5 || c.ax[a].st[k].r == 7);
+    auto zt_smem = [&](int b) {
+      return coul ? ((size_t)b * c.L[2] + c.L[2]) * sizeof(cx<R>)
+                  : ((size_t)(b * c.L[2] + std::max(1, zt_pad(b))) * c.L[3] +
+                     c.L[2] + c.L[3]) * sizeof(cx<R>);
+    };
+    // a compile-time pass takes the tile as chosen while its shared memory
+    // fits (tiles up to 16384 elements); the generic passes hold one
+    // element per thread and stage for 8 (16) elements: tiles up to 8192
+    const bool ct_tile = !odd && ct_zt<R>(c.L[2], nt, c.zt_b) != nullptr &&
+                         zt_smem(c.zt_b) <= 200u * 1024u;
     constexpr int pt_small = 8;
     auto threads_for = [](size_t n, int pt) {
       size_t t = (n + pt - 1) / pt;
       t = std::max<size_t>(128, (t + 31) / 32 * 32);
       return t;
     };
-    while (c.zt_b > 1 && (size_t)c.zt_b * c.L[2] * nt > 512u * pt_small)
-      c.zt_b /= 2;
-    while (c.zt_b > 1 && c.L[0] % c.zt_b) c.zt_b /= 2;
+    if (!ct_tile) {
+      while (c.zt_b > 1 && (size_t)c.zt_b * c.L[2] * nt > 512u * pt_small)
+        c.zt_b /= 2;
+      while (c.zt_b > 1 && c.L[0] % c.zt_b) c.zt_b /= 2;
+    }
     const size_t n_xy = (size_t)c.L[0] * c.L[1];
     const size_t n_zt = (size_t)c.zt_b * c.L[2] * nt;
-    if (n_xy > 8192 || n_zt > 8192)
+    if (n_xy > 8192 || (n_zt > 8192 && !ct_tile))
       return fail("FFT tile of %zu / %zu elements exceeds 8192", n_xy, n_zt);
-    odd = false;
-    for (int a = 0; a < 4; a++)
-      for (int k = 0; k < c.ax[a].nstages; k++)
-        odd |= (c.ax[a].st[k].r == 5 || c.ax[a].st[k].r == 7);
     pt_xy = (n_xy <= 512u * pt_small && !odd) ? pt_small : 16;
     pt_zt = (n_zt <= 512u * pt_small && !odd) ? pt_small : 16;
     bd_xy = (int)threads_for(n_xy, pt_xy);
@@ -272,9 +282,7 @@ class Engine {
     // tile (padded) plus the twiddle tables of its two axes
     sm_xy = ((size_t)c.xy_pitch * c.L[1] + c.L[0] + c.L[1]) * sizeof(cx<R>);
     // (the t-stride padding covers the generic pass's 1 and zt_pad)
-    sm_zt = coul ? ((size_t)c.zt_b * c.L[2] + c.L[2]) * sizeof(cx<R>)
-                 : ((size_t)(c.zt_b * c.L[2] + std::max(1, zt_pad(c.zt_b))) *
-                        c.L[3] + c.L[2] + c.L[3]) * sizeof(cx<R>);
+    sm_zt = zt_smem(c.zt_b);
     // the dynamic shared-memory limit is an attribute of the function, not
     // of a launch: raise it once to the largest tile any engine can use
     if (set_smem_limits()) return -1;

@@ -38,7 +38,8 @@ def test_observables_match_oracle(oracle, case, request):
     assert abs(pl - g["plaquette"]) < 1e-13
 
 
-@pytest.mark.parametrize("dims", [(4, 4, 4, 8), (8, 6, 4, 12), (6, 10, 5, 3)])
+@pytest.mark.parametrize("dims", [(4, 4, 4, 8), (8, 6, 4, 12), (6, 10, 5, 3),
+                                  (8, 8, 48, 96)])
 def test_fourier_accelerate_matches_oracle(oracle, dims):
     rng = np.random.default_rng(7)
     V = int(np.prod(dims))
