@@ -35,7 +35,9 @@ EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
            "gfix_landau_device", "gfix_coulomb", "gfix_coulomb_device",
            "gfix_observables", "gfix_reunit", "gfix_fourier_accelerate",
            "gfix_profile_landau", "gfix_profile_coulomb",
-           "gfix_theta_functional_noalloc",
+           "gfix_theta_functional_noalloc", "gfix_batch_create",
+           "gfix_batch_add", "gfix_batch_add_device", "gfix_batch_run",
+           "gfix_batch_result", "gfix_batch_destroy",
            "gfix_noalloc_error",
            "gfix_last_error", "gfix_release", "gfix_kernel_launches")
 
@@ -72,6 +74,17 @@ def load(path: Path | str | None = None):
     lib.gfix_reunit.argtypes = [C.c_void_p, _szp]
     lib.gfix_fourier_accelerate.restype = C.c_int
     lib.gfix_fourier_accelerate.argtypes = [C.c_void_p, _szp, C.c_int]
+    lib.gfix_batch_create.restype = C.c_void_p
+    lib.gfix_batch_create.argtypes = [C.POINTER(GfixParams)]
+    for fn in ("gfix_batch_add", "gfix_batch_add_device"):
+        getattr(lib, fn).restype = C.c_int
+        getattr(lib, fn).argtypes = [C.c_void_p, C.c_void_p, _szp]
+    lib.gfix_batch_run.restype = C.c_int
+    lib.gfix_batch_run.argtypes = [C.c_void_p]
+    lib.gfix_batch_result.restype = C.c_int
+    lib.gfix_batch_result.argtypes = [C.c_void_p, C.c_int, C.POINTER(GfixResult)]
+    lib.gfix_batch_destroy.restype = None
+    lib.gfix_batch_destroy.argtypes = [C.c_void_p]
     lib.gfix_profile_coulomb.restype = C.c_int
     lib.gfix_profile_coulomb.argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
                                          C.c_int, _dp, _dp]

@@ -146,6 +146,7 @@ class Engine {
   XyFn<R> xy_ct = nullptr;
   ZtFn<R> zt_ct = nullptr;
   cudaGraphExec_t gx_cg = nullptr, gx_sd = nullptr;
+  cudaGraph_t gr_cg = nullptr, gr_sd = nullptr;  // the same, uninstantiated
   int gx_sd_fixed = -1;
   bool primed = false;
   bool graph_ok = true;
@@ -157,7 +158,10 @@ class Engine {
     if (gx_cg) cudaGraphExecDestroy(gx_cg);
     if (gx_sd) cudaGraphExecDestroy(gx_sd);
     if (gx_coul) cudaGraphExecDestroy(gx_coul);
+    if (gr_cg) cudaGraphDestroy(gr_cg);
+    if (gr_sd) cudaGraphDestroy(gr_sd);
     gx_cg = gx_sd = gx_coul = nullptr;
+    gr_cg = gr_sd = nullptr;
     cudaFree(d_cst);
     cudaFreeHost(h_cst);
     cudaFree(d_sl);
@@ -452,7 +456,7 @@ class Engine {
 
   int capture(cudaGraphExec_t *out, bool cg, bool sd_fixed) {
     if (prime()) return -1;
-    cudaGraph_t g;
+    cudaGraph_t g = nullptr;
     CK(cudaGetLastError());
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
     const unsigned long long before = g_launches.load();
@@ -464,7 +468,10 @@ class Engine {
     g_launches.store(before);
     CK(cudaStreamEndCapture(s, &g));
     CK(cudaGraphInstantiate(out, g, 0));
-    cudaGraphDestroy(g);
+    // kept for batches, which nest it in a graph over many engines
+    cudaGraph_t &keep = cg ? gr_cg : gr_sd;
+    if (keep) cudaGraphDestroy(keep);
+    keep = g;
     return 0;
   }
 
@@ -577,69 +584,86 @@ class Engine {
     return 0;
   }
 
-  // GLU's FACG (src/Gfix/FACG.c:341-391) on the resident links
-  int solve_facg(const Params &p, size_t *iters, double *th) {
-    if (reset(p)) return -1;
-    if (theta_test(th)) return -1;
-    if (*th < p.acc) {
-      *iters = 0;
-      return 0;
-    }
-    ensure_graph(&gx_cg, true, false);
-    for (;;) {
-      k_begin_run<<<1, 1, 0, s>>>(d_st);
-      LAUNCHED(1);
-      sd_step(false, p.sd_fixed != 0);
+  // A solve as resumable steps, shared by the single driver (solve) and
+  // the batched one (batch_solve):
+  //   run_start  reset, theta_test, graph, launch of the first run's head
+  //   run_exec   the iteration graph of the run (nullptr: direct launches)
+  //   run_after  once the device says done (h_st current): GLU's end of
+  //              FACG / FASD, or the head of a continuation run
+  // GLU's FACG (src/Gfix/FACG.c:341-391) and FASD (FACG.c:395-446).
+  Params run_p;
+  bool run_cg = true;
+  size_t run_total = 0;
+
+  void run_head() {
+    k_begin_run<<<1, 1, 0, s>>>(d_st);
+    LAUNCHED(1);
+    if (run_cg) {
+      sd_step(false, run_p.sd_fixed != 0);
       k_copy_der<R><<<nb_site, kSiteThreads, 0, s>>>(c);
       LAUNCHED(1);
       scalar(OP_DER, 1);
-      if (replay(gx_cg, true, false)) return -1;
-      *th = h_st->tr;
-      const size_t loc = (size_t)h_st->iter;
-      if (loc >= p.max_iters) {
-        if (*th < 1E3 * p.acc) continue;  // continuation run
-        *iters = kSentinel;
-        return 0;
-      }
-      *iters = loc;
-      return 0;
     }
   }
 
-  // GLU's FASD (src/Gfix/FACG.c:395-446)
-  int solve_fasd(const Params &p, size_t *iters, double *th) {
+  int run_start(const Params &p, bool *fin, size_t *iters, double *th) {
+    run_p = p;
+    run_cg = p.algo == GFIX_CG;
+    run_total = 0;
+    *fin = false;
     if (reset(p)) return -1;
     if (theta_test(th)) return -1;
     if (*th < p.acc) {
       *iters = 0;
+      *fin = true;
       return 0;
     }
-    if (gx_sd_fixed != p.sd_fixed) {
-      if (gx_sd) cudaGraphExecDestroy(gx_sd);
-      gx_sd = nullptr;
-      gx_sd_fixed = p.sd_fixed;
-    }
-    ensure_graph(&gx_sd, false, p.sd_fixed != 0);
-    size_t total = 0;
-    for (;;) {
-      k_begin_run<<<1, 1, 0, s>>>(d_st);
-      LAUNCHED(1);
-      if (replay(gx_sd, false, p.sd_fixed != 0)) return -1;
-      *th = h_st->tr;
-      size_t loc = (size_t)h_st->iter;
-      if (loc >= p.max_iters) {
-        if (*th < 1E3 * p.acc) continue;  // loc_iters = 0, iters += 0
-        total = kSentinel;
+    if (run_cg) {
+      ensure_graph(&gx_cg, true, false);
+    } else {
+      if (gx_sd_fixed != p.sd_fixed) {
+        if (gx_sd) cudaGraphExecDestroy(gx_sd);
+        gx_sd = nullptr;
+        gx_sd_fixed = p.sd_fixed;
       }
-      total += loc;
-      *iters = total;
-      return 0;
+      ensure_graph(&gx_sd, false, p.sd_fixed != 0);
     }
+    run_head();
+    return 0;
+  }
+
+  cudaGraphExec_t run_exec() const { return run_cg ? gx_cg : gx_sd; }
+  cudaGraph_t run_graph() const { return run_cg ? gr_cg : gr_sd; }
+
+  int run_after(bool *fin, size_t *iters, double *th) {
+    *th = h_st->tr;
+    const size_t loc = (size_t)h_st->iter;
+    *fin = true;
+    if (loc >= run_p.max_iters) {
+      if (*th < 1E3 * run_p.acc) {  // continuation run
+        // (FASD: loc_iters = 0 again, nothing added)
+        *fin = false;
+        run_head();
+        return 0;
+      }
+      if (run_cg) {
+        *iters = kSentinel;
+        return 0;
+      }
+      run_total = kSentinel;
+    }
+    *iters = run_cg ? loc : run_total + loc;
+    return 0;
   }
 
   int solve(const Params &p, size_t *iters, double *th) {
-    return p.algo == GFIX_CG ? solve_facg(p, iters, th)
-                             : solve_fasd(p, iters, th);
+    bool fin = false;
+    if (run_start(p, &fin, iters, th)) return -1;
+    while (!fin) {
+      if (replay(run_exec(), run_cg, p.sd_fixed != 0)) return -1;
+      if (run_after(&fin, iters, th)) return -1;
+    }
+    return 0;
   }
 
   // Per-kernel device times of `n` CG iterations launched one by one with
@@ -1191,6 +1215,225 @@ static int landau_staged(Engine<double> *e64, const gfix_params *gp,
   return 0;
 }
 
+// ---------------------------------------------------------------------
+// Batches: many configurations, of any shapes, fixed together.  Every
+// configuration keeps its own engine (buffers, device control block,
+// iteration graph); one parent CUDA graph holds the iteration graph of every
+// unfinished configuration as a child, so one launch advances all of them
+// at once, concurrently.  A configuration that has converged turns its
+// kernels into no-ops through its own done flag (the per-instance mask);
+// the parent graph is rebuilt without it once a quarter of the live set has
+// finished.  Each configuration runs exactly the kernel sequence of a solve
+// of its own, so its results are those of gfix_landau.
+
+template <typename R>
+static int batch_solve(std::vector<Engine<R> *> &es, const Params &p,
+                       std::vector<size_t> &iters, std::vector<double> &th,
+                       cudaStream_t bs) {
+  const size_t n = es.size();
+  std::vector<char> fin(n, 0);
+  iters.assign(n, 0);
+  th.assign(n, 0.0);
+  bool graphs = true;
+  for (size_t i = 0; i < n; i++) {
+    bool f = false;
+    if (es[i]->run_start(p, &f, &iters[i], &th[i])) return -1;
+    fin[i] = f;
+    graphs &= es[i]->run_exec() != nullptr && es[i]->run_graph() != nullptr;
+  }
+  if (!graphs) {
+    // no graphs: one configuration after the other
+    for (size_t i = 0; i < n; i++) {
+      bool f = fin[i] != 0;
+      while (!f) {
+        if (es[i]->replay(es[i]->run_exec(), es[i]->run_cg, p.sd_fixed != 0))
+          return -1;
+        if (es[i]->run_after(&f, &iters[i], &th[i])) return -1;
+      }
+    }
+    return 0;
+  }
+  std::vector<cudaEvent_t> ev(n, nullptr);
+  for (auto &e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaGraphExec_t px = nullptr;
+  size_t built_live = 0, guard = 0;
+  unsigned long long per_replay = 0;
+  int batch = 2;
+  int rc = 0;
+  for (;;) {
+    std::vector<size_t> live;
+    for (size_t i = 0; i < n; i++)
+      if (!fin[i]) live.push_back(i);
+    if (live.empty()) break;
+    if (!px || live.size() * 4 <= built_live * 3) {
+      if (px) cudaGraphExecDestroy(px);
+      px = nullptr;
+      cudaGraph_t pg = nullptr;
+      per_replay = 0;
+      if (cudaGraphCreate(&pg, 0) != cudaSuccess) { rc = fail("graph create"); break; }
+      for (size_t i : live) {
+        cudaGraphNode_t node;
+        if (cudaGraphAddChildGraphNode(&node, pg, nullptr, 0,
+                                       es[i]->run_graph()) != cudaSuccess) {
+          rc = fail("child graph node: %s", cudaGetErrorString(cudaGetLastError()));
+          break;
+        }
+        per_replay += es[i]->per_iter_launches(es[i]->run_cg, p.sd_fixed != 0);
+      }
+      if (!rc && cudaGraphInstantiate(&px, pg, 0) != cudaSuccess) {
+        rc = fail("batch graph instantiate: %s",
+                  cudaGetErrorString(cudaGetLastError()));
+      }
+      cudaGraphDestroy(pg);
+      if (rc) break;
+      built_live = live.size();
+    }
+    // the heads of new runs were launched on the engines' own streams
+    for (size_t i : live) {
+      CK(cudaEventRecord(ev[i], es[i]->s));
+      CK(cudaStreamWaitEvent(bs, ev[i], 0));
+    }
+    for (int k = 0; k < batch; k++) {
+      CK(cudaGraphLaunch(px, bs));
+      LAUNCHED(per_replay);
+    }
+    for (size_t i : live)
+      CK(cudaMemcpyAsync(es[i]->h_st, es[i]->d_st, sizeof(DevState),
+                         cudaMemcpyDeviceToHost, bs));
+    CK(cudaStreamSynchronize(bs));
+    for (size_t i : live) {
+      if (!es[i]->h_st->done) continue;
+      bool f = false;
+      if (es[i]->run_after(&f, &iters[i], &th[i])) { rc = -1; break; }
+      fin[i] = f;
+    }
+    if (rc) break;
+    guard += batch;
+    if (guard > (size_t)p.max_iters * 64 + 1024) {
+      rc = fail("batch did not stop after %zu iterations", guard);
+      break;
+    }
+    batch = std::min(batch * 2, 32);
+  }
+  if (px) cudaGraphExecDestroy(px);
+  for (auto &e : ev) cudaEventDestroy(e);
+  return rc;
+}
+
+struct BatchInst {
+  size_t dims[4];
+  double *links = nullptr;  // host or device, double[V][4][9][2]
+  bool device = false;
+  std::unique_ptr<Engine<double>> e64;
+  std::unique_ptr<Engine<float>> e32;
+  gfix_result res;
+};
+
+struct Batch {
+  gfix_params p;
+  std::vector<std::unique_ptr<BatchInst>> inst;
+  cudaStream_t bs = nullptr;
+  ~Batch() {
+    inst.clear();
+    if (bs) cudaStreamDestroy(bs);
+  }
+};
+
+// mixed precision for a whole batch, phase by phase as landau_staged does
+// it for one configuration
+static int batch_run(Batch *b) {
+  const Params p = to_params(&b->p);
+  const size_t n = b->inst.size();
+  if (!n) return 0;
+  if (!b->bs) CK(cudaStreamCreateWithFlags(&b->bs, cudaStreamNonBlocking));
+  cudaEvent_t t0, t1;
+  CK(cudaEventCreate(&t0));
+  CK(cudaEventCreate(&t1));
+  CK(cudaDeviceSynchronize());
+  CK(cudaEventRecord(t0, b->bs));
+  std::vector<Engine<double> *> e64(n);
+  for (size_t i = 0; i < n; i++) {
+    BatchInst &I = *b->inst[i];
+    memset(&I.res, 0, sizeof I.res);
+    Engine<double> *e = I.e64.get();
+    e64[i] = e;
+    const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+    CK(cudaMemcpyAsync(e->d_aos, I.links, bytes,
+                       I.device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                       e->s));
+    if (e->from_aos(e->d_aos)) return -1;
+  }
+  std::vector<size_t> it32(n, 0), it64;
+  std::vector<double> th32(n, 0.0), th64;
+  Params p64 = p;
+  p64.traj_cap = 0;
+  if (b->p.precision == GFIX_MIXED) {
+    std::vector<Engine<float> *> e32(n);
+    for (size_t i = 0; i < n; i++) {
+      BatchInst &I = *b->inst[i];
+      if (!I.e32) {
+        I.e32 = std::make_unique<Engine<float>>();
+        if (I.e32->init(I.dims, true, false)) return -1;
+      }
+      e32[i] = I.e32.get();
+      CK(cudaStreamSynchronize(e64[i]->s));
+      k_convert<double, float><<<1184, 256, 0, e32[i]->s>>>(
+          e64[i]->d_U, e32[i]->d_U, (size_t)e64[i]->V * 36);
+      k_identity<float><<<(e64[i]->V + 255) / 256, 256, 0, e32[i]->s>>>(
+          e32[i]->d_G, e64[i]->V);
+      LAUNCHED(2);
+    }
+    Params p32 = p64;
+    p32.acc = std::max(b->p.switch_theta, b->p.accuracy);
+    if (batch_solve(e32, p32, it32, th32, b->bs)) return -1;
+    for (size_t i = 0; i < n; i++) {
+      Engine<double> *e = e64[i];
+      if (it32[i] == kSentinel || it32[i] > 0) {
+        cx<double> *G64 = e->c.fb[0];
+        k_convert<float, double><<<1184, 256, 0, e32[i]->s>>>(
+            e32[i]->d_G, G64, (size_t)e->V * 9);
+        LAUNCHED(1);
+        CK(cudaStreamSynchronize(e32[i]->s));
+        k_apply_gauge<<<e->nb_site, kSiteThreads, 0, e->s>>>(e->c, G64);
+        LAUNCHED(1);
+        double tt = 0.0;
+        if (e->reset(p64) || e->theta_test(&tt)) return -1;
+        if (!std::isfinite(th32[i]) || !std::isfinite(tt)) {
+          if (e->from_aos(e->d_aos)) return -1;
+          it32[i] = 0;
+          b->inst[i]->res.restarts++;
+        }
+      }
+    }
+  }
+  if (batch_solve(e64, p64, it64, th64, b->bs)) return -1;
+  for (size_t i = 0; i < n; i++) {
+    BatchInst &I = *b->inst[i];
+    Engine<double> *e = e64[i];
+    if (e->to_aos(e->d_aos)) return -1;
+    const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+    CK(cudaMemcpyAsync(I.links, e->d_aos, bytes,
+                       I.device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                       e->s));
+    const size_t f32 = (it32[i] == kSentinel) ? p.max_iters : it32[i];
+    I.res.iters_fp32 = b->p.precision == GFIX_MIXED ? f32 : 0;
+    I.res.iters = it64[i] == kSentinel ? kSentinel : I.res.iters_fp32 + it64[i];
+    I.res.theta = th64[i];
+  }
+  for (size_t i = 0; i < n; i++) {
+    CK(cudaEventRecord(b->inst[i]->e64->ev1, e64[i]->s));
+    CK(cudaStreamWaitEvent(b->bs, b->inst[i]->e64->ev1, 0));
+  }
+  CK(cudaEventRecord(t1, b->bs));
+  CK(cudaEventSynchronize(t1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, t0, t1));
+  for (auto &I : b->inst) I->res.gpu_ms = ms;
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  return 0;
+}
+
 }  // namespace gfix
 
 using namespace gfix;
@@ -1461,5 +1704,65 @@ int gfix_coulomb_device(double *d_links, const size_t dims[4],
   CK(cudaStreamSynchronize(e->s));
   return 0;
 }
+
+struct gfix_batch {
+  gfix::Batch b;
+};
+
+gfix_batch *gfix_batch_create(const gfix_params *p) {
+  if (!p) {
+    fail("null params");
+    return nullptr;
+  }
+  if (p->algo != GFIX_CG && p->algo != GFIX_SD) {
+    fail("unknown algo %d", p->algo);
+    return nullptr;
+  }
+  if (p->precision != GFIX_FP64 && p->precision != GFIX_MIXED) {
+    fail("unknown precision %d", p->precision);
+    return nullptr;
+  }
+  auto *b = new gfix_batch();
+  b->b.p = *p;
+  b->b.p.traj_theta = b->b.p.traj_func = nullptr;
+  b->b.p.traj_cap = 0;
+  return b;
+}
+
+static int batch_add(gfix_batch *b, double *links, const size_t dims[4],
+                     bool device) {
+  if (!b || !links) return fail("null batch or links");
+  if (check_params(dims, &b->b.p)) return -1;
+  auto I = std::make_unique<gfix::BatchInst>();
+  for (int k = 0; k < 4; k++) I->dims[k] = dims[k];
+  I->links = links;
+  I->device = device;
+  I->e64 = std::make_unique<Engine<double>>();
+  if (I->e64->init(dims, false, true)) return -1;
+  b->b.inst.push_back(std::move(I));
+  return (int)b->b.inst.size() - 1;
+}
+
+int gfix_batch_add(gfix_batch *b, double *links, const size_t dims[4]) {
+  return batch_add(b, links, dims, false);
+}
+
+int gfix_batch_add_device(gfix_batch *b, double *d_links, const size_t dims[4]) {
+  return batch_add(b, d_links, dims, true);
+}
+
+int gfix_batch_run(gfix_batch *b) {
+  if (!b) return fail("null batch");
+  return gfix::batch_run(&b->b);
+}
+
+int gfix_batch_result(const gfix_batch *b, int i, gfix_result *r) {
+  if (!b || !r || i < 0 || (size_t)i >= b->b.inst.size())
+    return fail("no configuration %d in the batch", i);
+  *r = b->b.inst[(size_t)i]->res;
+  return 0;
+}
+
+void gfix_batch_destroy(gfix_batch *b) { delete b; }
 
 }  // extern "C"

@@ -135,6 +135,39 @@ def _coulomb(ptr, cd, d, gf_alpha, accuracy, max_iters, algo, sd_fixed_step,
                      sit.astype(np.int64), int(r.restarts))
 
 
+def landau_batch(configs, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
+                 algo="FACG", sd_fixed_step=False, precision="FP64",
+                 switch_theta=1e-9) -> list:
+    """Landau FA gauge fixing of many configurations in one batch
+    (gfix_batch_*): `configs` is a sequence of (links, dims); returns one
+    FixResult per configuration, in order, each equal to landau_fix's."""
+    lib = _lib.load()
+    p, _, _ = _params(gf_alpha, accuracy, max_iters, algo, sd_fixed_step,
+                      precision, switch_theta, 0)
+    b = lib.gfix_batch_create(C.byref(p))
+    if not b:
+        check(-1)
+    try:
+        bufs = []
+        for links, dims in configs:
+            cd, d = _dims(dims)
+            U = _links(links, d)
+            bufs.append((U, cd))
+            if lib.gfix_batch_add(b, U.ctypes.data, cd) < 0:
+                check(-1)
+        check(lib.gfix_batch_run(b))
+        out = []
+        for i, (U, _) in enumerate(bufs):
+            r = GfixResult()
+            check(lib.gfix_batch_result(b, i, C.byref(r)))
+            out.append(FixResult(U, int(r.iters), float(r.theta),
+                                 int(r.iters_fp32), float(r.gpu_ms),
+                                 restarts=int(r.restarts)))
+        return out
+    finally:
+        lib.gfix_batch_destroy(b)
+
+
 # --- GLU-named entry points -------------------------------------------------
 
 def FACG(links, dims, gf_alpha, acc, max_iters, **kw):

@@ -131,6 +131,31 @@ int gfix_coulomb_device(double *d_links, const size_t dims[4],
                         const gfix_params *p, gfix_result *r,
                         double *slice_theta, size_t *slice_iters);
 
+/* Batches: many configurations, of any shapes, Landau-fixed together (no
+ * counterpart in GLU, which fixes one configuration per call).  Every
+ * configuration keeps its own device workspace; one CUDA graph launch
+ * advances all unfinished ones concurrently, and a converged configuration
+ * drops out (its kernels turn into no-ops, the graph is rebuilt without it
+ * as the live set shrinks).  Each configuration's result equals that of
+ * gfix_landau with the same parameters (trajectories are not recorded).
+ *
+ *   gfix_batch *b = gfix_batch_create(&p);
+ *   gfix_batch_add(b, links_a, dims_a);         // index 0
+ *   gfix_batch_add(b, links_b, dims_b);         // index 1
+ *   gfix_batch_run(b);                           // links fixed in place
+ *   gfix_batch_result(b, 0, &r);
+ *   gfix_batch_destroy(b);
+ *
+ * add returns the configuration's index or -1; the links must stay valid
+ * until the run returns.  gfix_batch_add_device takes links in HBM. */
+typedef struct gfix_batch gfix_batch;
+gfix_batch *gfix_batch_create(const gfix_params *p);
+int gfix_batch_add(gfix_batch *b, double *links, const size_t dims[4]);
+int gfix_batch_add_device(gfix_batch *b, double *d_links, const size_t dims[4]);
+int gfix_batch_run(gfix_batch *b);
+int gfix_batch_result(const gfix_batch *b, int i, gfix_result *r);
+void gfix_batch_destroy(gfix_batch *b);
+
 /* Observables on host links: theta_test_lin (src/Gfix/gftests.c:214-250),
  * gauge functional (gftests.c:132-147), average plaquette
  * (src/Field/plaqs_links.c:243-265).  out[0..2] in that order. */

@@ -1,0 +1,90 @@
+"""Batches of configurations (gfix_batch_*): every configuration of a batch
+must come out exactly as from its own gfix_landau call -- the batch runs
+each configuration's kernel sequence unchanged, only concurrently, with
+converged configurations masked out.  All calls go through the C ABI."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from glu_b200 import gfix  # noqa: E402
+from glu_b200._lib import GfixError  # noqa: E402
+from glu_b200.workload import random_su3, tiled_config  # noqa: E402
+
+
+def _dims(g):
+    return tuple(int(d) for d in g["dims"])
+
+
+def _transformed(U, dims, seed):
+    """U under a seeded random gauge transformation (same orbit)."""
+    rng = np.random.default_rng(seed)
+    V = U.shape[0]
+    g = random_su3(V, rng)
+    Lx, Ly, Lz, Lt = dims
+    idx = np.arange(V).reshape(Lt, Lz, Ly, Lx)
+    out = np.empty_like(U)
+    for mu, ax in enumerate((3, 2, 1, 0)):
+        fwd = np.roll(idx, -1, axis=ax).reshape(V)
+        out[:, mu] = g @ U[:, mu] @ np.conj(np.swapaxes(g[fwd], -1, -2))
+    return out
+
+
+@pytest.fixture(scope="module")
+def configs(lat400, hb8):
+    d4 = _dims(lat400)
+    d8 = _dims(hb8)
+    d16 = (16, 8, 8, 16)
+    return [
+        (lat400["links"], d4),
+        (_transformed(lat400["links"], d4, 5), d4),
+        (hb8["links"], d8),
+        (tiled_config(d16, seed=7), d16),
+        (_transformed(hb8["links"], d8, 9), d8),
+    ]
+
+
+@pytest.mark.parametrize("algo,precision,acc", [("FACG", "FP64", 1e-14),
+                                                ("FASD", "FP64", 1e-12),
+                                                ("FACG", "MIXED", 1e-14),
+                                                ("FASD", "MIXED", 1e-12)])
+def test_batch_equals_single_solves(configs, algo, precision, acc):
+    kw = dict(gf_alpha=0.08, accuracy=acc, max_iters=4000, algo=algo,
+              precision=precision, switch_theta=1e-9)
+    got = gfix.landau_batch(configs, **kw)
+    assert len(got) == len(configs)
+    for (U, d), r in zip(configs, got):
+        one = gfix.landau_fix(U, d, **kw)
+        assert r.iters == one.iters and r.iters_fp32 == one.iters_fp32
+        assert r.theta == one.theta
+        assert np.array_equal(r.links, one.links)
+        assert r.theta < acc
+
+
+def test_batch_of_one_and_repeated_runs(lat400):
+    d = _dims(lat400)
+    a = gfix.landau_batch([(lat400["links"], d)])[0]
+    b = gfix.landau_batch([(lat400["links"], d)])[0]
+    one = gfix.landau_fix(lat400["links"], d)
+    assert a.iters == b.iters == one.iters
+    assert np.array_equal(a.links, one.links) and np.array_equal(b.links, one.links)
+
+
+def test_empty_batch_and_bad_index():
+    assert gfix.landau_batch([]) == []
+    from glu_b200 import _lib
+    import ctypes as C
+    lib = _lib.load()
+    p, _, _ = gfix._params(0.08, 1e-14, 100, "FACG", False, "FP64", 1e-9, 0)
+    b = lib.gfix_batch_create(C.byref(p))
+    try:
+        r = _lib.GfixResult()
+        assert lib.gfix_batch_result(b, 0, C.byref(r)) != 0
+        with pytest.raises(GfixError):
+            _lib.check(lib.gfix_batch_result(b, 3, C.byref(r)))
+    finally:
+        lib.gfix_batch_destroy(b)
