@@ -54,9 +54,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--workload", default="landau", choices=["landau", "coulomb"],
+    ap.add_argument("--workload", default="landau",
+                    choices=["landau", "coulomb", "ensemble"],
                     help="landau: 32^3x64 Landau FACG (the headline); coulomb: "
-                         "64^3x128 Coulomb FACG, all slices batched")
+                         "64^3x128 Coulomb FACG, all slices batched; ensemble: "
+                         "48 x 16^3x32 + 16 x 24^3x48 Landau FASD in one batch")
     ap.add_argument("--dims", default=None,
                     help="lattice extents; default 32,32,32,64 (landau) or "
                          "64,64,64,128 (coulomb)")
@@ -284,8 +286,8 @@ def reference_iters(dims):
     return None, None
 
 
-def cpu_sample(U, dims, sample_s: float, nthreads: int):
-    """Seconds per FACG iteration of the reference (oracle/_ref) with
+def cpu_sample(U, dims, sample_s: float, nthreads: int, algo: str = "FACG"):
+    """Seconds per FACG (FASD) iteration of the reference (oracle/_ref) with
     nthreads OpenMP threads, from two runs of k1 < k2 iterations (acc 1e-30:
     exactly k iterations, no continuation), and the fixed cost of a call."""
     from oracle.oracle import REF_SO, Oracle, Reference
@@ -298,7 +300,7 @@ def cpu_sample(U, dims, sample_s: float, nthreads: int):
             R.put_links(U)
             R.lib.ref_reset_fft_seconds()
             t = time.perf_counter()
-            R.landau_fa(1e-30, k, "FACG")
+            R.landau_fa(1e-30, k, algo)
             return time.perf_counter() - t, R.fft_seconds()
     else:  # the oracle port, single threaded
         O = Oracle()
@@ -306,7 +308,7 @@ def cpu_sample(U, dims, sample_s: float, nthreads: int):
 
         def run(k):
             t = time.perf_counter()
-            O.landau(U, dims, ALPHA, 1e-30, k, "FACG")
+            O.landau(U, dims, ALPHA, 1e-30, k, algo)
             return time.perf_counter() - t, 0.0
     t1, f1 = run(1)
     k2 = max(2, int(sample_s / max(t1, 1e-3)))
@@ -729,6 +731,204 @@ def coulomb_main(args, dims, rank, world, local):
         emit(coulomb_line(args, dims, world, res, cpu))
 
 
+# ---------------------------------------------------------------------------
+# Ensemble workload: 48 configurations of 16^3x32 and 16 of 24^3x48 fixed in
+# one batch (gfix_batch_*), Landau FASD to theta < 1e-12, mixed precision.
+# A step is the fix of the whole ensemble; value counts configurations.
+
+E_GROUPS = ((48, (16, 16, 16, 32)), (16, (24, 24, 24, 48)))
+E_ACC = 1e-12
+
+
+def e_metric_name() -> str:
+    return ("gauge-fixed configs/hour (ensemble 48x16^3x32 + 16x24^3x48, "
+            "Landau FASD, theta<1e-12)")
+
+
+def ensemble_configs(rank: int = 0):
+    """(dims, links) per configuration: the 8^4 heatbath stand-in tiled to
+    the shape, each with its own seeded gauge transformation (seeds
+    100..163, offset by 64 per rank)."""
+    from glu_b200.workload import tiled_config
+    out, seed = [], 100 + 64 * rank
+    for n, dims in E_GROUPS:
+        for _ in range(n):
+            out.append((dims, tiled_config(dims, seed=seed)))
+            seed += 1
+    return out
+
+
+def _eparams(prec: str):
+    p = _params(prec)
+    p.algo = 1          # FASD (line search)
+    p.accuracy = E_ACC
+    return p
+
+
+def ensemble_main(args, rank, world, local):
+    import ctypes as C
+    import torch
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cfgs = ensemble_configs(0)
+        rec = ensemble_iters_record()
+        if rec is None:
+            emit({"impl": "reference", "unavailable":
+                  "no recorded FASD iteration counts of the ensemble"})
+            return
+        cores = os.cpu_count() or 1
+        t_fix = 0.0
+        samples = []
+        for n, dims in E_GROUPS:
+            U = next(u for d, u in cfgs if d == dims)
+            s = cpu_sample(U, dims, args.cpu_sample_s / 2, cores, "FASD")
+            samples.append(s)
+            t_fix += n * s["fixed_s"] + s["s_iter"] * rec[str(dims[0])]
+        value = len(cfgs) * 3600.0 / t_fix
+        emit({"metric": e_metric_name(), "value": value, "unit": UNIT,
+              "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+              "ms_per_step": t_fix * 1e3, "higher_is_better": True,
+              "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+              "data": "synthetic (8^4 GLU heatbath tiled + random gauge)",
+              "config": {"workload": "ensemble 48x16^3x32 + 16x24^3x48 Landau FASD theta<1e-12",
+                         "parallelism": "host OpenMP, one configuration at a time"},
+              "impl": "reference",
+              "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores,
+                               "kind": samples[0]["kind"],
+                               "sample": "; ".join("%s: %d FASD iterations, %.3f s/iteration"
+                                                   % ("x".join(map(str, d)), s["sample_iters"], s["s_iter"])
+                                                   for (n, d), s in zip(E_GROUPS, samples))},
+              "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                      "d2h_bytes_per_step": 0}})
+        return
+    torch.cuda.set_device(local)
+    from glu_b200 import _lib
+    from glu_b200._lib import GfixResult, check
+    lib = _lib.load()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    cfgs = ensemble_configs(rank)
+    pristine = [torch.from_numpy(u.view(np.float64).reshape(-1)).to("cuda") for _, u in cfgs]
+    work = [torch.empty_like(t) for t in pristine]
+    hwork = [torch.empty(t.shape, dtype=torch.float64, pin_memory=True) for t in pristine]
+    cds = [(C.c_size_t * 4)(*d) for d, _ in cfgs]
+    nbytes = sum(t.numel() * 8 for t in pristine)
+    sites = sum(int(np.prod(d)) for d, _ in cfgs)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    out = {}
+    with Clocks(local) as clk:
+        for prec in ([args.precision, "fp64"] if args.precision == "mixed" else ["fp64"]):
+            p = _eparams(prec)
+            res = {}
+            for mode in ("device", "host"):
+                b = lib.gfix_batch_create(C.byref(p))
+                if not b:
+                    check(-1)
+                try:
+                    for i in range(len(cfgs)):
+                        ptr = work[i].data_ptr() if mode == "device" else hwork[i].data_ptr()
+                        add = lib.gfix_batch_add_device if mode == "device" else lib.gfix_batch_add
+                        if add(b, ptr, cds[i]) < 0:
+                            check(-1)
+                    ms = 0.0
+                    l0 = 0
+                    for k in range(args.warmup + args.steps):
+                        if k == args.warmup:
+                            l0 = lib.gfix_kernel_launches()
+                        for i in range(len(cfgs)):
+                            (work[i] if mode == "device" else hwork[i]).copy_(pristine[i])
+                        barrier()
+                        a, e = ev(), ev()
+                        a.record()
+                        check(lib.gfix_batch_run(b))
+                        e.record()
+                        barrier()
+                        if k >= args.warmup:
+                            ms += a.elapsed_time(e)
+                    launches = lib.gfix_kernel_launches() - l0
+                    its = []
+                    for i in range(len(cfgs)):
+                        r = GfixResult()
+                        check(lib.gfix_batch_result(b, i, C.byref(r)))
+                        its.append((int(r.iters), int(r.iters_fp32), float(r.theta)))
+                    res[mode] = dict(ms=max_over_ranks(ms), iters=its, launches=launches)
+                finally:
+                    lib.gfix_batch_destroy(b)
+            out[prec] = res
+    prec = args.precision
+    steps = args.steps
+    n = len(cfgs)
+    o = out[prec]["device"]
+    line = {
+        "metric": e_metric_name(), "value": world * n * steps * 3600e3 / o["ms"],
+        "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": o["ms"] / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if prec == "mixed" else "f64",
+        "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled to each shape + seeded random gauge transforms, seeds 100-163)",
+        "config": {"workload": "ensemble 48x16^3x32 + 16x24^3x48 Landau FASD theta<1e-12",
+                   "configs": n, "sites": sites, "precision": prec,
+                   "switch_theta": 1e-9 if prec == "mixed" else None,
+                   "iters_min_max": [min(x[0] for x in o["iters"]), max(x[0] for x in o["iters"])],
+                   "iters_total": sum(x[0] for x in o["iters"]),
+                   "final_theta_max": max(x[2] for x in o["iters"]),
+                   "fp64_only": {"value": world * n * steps * 3600e3 / out["fp64"]["device"]["ms"],
+                                 "ms_per_step": out["fp64"]["device"]["ms"] / steps,
+                                 "iters_total": sum(x[0] for x in out["fp64"]["device"]["iters"]),
+                                 "e2e": world * n * steps * 3600e3 / out["fp64"]["host"]["ms"]},
+                   "l2": "inputs (%.2f GB of links) larger than the 126 MB L2" % (nbytes / 1e9),
+                   "parallelism": "one batch per GPU" if world > 1 else "single GPU, one batch"},
+        "e2e": {"value": world * n * steps * 3600e3 / out[prec]["host"]["ms"], "unit": UNIT,
+                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+        "gpu_launches": o["launches"],
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            f64 = out["fp64"]["device"]["iters"]
+            t_fix = 0.0
+            desc = []
+            cores = os.cpu_count() or 1
+            i0 = 0
+            for cnt, dims in E_GROUPS:
+                s = cpu_sample(cfgs[i0][1], dims, args.cpu_sample_s / 2, cores, "FASD")
+                its = sum(x[0] for x in f64[i0:i0 + cnt])
+                t_fix += cnt * s["fixed_s"] + s["s_iter"] * its
+                desc.append("%s: %d FASD iterations sampled, %.3f s/iteration x %d iterations"
+                            % ("x".join(map(str, dims)), s["sample_iters"], s["s_iter"], its))
+                i0 += cnt
+            line["cpu_baseline"] = {"value": n * 3600.0 / t_fix, "unit": UNIT,
+                                    "cores": cores, "kind": s["kind"], "sample": "; ".join(desc)}
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "kind": "unavailable", "sample": str(e)}
+    if rank == 0:
+        emit(line)
+
+
+def ensemble_iters_record():
+    f = ROOT / "profiles" / "ensemble_fix.json"
+    if f.exists():
+        return json.loads(f.read_text()).get("fasd_fp64_iters_by_group")
+    return None
+
+
 def main():
     args = parse()
     if args.dims is None:
@@ -737,6 +937,9 @@ def main():
     rank, world, local = dist_env()
     if args.workload == "coulomb":
         coulomb_main(args, dims, rank, world, local)
+        return
+    if args.workload == "ensemble":
+        ensemble_main(args, rank, world, local)
         return
     if args.profile_only:
         profile_only(args, dims)
