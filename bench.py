@@ -65,6 +65,10 @@ def parse():
     ap.add_argument("--profile-iters", type=int, default=20)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="coulomb: one configuration's time slices split over "
+                         "the ranks (strong scaling; ring exchange of the "
+                         "boundary gauge field) instead of one per rank")
     ap.add_argument("--profile-only", action="store_true",
                     help="only the per-kernel event timing of --profile-iters "
                          "CG iterations (a short, bounded launch list for ncu)")
@@ -675,6 +679,94 @@ def coulomb_profile_only(args, dims):
                       for k in range(7)}})
 
 
+def coulomb_shard(args, dims, rank, world, local):
+    """One configuration, its time slices split over the ranks
+    (glu_b200.shard): every step fixes the whole configuration."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    from glu_b200.shard import coulomb_sharded, slice_blocks
+    from glu_b200.workload import tiled_config_device
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    t0, t1 = slice_blocks(dims[3], world)[rank]
+    lcu = dims[0] * dims[1] * dims[2]
+    U = tiled_config_device(dims, seed=4)
+    block = torch.view_as_real(U[t0 * lcu:t1 * lcu]).reshape(-1).contiguous()
+    del U
+    bdims = (dims[0], dims[1], dims[2], t1 - t0)
+    work = torch.empty_like(block)
+    hwork = torch.empty(block.shape, dtype=torch.float64, pin_memory=True)
+    p = _cparams(args.precision)
+    from glu_b200 import _lib
+    lib = _lib.load()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    with Clocks(local) as clk:
+        ms, e_ms, iters = 0.0, 0.0, 0
+        l0 = 0
+        for k in range(args.warmup + args.steps):
+            if k == args.warmup:
+                l0 = lib.gfix_kernel_launches()
+            work.copy_(block)
+            barrier()
+            a, b = ev(), ev()
+            a.record()
+            r = coulomb_sharded(work, bdims, params=p)
+            b.record()
+            barrier()
+            if k >= args.warmup:
+                ms += a.elapsed_time(b)
+                iters = r.iters
+        launches = lib.gfix_kernel_launches() - l0
+        for _ in range(args.steps):
+            hwork.copy_(block)
+            barrier()
+            a, b = ev(), ev()
+            a.record()
+            work.copy_(hwork, non_blocking=True)
+            coulomb_sharded(work, bdims, params=p)
+            hwork.copy_(work)
+            b.record()
+            barrier()
+            e_ms += a.elapsed_time(b)
+    ms, e_ms = max_over_ranks(ms), max_over_ranks(e_ms)
+    if rank == 0:
+        steps = args.steps
+        emit({"metric": c_metric_name(dims), "value": steps * 3600e3 / ms, "unit": UNIT,
+              "n_gpus": world, "steps": steps, "warmup": args.warmup,
+              "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "strong",
+              "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+              "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled + seeded random gauge transform, on device)",
+              "config": {"workload": "Coulomb FACG theta<1e-14 per slice, %s, slices split over ranks"
+                                     % "x".join(map(str, dims)),
+                         "dims": list(dims), "precision": args.precision, "iters": iters,
+                         "slices_per_rank": t1 - t0,
+                         "l2": "inputs larger than the 126 MB L2",
+                         "parallelism": "time slices sharded over %d GPUs, ring exchange of "
+                                        "one slice's gauge field" % world},
+              "e2e": {"value": steps * 3600e3 / e_ms, "unit": UNIT,
+                      "h2d_bytes_per_step": block.numel() * 8 * world,
+                      "d2h_bytes_per_step": block.numel() * 8 * world},
+              "gpu_launches": launches, "clocks": clk.summary()})
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def coulomb_main(args, dims, rank, world, local):
     if args.profile_only:
         coulomb_profile_only(args, dims)
@@ -711,6 +803,9 @@ def coulomb_main(args, dims, rank, world, local):
                                             dims[2], s_step, n_steps)},
               "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                       "d2h_bytes_per_step": 0}})
+        return
+    if args.shard:
+        coulomb_shard(args, dims, rank, world, local)
         return
     res, U2 = coulomb_gpu(args, dims, rank, world, local)
     cpu = None

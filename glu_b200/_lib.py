@@ -37,7 +37,8 @@ EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
            "gfix_profile_landau", "gfix_profile_coulomb",
            "gfix_theta_functional_noalloc", "gfix_batch_create",
            "gfix_batch_add", "gfix_batch_add_device", "gfix_batch_run",
-           "gfix_batch_result", "gfix_batch_destroy",
+           "gfix_batch_result", "gfix_batch_destroy", "gfix_coulomb_slices",
+           "gfix_coulomb_slices_finish",
            "gfix_noalloc_error",
            "gfix_last_error", "gfix_release", "gfix_kernel_launches")
 
@@ -74,6 +75,13 @@ def load(path: Path | str | None = None):
     lib.gfix_reunit.argtypes = [C.c_void_p, _szp]
     lib.gfix_fourier_accelerate.restype = C.c_int
     lib.gfix_fourier_accelerate.argtypes = [C.c_void_p, _szp, C.c_int]
+    lib.gfix_coulomb_slices.restype = C.c_int
+    lib.gfix_coulomb_slices.argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
+                                        C.POINTER(GfixResult), _dp, _szp, C.c_void_p,
+                                        C.c_void_p]
+    lib.gfix_coulomb_slices_finish.restype = C.c_int
+    lib.gfix_coulomb_slices_finish.argtypes = [C.c_void_p, _szp, C.c_void_p,
+                                               C.c_void_p]
     lib.gfix_batch_create.restype = C.c_void_p
     lib.gfix_batch_create.argtypes = [C.POINTER(GfixParams)]
     for fn in ("gfix_batch_add", "gfix_batch_add_device"):

@@ -484,7 +484,10 @@ __global__ void k_cscalar(CoulState *cs, Slice *sl, const double *part,
 
 // the slice transforms of Coulomb_FA (gtransform_slice, src/Gfix/gtrans.c:
 // 214-238): U_i(x,t) <- g_t(x) U_i(x,t) g_t(x+i)^dag for i < 3 and
-// U_t(x,t) <- g_t(x) U_t(x,t) g_{t+1}(x)^dag, periodic in t
+// U_t(x,t) <- g_t(x) U_t(x,t) g_{t+1}(x)^dag.  ALL_T: every temporal link,
+// periodic in t (a whole lattice); otherwise the last slice's temporal links
+// are left for k_cfinish_aos (a block of slices whose successor slice lives
+// elsewhere).
 template <typename R, int MU>
 __device__ __forceinline__ void cslice_link(const CCtx<R> &c, const SliceSite &q,
                                             int s, int t, const cx<R> *A) {
@@ -498,7 +501,8 @@ __device__ __forceinline__ void cslice_link(const CCtx<R> &c, const SliceSite &q
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kCoulThreads) k_cslice_transform(CCtx<R> c) {
+__global__ void __launch_bounds__(kCoulThreads) k_cslice_transform(CCtx<R> c,
+                                                                   int all_t) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= c.V) return;
   const int t = s / c.Lcu;
@@ -508,7 +512,44 @@ __global__ void __launch_bounds__(kCoulThreads) k_cslice_transform(CCtx<R> c) {
   cslice_link<R, 0>(c, q, s, t, A);
   cslice_link<R, 1>(c, q, s, t, A);
   cslice_link<R, 2>(c, q, s, t, A);
-  cslice_link<R, 3>(c, q, s, t, A);
+  if (all_t || t < c.L[3] - 1) cslice_link<R, 3>(c, q, s, t, A);
+}
+
+// the temporal links of the last local slice, U_t <- g_last U_t g_next^dag,
+// in the caller's AoS links (double[V][4][9][2]); g_last and g_next are the
+// fields of that slice and of the following one (double[9][Lcu][2])
+__global__ void __launch_bounds__(kCoulThreads)
+    k_cfinish_aos(double2 *links, const double2 *g_last, const double2 *g_next,
+                  int V, int Lcu) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Lcu) return;
+  const int s = V - Lcu + i;
+  cx<double> A[9], B[9], U[9];
+#pragma unroll
+  for (int e = 0; e < 9; e++) {
+    const double2 a = g_last[(size_t)e * Lcu + i];
+    const double2 b = g_next[(size_t)e * Lcu + i];
+    A[e] = mk<double>(a.x, a.y);
+    B[e] = mk<double>(b.x, b.y);
+  }
+  double2 *u = links + ((size_t)s * 4 + 3) * 9;
+#pragma unroll
+  for (int e = 0; e < 9; e++) U[e] = mk<double>(u[e].x, u[e].y);
+  gtransform(A, U, B);
+#pragma unroll
+  for (int e = 0; e < 9; e++) u[e] = make_double2(U[e].x, U[e].y);
+}
+
+// g of local slice t, exported as double[9][Lcu][2]
+__global__ void k_cexport_slice(const cx<double> *g, double2 *out, int V,
+                                int Lcu, int t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= Lcu) return;
+#pragma unroll
+  for (int e = 0; e < 9; e++) {
+    const cx<double> v = g[(size_t)e * V + (size_t)t * Lcu + i];
+    out[(size_t)e * Lcu + i] = make_double2(v.x, v.y);
+  }
 }
 
 // in / in_old and sn ping-pong after every step of every live slice

@@ -896,10 +896,12 @@ class Engine {
     return 0;
   }
 
-  // transform = false leaves the links untouched (a mixed-precision phase)
+  // transform: 0 leaves the links untouched (a mixed-precision phase), 1
+  // the slice transforms of a whole lattice, 2 all but the last slice's
+  // temporal links (a block of slices of a larger lattice)
   int csolve(const Params &p, size_t *iters, double *slice_theta,
              size_t *slice_iters, size_t *traj_len, bool identity = true,
-             bool transform = true) {
+             int transform = 1) {
     if (cstart(p, identity)) return -1;
     const int T = c.L[3];
     const size_t per = p.traj_cap ? p.traj_cap / T : 0;
@@ -930,7 +932,7 @@ class Engine {
     }
     if (transform) {
       k_cslice_transform<R><<<(V + kCoulThreads - 1) / kCoulThreads,
-                              kCoulThreads, 0, s>>>(cc);
+                              kCoulThreads, 0, s>>>(cc, transform == 1);
       LAUNCHED(1);
     }
     CK(cudaMemcpyAsync(h_sl, d_sl, sizeof(Slice) * T, cudaMemcpyDeviceToHost,
@@ -1587,7 +1589,7 @@ int gfix_profile_landau(const double *d_links, const size_t dims[4],
 // g = 1).  Trajectories then hold the FP64 phase.
 static int coulomb_staged(Engine<double> *e, const gfix_params *gp,
                           gfix_result *r, double *slice_theta,
-                          size_t *slice_iters) {
+                          size_t *slice_iters, int transform = 1) {
   const Params p = to_params(gp);
   const int T = e->c.L[3];
   std::vector<double> th(T), th32(T);
@@ -1609,7 +1611,7 @@ static int coulomb_staged(Engine<double> *e, const gfix_params *gp,
     p32.acc = gp->switch_theta;
     p32.traj_cap = 0;
     p32.traj_theta = p32.traj_func = nullptr;
-    if (f->csolve(p32, &n32, th32.data(), it32.data(), nullptr, true, false))
+    if (f->csolve(p32, &n32, th32.data(), it32.data(), nullptr, true, 0))
       return -1;
     bool finite = true;
     for (int t = 0; t < T; t++) finite &= std::isfinite(th32[t]) != 0;
@@ -1628,7 +1630,8 @@ static int coulomb_staged(Engine<double> *e, const gfix_params *gp,
       res.restarts++;
     }
   }
-  if (e->csolve(p, &iters, th.data(), it.data(), &tl, !from_g, true)) return -1;
+  if (e->csolve(p, &iters, th.data(), it.data(), &tl, !from_g, transform))
+    return -1;
   CK(cudaEventRecord(e->ev1, e->s));
   if (e->to_aos(e->d_aos)) return -1;
   CK(cudaStreamSynchronize(e->s));
@@ -1687,6 +1690,45 @@ int gfix_profile_coulomb(const double *d_links, const size_t dims[4],
     return f->profile_coul(to_params(p), iters, ms, bytes);
   }
   return e->profile_coul(to_params(p), iters, ms, bytes);
+}
+
+int gfix_coulomb_slices(double *d_links, const size_t dims[4],
+                        const gfix_params *p, gfix_result *r,
+                        double *slice_theta, size_t *slice_iters,
+                        double *d_g_first, double *d_g_last) {
+  if (check_params(dims, p)) return -1;
+  if (!d_links || !d_g_first || !d_g_last) return fail("null links or g buffer");
+  Engine<double> *e = engine_coul(dims);
+  if (!e) return -1;
+  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpyAsync(e->d_aos, d_links, bytes, cudaMemcpyDeviceToDevice, e->s));
+  if (coulomb_staged(e, p, r, slice_theta, slice_iters, 2)) return -1;
+  CK(cudaMemcpyAsync(d_links, e->d_aos, bytes, cudaMemcpyDeviceToDevice, e->s));
+  const unsigned nb = (unsigned)((e->Lcu + 127) / 128);
+  k_cexport_slice<<<nb, 128, 0, e->s>>>(e->d_G, reinterpret_cast<double2 *>(d_g_first),
+                                       e->V, e->Lcu, 0);
+  k_cexport_slice<<<nb, 128, 0, e->s>>>(e->d_G, reinterpret_cast<double2 *>(d_g_last),
+                                       e->V, e->Lcu, e->c.L[3] - 1);
+  LAUNCHED(2);
+  CK(cudaStreamSynchronize(e->s));
+  return 0;
+}
+
+int gfix_coulomb_slices_finish(double *d_links, const size_t dims[4],
+                               const double *d_g_last, const double *d_g_next) {
+  if (!d_links || !d_g_last || !d_g_next || !dims) return fail("null argument");
+  for (int i = 0; i < 4; i++)
+    if (dims[i] < 2) return fail("extent %zu of dimension %d below 2", dims[i], i);
+  const size_t lcu = dims[0] * dims[1] * dims[2], V = lcu * dims[3];
+  if (V > (size_t)INT32_MAX / 4) return fail("lattice volume %zu too large", V);
+  CK(cudaDeviceSynchronize());
+  k_cfinish_aos<<<(unsigned)((lcu + 127) / 128), 128>>>(
+      reinterpret_cast<double2 *>(d_links), reinterpret_cast<const double2 *>(d_g_last),
+      reinterpret_cast<const double2 *>(d_g_next), (int)V, (int)lcu);
+  LAUNCHED(1);
+  CK(cudaDeviceSynchronize());
+  return 0;
 }
 
 int gfix_coulomb_device(double *d_links, const size_t dims[4],

@@ -156,6 +156,24 @@ int gfix_batch_run(gfix_batch *b);
 int gfix_batch_result(const gfix_batch *b, int i, gfix_result *r);
 void gfix_batch_destroy(gfix_batch *b);
 
+/* Coulomb fixing of one rank's block of time slices of a larger lattice
+ * (slices are independent problems; GLU's Coulomb_FA, CFACG.c:531-636,
+ * fixes them one after the other).  d_links: the block's links in HBM,
+ * double[V][4][9][2] for dims = {Lx, Ly, Lz, T_block >= 2}.  Solves every
+ * slice, applies the slice transforms except to the temporal links of the
+ * block's last slice, and writes the gauge fields of the block's first and
+ * last slices to d_g_first / d_g_last (double[9][Lx Ly Lz][2] in HBM).
+ * gfix_coulomb_slices_finish then transforms those last temporal links with
+ * d_g_last and the following block's d_g_first (d_g_next, from the rank
+ * that owns the following slice).  Over all blocks this equals gfix_coulomb
+ * on the whole lattice, bit for bit. */
+int gfix_coulomb_slices(double *d_links, const size_t dims[4],
+                        const gfix_params *p, gfix_result *r,
+                        double *slice_theta, size_t *slice_iters,
+                        double *d_g_first, double *d_g_last);
+int gfix_coulomb_slices_finish(double *d_links, const size_t dims[4],
+                               const double *d_g_last, const double *d_g_next);
+
 /* Observables on host links: theta_test_lin (src/Gfix/gftests.c:214-250),
  * gauge functional (gftests.c:132-147), average plaquette
  * (src/Field/plaqs_links.c:243-265).  out[0..2] in that order. */

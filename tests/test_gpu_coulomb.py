@@ -207,3 +207,43 @@ def test_mixed_precision_reaches_fp64_accuracy(case, request):
     assert np.abs(tr(r.links) - tr(r64.links)).max() < 1e-5
     fs = lambda U: 1.0 - tr(U).real.sum() / (9.0 * U.shape[0])  # noqa: E731
     assert abs(fs(r.links) - fs(r64.links)) < 1e-13
+
+
+@pytest.mark.parametrize("blocks", [[(0, 4), (4, 8)], [(0, 2), (2, 5), (5, 8)]])
+def test_slice_blocks_equal_whole_lattice(lat400, blocks):
+    """gfix_coulomb_slices on blocks of slices (one per rank in a sharded
+    fix), the boundary fields passed along the ring, then
+    gfix_coulomb_slices_finish: bit-equal to gfix_coulomb on the whole."""
+    import ctypes as C
+    from glu_b200 import _lib
+    from glu_b200._lib import GfixResult, check
+    g = lat400
+    d = _dims(g)
+    whole = gfix.coulomb_fix(g["links"], d, 0.09, ACC, 650, "FACG")
+    lib = _lib.load()
+    p, _, _ = gfix._params(0.09, ACC, 650, "FACG", False, "FP64", 1e-9, 0)
+    lcu = d[0] * d[1] * d[2]
+    U = np.ascontiguousarray(g["links"])
+    dev, gf, gl, its = [], [], [], []
+    for t0, t1 in blocks:
+        blk = torch.from_numpy(U[t0 * lcu:t1 * lcu].view(np.float64).reshape(-1).copy()).cuda()
+        dims = (C.c_size_t * 4)(d[0], d[1], d[2], t1 - t0)
+        gfirst = torch.empty(9 * lcu * 2, dtype=torch.float64, device="cuda")
+        glast = torch.empty_like(gfirst)
+        r = GfixResult()
+        th = np.zeros(t1 - t0)
+        it = np.zeros(t1 - t0, dtype=np.uintp)
+        check(lib.gfix_coulomb_slices(blk.data_ptr(), dims, C.byref(p), C.byref(r),
+                                      th.ctypes.data_as(C.POINTER(C.c_double)),
+                                      it.ctypes.data_as(C.POINTER(C.c_size_t)),
+                                      gfirst.data_ptr(), glast.data_ptr()))
+        dev.append((blk, dims))
+        gf.append(gfirst)
+        gl.append(glast)
+        its.append(it.astype(np.int64))
+    for k, (blk, dims) in enumerate(dev):
+        check(lib.gfix_coulomb_slices_finish(blk.data_ptr(), dims, gl[k].data_ptr(),
+                                             gf[(k + 1) % len(dev)].data_ptr()))
+    got = np.concatenate([b.cpu().numpy() for b, _ in dev]).view(np.complex128)
+    assert np.array_equal(got.reshape(whole.links.shape), whole.links)
+    assert np.array_equal(np.concatenate(its), whole.slice_iters)
