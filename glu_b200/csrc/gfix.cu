@@ -594,6 +594,11 @@ class Engine {
   Params run_p;
   bool run_cg = true;
   size_t run_total = 0;
+  // warm start of a CG solve (mixed precision): set by the hand-over, which
+  // has put in_old into fb[1] and the last direction into sb[0]; run_start
+  // then continues the conjugate directions instead of an SD start
+  bool warm = false;
+  double warm_inold = 0.0;
 
   void run_head() {
     k_begin_run<<<1, 1, 0, s>>>(d_st);
@@ -628,6 +633,17 @@ class Engine {
       }
       ensure_graph(&gx_sd, false, p.sd_fixed != 0);
     }
+    if (warm && run_cg) {
+      // (reset left parity = sparity = 0: in_old = fb[1], sn_old = sb[0])
+      k_begin_run<<<1, 1, 0, s>>>(d_st);
+      LAUNCHED(1);
+      CK(cudaMemcpyAsync(&d_st->inold, &warm_inold, sizeof(double),
+                         cudaMemcpyHostToDevice, s));
+      CK(cudaStreamSynchronize(s));
+      warm = false;
+      return 0;
+    }
+    warm = false;
     run_head();
     return 0;
   }
@@ -1140,6 +1156,50 @@ static Params to_params(const gfix_params *p) {
 }
 
 // Landau solve of the links staged (AoS FP64) in e64->d_aos
+// Mixed precision hand-over from the FP32 phase (engine f, finished, it32
+// iterations, theta th32) to the FP64 engine e: U64 <- G U64 G^dag with the
+// accumulated G reunitarised in FP64; for FACG the FP32 run's last direction
+// and accelerated derivative become the FP64 run's sn_old / in_old, so the
+// conjugate directions continue across the switch.  A phase that ended
+// non-finite hands over nothing (FP64 from the staged input links; it32 = 0,
+// *restart = 1).
+static int mixed_handover(Engine<double> *e, Engine<float> *f, const Params &p64,
+                          size_t *it32, double th32, int *restart) {
+  *restart = 0;
+  if (!(*it32 == kSentinel || *it32 > 0)) return 0;
+  cx<double> *G64 = e->c.fb[0];  // 9 V complex fit in the field pool
+  k_convert<float, double><<<1184, 256, 0, f->s>>>(f->d_G, G64,
+                                                   (size_t)e->V * 9);
+  LAUNCHED(1);
+  CK(cudaStreamSynchronize(f->s));
+  k_apply_gauge<<<e->nb_site, kSiteThreads, 0, e->s>>>(e->c, G64);
+  LAUNCHED(1);
+  double tt = 0.0;
+  if (e->reset(p64) || e->theta_test(&tt)) return -1;
+  if (!std::isfinite(th32) || !std::isfinite(tt)) {
+    if (e->from_aos(e->d_aos)) return -1;
+    *it32 = 0;
+    *restart = 1;
+    return 0;
+  }
+  if (p64.algo == GFIX_CG && *it32 != kSentinel) {
+    // f's state after its last iteration: in_old = fb[parity ^ 1] (the END
+    // step flipped it), sn_old = sb[sparity]
+    if (f->read_state()) return -1;
+    const cx<float> *in_old = f->c.fb[f->h_st->parity ^ 1];
+    const cx<float> *sn_old = f->c.sb[f->h_st->sparity];
+    k_convert<float, double><<<1184, 256, 0, e->s>>>(in_old, e->c.fb[1],
+                                                     (size_t)e->V * 4);
+    k_convert<float, double><<<1184, 256, 0, e->s>>>(sn_old, e->c.sb[0],
+                                                     (size_t)e->V * 4);
+    LAUNCHED(2);
+    CK(cudaStreamSynchronize(e->s));
+    e->warm = true;
+    e->warm_inold = f->h_st->inold;
+  }
+  return 0;
+}
+
 static int landau_staged(Engine<double> *e64, const gfix_params *gp,
                          gfix_result *r) {
   Params p = to_params(gp);
@@ -1168,22 +1228,10 @@ static int landau_staged(Engine<double> *e64, const gfix_params *gp,
     if (e32->solve(p32, &it32, &th32)) return -1;
     size_t tl32 = 0;
     if (e32->fetch_traj(p32, &tl32)) return -1;
-    if (it32 == kSentinel || it32 > 0) {
-      // hand over: U64 <- G U64 G^dag with G reunitarised in FP64
-      cx<double> *G64 = e64->c.fb[0];  // 9 V complex fit in the field pool
-      k_convert<float, double><<<1184, 256, 0, e32->s>>>(e32->d_G, G64,
-                                                          (size_t)e64->V * 9);
-      LAUNCHED(1);
-      CK(cudaStreamSynchronize(e32->s));
-      k_apply_gauge<<<e64->nb_site, kSiteThreads, 0, e64->s>>>(e64->c, G64);
-      LAUNCHED(1);
-      // a phase that ended non-finite hands over nothing: restart in FP64
-      // from the staged input links
-      double tt = 0.0;
-      if (e64->reset(p) || e64->theta_test(&tt)) return -1;
-      if (!std::isfinite(th32) || !std::isfinite(tt)) {
-        if (e64->from_aos(e64->d_aos)) return -1;
-        it32 = 0;
+    {
+      int restart = 0;
+      if (mixed_handover(e64, e32, p, &it32, th32, &restart)) return -1;
+      if (restart) {
         tl32 = 0;
         res.restarts++;
       }
@@ -1389,23 +1437,10 @@ static int batch_run(Batch *b) {
     p32.acc = std::max(b->p.switch_theta, b->p.accuracy);
     if (batch_solve(e32, p32, it32, th32, b->bs)) return -1;
     for (size_t i = 0; i < n; i++) {
-      Engine<double> *e = e64[i];
-      if (it32[i] == kSentinel || it32[i] > 0) {
-        cx<double> *G64 = e->c.fb[0];
-        k_convert<float, double><<<1184, 256, 0, e32[i]->s>>>(
-            e32[i]->d_G, G64, (size_t)e->V * 9);
-        LAUNCHED(1);
-        CK(cudaStreamSynchronize(e32[i]->s));
-        k_apply_gauge<<<e->nb_site, kSiteThreads, 0, e->s>>>(e->c, G64);
-        LAUNCHED(1);
-        double tt = 0.0;
-        if (e->reset(p64) || e->theta_test(&tt)) return -1;
-        if (!std::isfinite(th32[i]) || !std::isfinite(tt)) {
-          if (e->from_aos(e->d_aos)) return -1;
-          it32[i] = 0;
-          b->inst[i]->res.restarts++;
-        }
-      }
+      int restart = 0;
+      if (mixed_handover(e64[i], e32[i], p64, &it32[i], th32[i], &restart))
+        return -1;
+      b->inst[i]->res.restarts += restart;
     }
   }
   if (batch_solve(e64, p64, it64, th64, b->bs)) return -1;
