@@ -38,7 +38,7 @@ EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
            "gfix_theta_functional_noalloc", "gfix_batch_create",
            "gfix_batch_add", "gfix_batch_add_device", "gfix_batch_run",
            "gfix_batch_result", "gfix_batch_destroy", "gfix_coulomb_slices",
-           "gfix_coulomb_slices_finish",
+           "gfix_coulomb_slices_finish", "gfix_fft_tuning", "gfix_fft_plan",
            "gfix_noalloc_error",
            "gfix_last_error", "gfix_release", "gfix_kernel_launches")
 
@@ -82,6 +82,11 @@ def load(path: Path | str | None = None):
     lib.gfix_coulomb_slices_finish.restype = C.c_int
     lib.gfix_coulomb_slices_finish.argtypes = [C.c_void_p, _szp, C.c_void_p,
                                                C.c_void_p]
+    lib.gfix_fft_tuning.restype = None
+    lib.gfix_fft_tuning.argtypes = [C.c_int]
+    lib.gfix_fft_plan.restype = C.c_int
+    lib.gfix_fft_plan.argtypes = [_szp, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                  C.POINTER(C.c_float)]
     lib.gfix_batch_create.restype = C.c_void_p
     lib.gfix_batch_create.argtypes = [C.POINTER(GfixParams)]
     for fn in ("gfix_batch_add", "gfix_batch_add_device"):

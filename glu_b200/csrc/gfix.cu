@@ -54,15 +54,21 @@ static int fail(const char *fmt, ...) {
 constexpr size_t kSentinel = 123456789;
 
 // radices 8, 4, 2, 3, 5, 7 and the Stockham stage table of length n
-static int factorize(int n, FftAxis &ax) {
+// radix orders of the generic passes' stage tables (the autotuner tries
+// them; 0, largest radices first, is the default)
+constexpr int kRadixOrders = 3;
+static const int kRadixPref[kRadixOrders][6] = {
+    {8, 4, 2, 3, 5, 7}, {4, 8, 2, 3, 5, 7}, {2, 4, 8, 3, 5, 7}};
+
+static int factorize(int n, FftAxis &ax, int order = 0) {
   ax.n = n;
   ax.nstages = 0;
   int m = n;
   int rad[kMaxStages];
   int ns = 0;
-  const int pref[6] = {8, 4, 2, 3, 5, 7};
-  for (int r : pref)
-    while (m % r == 0 && m > 1) {
+  const int *pref = kRadixPref[order];
+  for (int i = 0; i < 6; i++)
+    for (const int r = pref[i]; m % r == 0 && m > 1;) {
       if (ns == kMaxStages) return -1;
       rad[ns++] = r;
       m /= r;
@@ -82,6 +88,17 @@ static int factorize(int n, FftAxis &ax) {
   }
   ax.nstages = ns;
   return 0;
+}
+
+// FFT plans: 0 = the default plan per shape (bit-reproducible runs), 1 =
+// autotuned per shape at first use (gfix_fft_tuning, GLU_GFIX_FFT_TUNE=1)
+static int g_fft_tune = -1;
+static int fft_tuning() {
+  if (g_fft_tune < 0) {
+    const char *e = getenv("GLU_GFIX_FFT_TUNE");
+    g_fft_tune = (e && atoi(e) != 0) ? 1 : 0;
+  }
+  return g_fft_tune;
 }
 
 // compile-time specialised FFT passes for the common extents; nullptr
@@ -108,10 +125,11 @@ static ZtFn<R> ct_zt(int lz, int lt, int b) {
   GFIX_ZT(4, 4, 2) GFIX_ZT(4, 8, 2) GFIX_ZT(8, 8, 2) GFIX_ZT(8, 16, 2)
   GFIX_ZT(16, 16, 2) GFIX_ZT(16, 32, 2) GFIX_ZT(24, 48, 2)
   GFIX_ZT(32, 32, 2) GFIX_ZT(32, 64, 2) GFIX_ZT(48, 96, 2)
+  GFIX_ZT(32, 64, 1) GFIX_ZT(32, 64, 4) GFIX_ZT(48, 96, 1) GFIX_ZT(16, 32, 4)
   GFIX_ZT(4, 1, 8) GFIX_ZT(8, 1, 8) GFIX_ZT(16, 1, 8) GFIX_ZT(24, 1, 8)
   GFIX_ZT(32, 1, 8) GFIX_ZT(48, 1, 8) GFIX_ZT(64, 1, 8)
   GFIX_ZT(8, 1, 16) GFIX_ZT(16, 1, 16) GFIX_ZT(24, 1, 16) GFIX_ZT(32, 1, 16)
-  GFIX_ZT(48, 1, 16) GFIX_ZT(64, 1, 16)
+  GFIX_ZT(48, 1, 16) GFIX_ZT(64, 1, 16) GFIX_ZT(32, 1, 32) GFIX_ZT(64, 1, 32)
 #undef GFIX_ZT
   return nullptr;
 }
@@ -240,77 +258,49 @@ class Engine {
     c.cs_ld = ld;
     // tiles
     c.xy_pitch = c.L[0] + 1;
-    // x columns per zt tile: 2 (32-byte rows in FP64) for Landau's big
-    // (z, t) tiles; Coulomb tiles hold one slice's z pencils only
-    const int want_b = coul ? 16 : 2;
+    // x columns per zt tile: Landau's (z, t) tiles take 4 where a
+    // compile-time pass for them exists (the autotuner's pick on 16^3x32
+    // and 32^3x64), else 2 (32-byte rows in FP64); Coulomb tiles hold one
+    // slice's z pencils only and take 16
+    odd = false;
+    for (int a = 0; a < 4; a++)
+      for (int k = 0; k < c.ax[a].nstages; k++)
+        odd |= (c.ax[a].st[k].r == 5 || c.ax[a].st[k].r == 7);
     const int nt = coul ? 1 : c.L[3];
+    int want_b = coul ? 16 : 2;
+    if (!coul && !odd && c.L[0] % 4 == 0 && ct_zt<R>(c.L[2], nt, 4) != nullptr &&
+        zt_smem(4) <= 200u * 1024u)
+      want_b = 4;
     c.zt_b = 1;
     for (int b = want_b; b >= 1; b--)
       if (c.L[0] % b == 0) {
         c.zt_b = b;
         break;
       }
-    odd = false;
-    for (int a = 0; a < 4; a++)
-      for (int k = 0; k < c.ax[a].nstages; k++)
-        odd |= (c.ax[a].st[k].r == 5 || c.ax[a].st[k].r == 7);
-    auto zt_smem = [&](int b) {
-      return coul ? ((size_t)b * c.L[2] + c.L[2]) * sizeof(cx<R>)
-                  : ((size_t)(b * c.L[2] + std::max(1, zt_pad(b))) * c.L[3] +
-                     c.L[2] + c.L[3]) * sizeof(cx<R>);
-    };
     // a compile-time pass takes the tile as chosen while its shared memory
     // fits (tiles up to 16384 elements); the generic passes hold one
     // element per thread and stage for 8 (16) elements: tiles up to 8192
     const bool ct_tile = !odd && ct_zt<R>(c.L[2], nt, c.zt_b) != nullptr &&
                          zt_smem(c.zt_b) <= 200u * 1024u;
-    constexpr int pt_small = 8;
-    auto threads_for = [](size_t n, int pt) {
-      size_t t = (n + pt - 1) / pt;
-      t = std::max<size_t>(128, (t + 31) / 32 * 32);
-      return t;
-    };
     if (!ct_tile) {
-      while (c.zt_b > 1 && (size_t)c.zt_b * c.L[2] * nt > 512u * pt_small)
-        c.zt_b /= 2;
+      while (c.zt_b > 1 && (size_t)c.zt_b * c.L[2] * nt > 4096u) c.zt_b /= 2;
       while (c.zt_b > 1 && c.L[0] % c.zt_b) c.zt_b /= 2;
     }
-    const size_t n_xy = (size_t)c.L[0] * c.L[1];
-    const size_t n_zt = (size_t)c.zt_b * c.L[2] * nt;
-    if (n_xy > 8192 || (n_zt > 8192 && !ct_tile))
-      return fail("FFT tile of %zu / %zu elements exceeds 8192", n_xy, n_zt);
-    pt_xy = (n_xy <= 512u * pt_small && !odd) ? pt_small : 16;
-    pt_zt = (n_zt <= 512u * pt_small && !odd) ? pt_small : 16;
-    bd_xy = (int)threads_for(n_xy, pt_xy);
-    bd_zt = (int)threads_for(n_zt, pt_zt);
+    if ((size_t)c.L[0] * c.L[1] > 8192)
+      return fail("FFT xy tile of %d elements exceeds 8192", c.L[0] * c.L[1]);
     // tile (padded) plus the twiddle tables of its two axes
     sm_xy = ((size_t)c.xy_pitch * c.L[1] + c.L[0] + c.L[1]) * sizeof(cx<R>);
-    // (the t-stride padding covers the generic pass's 1 and zt_pad)
-    sm_zt = zt_smem(c.zt_b);
     // the dynamic shared-memory limit is an attribute of the function, not
     // of a launch: raise it once to the largest tile any engine can use
     if (set_smem_limits()) return -1;
-    // compile-time specialised passes where the extents have one
-    xy_ct = odd ? nullptr : ct_xy<R>(c.L[0], c.L[1]);
-    zt_ct = odd ? nullptr : ct_zt<R>(c.L[2], nt, c.zt_b);
-    // the FFT passes live in shared memory: ask for the largest carveout so
-    // that several tiles are resident per SM
-    if (xy_ct) {
-      bd_xy = ct_threads(c.L[0] * c.L[1]);
-      CK(cudaFuncSetAttribute(xy_ct, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sm_xy));
-      CK(cudaFuncSetAttribute(xy_ct, cudaFuncAttributePreferredSharedMemoryCarveout,
-                              (int)cudaSharedmemCarveoutMaxShared));
-    }
-    if (zt_ct) {
-      bd_zt = ct_threads(c.zt_b * c.L[2] * nt);
-      CK(cudaFuncSetAttribute(zt_ct, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)sm_zt));
-      CK(cudaFuncSetAttribute(zt_ct, cudaFuncAttributePreferredSharedMemoryCarveout,
-                              (int)cudaSharedmemCarveoutMaxShared));
-    }
+    // default plan (FFTW's ESTIMATE, so to speak): compile-time passes where
+    // the extents have one, largest radices first
+    if (apply_xy(true, 0) && apply_xy(false, 0))
+      return fail("no xy FFT pass for %d x %d", c.L[0], c.L[1]);
+    if (apply_zt(c.zt_b, ct_tile, 0) && apply_zt(c.zt_b, false, 0))
+      return fail("FFT tile of %zu elements exceeds 8192",
+                  (size_t)c.zt_b * c.L[2] * nt);
     g_xy = dim3(V / (c.L[0] * c.L[1]), 4);
-    g_zt = dim3((c.L[0] / c.zt_b) * c.L[1] * (coul ? c.L[3] : 1), 4);
     nb_site = (V + kSiteThreads - 1) / kSiteThreads;
     const size_t nparts =
         std::max<size_t>((size_t)nb_site, (size_t)g_xy.x * g_xy.y) + 1024;
@@ -330,6 +320,145 @@ class Engine {
     if (with_G) CK(cudaMalloc(&d_G, (size_t)V * 9 * sizeof(cx<R>)));
     c.G = d_G;
     if (with_staging) CK(cudaMalloc(&d_aos, (size_t)V * 36 * sizeof(double2)));
+    if (fft_tuning() && tune_fft()) return -1;
+    return 0;
+  }
+
+  // --- FFT plans ------------------------------------------------------
+  size_t zt_smem(int b) const {
+    return coul ? ((size_t)b * c.L[2] + c.L[2]) * sizeof(cx<R>)
+                : ((size_t)(b * c.L[2] + std::max(1, zt_pad(b))) * c.L[3] +
+                   c.L[2] + c.L[3]) * sizeof(cx<R>);
+  }
+  static size_t threads_for(size_t n, int pt) {
+    size_t t = (n + pt - 1) / pt;
+    return std::max<size_t>(128, (t + 31) / 32 * 32);
+  }
+  // the xy pass: compile-time (use_ct) or generic with radix order `order`;
+  // -1 where that pass does not exist for these extents
+  int apply_xy(bool use_ct, int order) {
+    for (int a = 0; a < 2; a++)
+      if (factorize(c.L[a], c.ax[a], order)) return -1;
+    const size_t n = (size_t)c.L[0] * c.L[1];
+    if (use_ct) {
+      XyFn<R> fn = odd ? nullptr : ct_xy<R>(c.L[0], c.L[1]);
+      if (!fn) return -1;
+      xy_ct = fn;
+      bd_xy = ct_threads((int)n);
+      CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sm_xy));
+      CK(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                              (int)cudaSharedmemCarveoutMaxShared));
+    } else {
+      xy_ct = nullptr;
+      pt_xy = (n <= 4096u && !odd) ? 8 : 16;
+      bd_xy = (int)threads_for(n, pt_xy);
+    }
+    xy_plan = use_ct ? -1 : order;
+    return 0;
+  }
+  // the z(,t) pass with tiles of b x columns
+  int apply_zt(int b, bool use_ct, int order) {
+    const int nt = coul ? 1 : c.L[3];
+    if (b < 1 || c.L[0] % b) return -1;
+    for (int a = 2; a < 4; a++)
+      if (factorize(c.L[a], c.ax[a], order)) return -1;
+    const size_t n = (size_t)b * c.L[2] * nt;
+    if (use_ct) {
+      ZtFn<R> fn = odd ? nullptr : ct_zt<R>(c.L[2], nt, b);
+      if (!fn || zt_smem(b) > 200u * 1024u) return -1;
+      zt_ct = fn;
+      bd_zt = ct_threads((int)n);
+      CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)zt_smem(b)));
+      CK(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                              (int)cudaSharedmemCarveoutMaxShared));
+    } else {
+      if (n > 8192) return -1;
+      zt_ct = nullptr;
+      pt_zt = (n <= 4096u && !odd) ? 8 : 16;
+      bd_zt = (int)threads_for(n, pt_zt);
+    }
+    c.zt_b = b;
+    sm_zt = zt_smem(b);
+    g_zt = dim3((c.L[0] / b) * c.L[1] * (coul ? c.L[3] : 1), 4);
+    zt_plan = use_ct ? -1 : order;
+    return 0;
+  }
+  int xy_plan = -1, zt_plan = -1;  // -1 compile-time pass, else radix order
+
+  // FFTW's MEASURE, so to speak: time every available xy and zt pass once
+  // for these extents (compile-time or generic, each radix order; every zt
+  // tile width dividing Lx) and keep the fastest.  One plan per shape and
+  // precision and process; plans change rounding, not results beyond it.
+  struct TunedPlan {
+    bool xy_ct;
+    int xy_order, zt_b;
+    bool zt_ct;
+    int zt_order;
+    float xy_ms, zt_ms;
+  };
+  static std::map<std::tuple<int, int, int, int, bool>, TunedPlan> &tuned() {
+    static std::map<std::tuple<int, int, int, int, bool>, TunedPlan> m;
+    return m;
+  }
+  int time_pass(bool xy, float *ms) {
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    for (int k = 0; k < 2; k++) xy ? fft_xy(0, 0) : fft_zt();
+    CK(cudaEventRecord(a, s));
+    for (int k = 0; k < 5; k++) xy ? fft_xy(0, 0) : fft_zt();
+    CK(cudaEventRecord(b, s));
+    CK(cudaEventSynchronize(b));
+    CK(cudaEventElapsedTime(ms, a, b));
+    *ms /= 5.f;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  }
+  int tune_fft() {
+    const auto key = std::make_tuple(c.L[0], c.L[1], c.L[2], c.L[3], coul);
+    auto it = tuned().find(key);
+    TunedPlan P;
+    if (it == tuned().end()) {
+      Params p;
+      if (reset(p)) return -1;
+      CK(cudaMemsetAsync(d_F, 0, (size_t)V * 16 * sizeof(cx<R>), s));
+      float best = 1e30f, t = 0.f;
+      P = TunedPlan{xy_ct != nullptr, xy_plan < 0 ? 0 : xy_plan, c.zt_b,
+                    zt_ct != nullptr, zt_plan < 0 ? 0 : zt_plan, 0.f, 0.f};
+      for (int ct = 1; ct >= 0; ct--)
+        for (int o = 0; o < (ct ? 1 : kRadixOrders); o++) {
+          if (apply_xy(ct != 0, o)) continue;
+          if (time_pass(true, &t)) return fail("FFT autotuning failed");
+          if (t < best) {
+            best = t;
+            P.xy_ct = ct != 0;
+            P.xy_order = o;
+            P.xy_ms = t;
+          }
+        }
+      best = 1e30f;
+      for (int b = 1; b <= 32; b *= 2)
+        for (int ct = 1; ct >= 0; ct--)
+          for (int o = 0; o < (ct ? 1 : kRadixOrders); o++) {
+            if (apply_zt(b, ct != 0, o)) continue;
+            if (time_pass(false, &t)) return fail("FFT autotuning failed");
+            if (t < best) {
+              best = t;
+              P.zt_b = b;
+              P.zt_ct = ct != 0;
+              P.zt_order = o;
+              P.zt_ms = t;
+            }
+          }
+      tuned()[key] = P;
+    } else {
+      P = it->second;
+    }
+    if (apply_xy(P.xy_ct, P.xy_order) || apply_zt(P.zt_b, P.zt_ct, P.zt_order))
+      return fail("tuned FFT plan not applicable");
     return 0;
   }
 
@@ -1484,6 +1613,48 @@ const char *gfix_last_error(void) { return g_err.c_str(); }
 
 unsigned long long gfix_kernel_launches(void) { return g_launches.load(); }
 
+void gfix_fft_tuning(int on) {
+  g_fft_tune = on ? 1 : 0;
+  // workspaces built under the other setting are rebuilt at next use
+  g_e64.clear();
+  g_e32.clear();
+  g_ec.clear();
+  g_ec32.clear();
+}
+
+int gfix_fft_plan(const size_t dims[4], int coulomb, int precision, int *plan,
+                  float *ms) {
+  if (!dims || !plan) return fail("null argument");
+  for (int i = 0; i < 4; i++)
+    if (dims[i] < 2) return fail("extent %zu of dimension %d below 2", dims[i], i);
+  auto get = [&](auto *e) {
+    plan[0] = e->xy_plan;
+    plan[1] = e->c.zt_b;
+    plan[2] = e->zt_plan;
+    if (ms) {
+      ms[0] = ms[1] = 0.f;
+      const auto key = std::make_tuple(e->c.L[0], e->c.L[1], e->c.L[2],
+                                       e->c.L[3], e->coul);
+      auto it = e->tuned().find(key);
+      if (it != e->tuned().end()) {
+        ms[0] = it->second.xy_ms;
+        ms[1] = it->second.zt_ms;
+      }
+    }
+    return 0;
+  };
+  if (precision == GFIX_MIXED) {
+    if (coulomb) {
+      Engine<float> *f = engine_coul32(dims);
+      return f ? get(f) : -1;
+    }
+    Engine<float> *f = engine32(dims);
+    return f ? get(f) : -1;
+  }
+  Engine<double> *e = coulomb ? engine_coul(dims) : engine64(dims);
+  return e ? get(e) : -1;
+}
+
 void gfix_release(void) {
   g_e64.clear();
   g_e32.clear();
@@ -1577,7 +1748,28 @@ int gfix_reunit(double *links, const size_t dims[4]) {
 
 int gfix_fourier_accelerate(double *fields, const size_t dims[4], int ndim) {
   if (!fields || !dims) return fail("null argument");
-  if (ndim != 4) return fail("only the 4D (Landau) transform is built here");
+  if (ndim == 3) {
+    // one slice: the Coulomb engine of a 2-slice lattice, slice 0 carrying
+    // the fields, slice 1 zero (the slices are transformed independently)
+    const size_t d3[4] = {dims[0], dims[1], dims[2], 2};
+    Engine<double> *e = engine_coul(d3);
+    if (!e) return -1;
+    Params p;
+    if (e->reset(p)) return -1;
+    if (e->d_cmask) CK(cudaMemsetAsync(e->d_cmask, 0, 2 * sizeof(int), e->s));
+    const size_t lcu = (size_t)e->Lcu, V = (size_t)e->V;
+    CK(cudaMemsetAsync(e->c.fb[0], 0, V * 4 * sizeof(cx<double>), e->s));
+    for (int k = 0; k < 4; k++)
+      CK(cudaMemcpyAsync(e->c.fb[0] + k * V, fields + k * lcu * 2,
+                         lcu * sizeof(cx<double>), cudaMemcpyHostToDevice, e->s));
+    e->fft(false);
+    for (int k = 0; k < 4; k++)
+      CK(cudaMemcpyAsync(fields + k * lcu * 2, e->c.fb[0] + k * V,
+                         lcu * sizeof(cx<double>), cudaMemcpyDeviceToHost, e->s));
+    CK(cudaStreamSynchronize(e->s));
+    return 0;
+  }
+  if (ndim != 4) return fail("ndim %d: the transform is 3 (Coulomb) or 4 (Landau)", ndim);
   Engine<double> *e = engine64(dims);
   if (!e) return -1;
   const size_t bytes = (size_t)e->V * 4 * sizeof(double2);

@@ -246,8 +246,21 @@ size_t Coulomb(struct site *lat, const double accuracy, const size_t iter) {
 }
 
 void FOURIER_ACCELERATE2(struct fftw_stuff *FFTW) {
-  (void)FFTW;
-  fprintf(stderr, "[GF] FOURIER_ACCELERATE2 on the GPU needs gfix_coulomb\n");
+  // one time slice: 4 fields of Lcu complex numbers (CFACG.c:69-88)
+  glu_fftw_stuff *F = reinterpret_cast<glu_fftw_stuff *>(FFTW);
+  size_t d[4];
+  dims_of(d);
+  const size_t lcu = d[0] * d[1] * d[2];
+  std::vector<double> f(lcu * 8);
+  for (int k = 0; k < 4; k++)
+    memcpy(f.data() + (size_t)k * lcu * 2, F->in[k], lcu * 2 * sizeof(double));
+  if (gfix_fourier_accelerate(f.data(), d, 3) != 0) {
+    fprintf(stderr, "[GF] GPU Fourier acceleration failed: %s\n",
+            gfix_last_error());
+    return;
+  }
+  for (int k = 0; k < 4; k++)
+    memcpy(F->in[k], f.data() + (size_t)k * lcu * 2, lcu * 2 * sizeof(double));
 }
 
 }  // extern "C"

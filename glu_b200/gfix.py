@@ -234,13 +234,33 @@ def latt_reunitU(links, dims):
     return U
 
 
-def fourier_accelerate(fields, dims):
-    """The GPU FOURIER_ACCELERATE3 on 4 packed fields of shape (4, V)."""
+def fourier_accelerate(fields, dims, ndim=4):
+    """The GPU FOURIER_ACCELERATE3 (ndim 4, fields of shape (4, V)) or
+    FOURIER_ACCELERATE2 (ndim 3, one time slice, shape (4, Lx Ly Lz))."""
     lib = _lib.load()
     cd, d = _dims(dims)
     f = np.ascontiguousarray(fields, dtype=np.complex128).copy()
-    check(lib.gfix_fourier_accelerate(f.ctypes.data, cd, 4))
+    check(lib.gfix_fourier_accelerate(f.ctypes.data, cd, ndim))
     return f
+
+
+def fft_tuning(on: bool):
+    """Autotuned FFT plans per lattice shape (True) or the fixed default
+    plans (False, bit-reproducible); see gfix_fft_tuning."""
+    _lib.load().gfix_fft_tuning(1 if on else 0)
+
+
+def fft_plan(dims, coulomb=False, precision="FP64"):
+    """((xy pass, zt tile width, zt pass), (xy ms, zt ms)) of a shape's
+    workspace: pass -1 = compile-time, else the generic pass's radix order;
+    times 0 unless tuned."""
+    lib = _lib.load()
+    cd, _ = _dims(dims)
+    plan = (C.c_int * 3)()
+    ms = (C.c_float * 2)()
+    check(lib.gfix_fft_plan(cd, int(bool(coulomb)), {"FP64": 0, "MIXED": 1}[precision],
+                            plan, ms))
+    return tuple(plan), tuple(ms)
 
 
 def kernel_launches() -> int:

@@ -227,6 +227,25 @@ int gfix_theta_functional_noalloc(const double *d_links, const size_t dims[4],
                                   double *d_out);
 const char *gfix_noalloc_error(void);
 
+/* FFT plans.  0 (default): a fixed plan per lattice shape -- compile-time
+ * passes where the extents have one, largest radices first -- so repeated
+ * runs are bit-identical.  1: at the first use of a shape every available
+ * xy and z(,t) pass is timed once (compile-time or generic, each radix order
+ * of the generic pass, every zt tile width dividing Lx) and the fastest is
+ * kept for the process; plans differ in rounding only.  The environment
+ * variable GLU_GFIX_FFT_TUNE=1 sets 1 at load.  Switching drops the cached
+ * workspaces. */
+void gfix_fft_tuning(int on);
+
+/* The plan of a shape (building its workspace): plan[0] = xy pass (-1
+ * compile-time, else the generic pass's radix order), plan[1] = zt tile
+ * width, plan[2] = zt pass (-1 compile-time, else radix order); ms[0..1]
+ * (may be NULL) the measured times of the tuned xy / zt pass (0 untuned).
+ * coulomb: 1 for the Coulomb workspace (3D FFT per slice);
+ * precision: GFIX_MIXED reports the FP32 workspace. */
+int gfix_fft_plan(const size_t dims[4], int coulomb, int precision, int *plan,
+                  float *ms);
+
 /* message of the last failed call (thread-local, never NULL) */
 const char *gfix_last_error(void);
 

@@ -49,6 +49,17 @@ def test_fourier_accelerate_matches_oracle(oracle, dims):
     assert np.abs(got - ref).max() < 1e-13 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("dims", [(4, 4, 4, 8), (16, 8, 32, 2), (6, 10, 5, 3)])
+def test_fourier_accelerate3_matches_oracle(oracle, dims):
+    """FOURIER_ACCELERATE2 (one time slice, MAX_COULOMB / p^2 in 3D)."""
+    rng = np.random.default_rng(8)
+    n = dims[0] * dims[1] * dims[2]
+    f = rng.normal(size=(4, n)) + 1j * rng.normal(size=(4, n))
+    got = gfix.fourier_accelerate(f, dims, 3)
+    ref = oracle.fourier_accelerate(f, dims, 3)
+    assert np.abs(got - ref).max() < 1e-13 * np.abs(ref).max()
+
+
 def test_reunit_matches_oracle(oracle, lat400):
     g = lat400
     rng = np.random.default_rng(1)
