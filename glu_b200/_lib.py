@@ -39,6 +39,7 @@ EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
            "gfix_batch_add", "gfix_batch_add_device", "gfix_batch_run",
            "gfix_batch_result", "gfix_batch_destroy", "gfix_coulomb_slices",
            "gfix_coulomb_slices_finish", "gfix_fft_tuning", "gfix_fft_plan",
+           "gfix_link_diagnostics",
            "gfix_noalloc_error",
            "gfix_last_error", "gfix_release", "gfix_kernel_launches")
 
@@ -71,6 +72,8 @@ def load(path: Path | str | None = None):
                                      C.POINTER(GfixResult), _dp, _szp]
     lib.gfix_observables.restype = C.c_int
     lib.gfix_observables.argtypes = [C.c_void_p, _szp, _dp]
+    lib.gfix_link_diagnostics.restype = C.c_int
+    lib.gfix_link_diagnostics.argtypes = [C.c_void_p, _szp, _dp]
     lib.gfix_reunit.restype = C.c_int
     lib.gfix_reunit.argtypes = [C.c_void_p, _szp]
     lib.gfix_fourier_accelerate.restype = C.c_int

@@ -58,6 +58,67 @@ __global__ void k_reunit_links(cx<R> *U, size_t nlinks, size_t V) {
   for (int e = 0; e < 9; e++) p[(size_t)e * V] = u[e];
 }
 
+// Link diagnostics of GLU's output (src/Field/plaqs_links.c:399-446,
+// src/Gfix/gftests.c:35-129), per block of sites of one time slice t
+// (grid (blocks per slice, Lt)): Re tr of the spatial and of the temporal
+// links, the largest Re tr of any link, and the sum over the slice of the
+// Hermitian projection of the temporal links (entries 00, 01, 02, 11, 12 of
+// Hermitian_proj, exactQ.c:358-371: 8 reals).  Partials: 11 per block.
+constexpr int kDiagThreads = 128;
+constexpr int kDiagVals = 11;
+
+template <typename R>
+__global__ void __launch_bounds__(kDiagThreads) k_link_diag(Ctx<R> c, int lcu,
+                                                             int nbs) {
+  const int t = blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[kDiagVals];
+#pragma unroll
+  for (int k = 0; k < kDiagVals; k++) v[k] = 0.0;
+  v[2] = -1e300;
+  if (i < lcu) {
+    const int s = t * lcu + i;
+#pragma unroll 1
+    for (int mu = 0; mu < 4; mu++) {
+      cx<R> u[9];
+      load_link(c.U, c.V, mu, s, u);
+      const double tr = (double)u[0].x + (double)u[4].x + (double)u[8].x;
+      if (mu < 3)
+        v[0] += tr;
+      else
+        v[1] += tr;
+      v[2] = fmax(v[2], tr);
+      if (mu == 3) {
+        const double i0 = u[0].y, i4 = u[4].y, i8 = u[8].y;
+        v[3] += (2 * i0 - i4 - i8) / 3.;
+        // -i (a - conj(b)) / 2 = ((a.y + b.y) / 2, -(a.x - b.x) / 2)
+        v[4] += 0.5 * ((double)u[1].y + (double)u[3].y);
+        v[5] += -0.5 * ((double)u[1].x - (double)u[3].x);
+        v[6] += 0.5 * ((double)u[2].y + (double)u[6].y);
+        v[7] += -0.5 * ((double)u[2].x - (double)u[6].x);
+        v[8] += (2 * i4 - i0 - i8) / 3.;
+        v[9] += 0.5 * ((double)u[5].y + (double)u[7].y);
+        v[10] += -0.5 * ((double)u[5].x - (double)u[7].x);
+      }
+    }
+  }
+  // sums (the maximum through its own warp and block reduction)
+  double m = v[2];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+  __shared__ double smax[kDiagThreads / 32];
+  if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = m;
+  v[2] = 0.0;
+  double *out = c.part + (size_t)kDiagVals * ((size_t)t * nbs + blockIdx.x);
+  block_sum_store<kDiagVals>(v, out);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mm = smax[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) mm = fmax(mm, smax[w]);
+    out[2] = mm;
+  }
+}
+
 template <typename R>
 __global__ void k_identity(cx<R> *G, int V) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -1726,6 +1727,59 @@ int gfix_observables(const double *links, const size_t dims[4], double *out) {
   double sum = 0.0;
   for (double v : part) sum += v;
   out[2] = 2.0 * sum / (3.0 * 4 * 3 * (double)e->V);
+  return 0;
+}
+
+int gfix_link_diagnostics(const double *links, const size_t dims[4],
+                          double *out) {
+  if (!links || !dims || !out) return fail("null argument");
+  Engine<double> *e = engine64(dims);
+  if (!e) return -1;
+  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
+  if (e->from_aos(e->d_aos)) return -1;
+  const int T = e->c.L[3], lcu = e->V / T;
+  const int nbs = (lcu + kDiagThreads - 1) / kDiagThreads;
+  std::vector<double> part((size_t)kDiagVals * nbs * T);
+  double *d_p = nullptr;
+  CK(cudaMalloc(&d_p, part.size() * sizeof(double)));
+  Ctx<double> c = e->c;
+  c.part = d_p;
+  k_link_diag<double><<<dim3(nbs, T), kDiagThreads, 0, e->s>>>(c, lcu, nbs);
+  LAUNCHED(1);
+  CK(cudaMemcpyAsync(part.data(), d_p, part.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost, e->s));
+  CK(cudaStreamSynchronize(e->s));
+  cudaFree(d_p);
+  // fixed-order sums; const_time: per slice t >= 1 the differences of the
+  // Hermitian-projection sums from slice 0 (gftests.c:84-95)
+  double sp = 0.0, tl = 0.0, mx = -1e300;
+  std::vector<std::array<double, 8>> hs(T);
+  for (int t = 0; t < T; t++) {
+    hs[t].fill(0.0);
+    for (int b = 0; b < nbs; b++) {
+      const double *q = &part[(size_t)kDiagVals * ((size_t)t * nbs + b)];
+      sp += q[0];
+      tl += q[1];
+      mx = std::max(mx, q[2]);
+      for (int k = 0; k < 8; k++) hs[t][k] += q[3 + k];
+    }
+  }
+  double av = 0.0;
+  for (int t = 1; t < T; t++) {
+    const auto &a = hs[0], &b = hs[t];
+    av += std::fabs(a[0] - b[0]);
+    av += std::hypot(a[1] - b[1], a[2] - b[2]);
+    av += std::hypot(a[3] - b[3], a[4] - b[4]);
+    av += std::fabs(a[5] - b[5]);
+    av += std::hypot(a[6] - b[6], a[7] - b[7]);
+  }
+  const double V = (double)e->V;
+  out[0] = sp / (3.0 * 3.0 * V);        // all_links: spatial
+  out[1] = tl / (3.0 * V);              //            temporal
+  out[2] = (sp + tl) / (4.0 * 3.0 * V); // indivlinks average
+  out[3] = mx / 3.0;                    // largest Re tr / NC
+  out[4] = T > 1 ? av / (9.0 * (T - 1)) : 0.0;  // const_time, linear
   return 0;
 }
 

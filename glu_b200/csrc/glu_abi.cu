@@ -182,9 +182,13 @@ size_t Landau(struct site *lat, const double accuracy, const size_t iter,
   double obs[3] = {0, 0, 0};
   gfix_observables(buf.p, d, obs);
   scatter(L, buf.p, V);
+  double dg[5] = {0, 0, 0, 0, 0};
+  gfix_link_diagnostics(buf.p, d, dg);
   printf("[GF] Plaquette :: %1.15f \n[GF] Accuracy :: %1.4e\n", obs[2],
          r.theta);
-  printf("[GF] Iters :: %zu\n", r.iters);
+  printf("[GF] Iters :: %zu\n[GF] Link trace :: %1.15f || Maximum :: %1.15f\n",
+         r.iters, dg[2], dg[3]);
+  printf("[GF] Temporal constance || Lin %e || Log (not computed)\n", dg[4]);
   printf("[GF] Functional :: %1.15f\n", obs[1]);
   return r.iters;
 }
@@ -237,11 +241,13 @@ size_t Coulomb(struct site *lat, const double accuracy, const size_t iter) {
   if (!buf.p) return it;
   gather(L, buf.p, V);
   gfix_reunit(buf.p, d);
-  double obs[3] = {0, 0, 0};
+  double obs[3] = {0, 0, 0}, dg[5] = {0, 0, 0, 0, 0};
   gfix_observables(buf.p, d, obs);
+  gfix_link_diagnostics(buf.p, d, dg);
   scatter(L, buf.p, V);
-  printf("[GF] Tuning :: %f || Iterations :: %zu ||\n[GF] Plaquette :: %1.15f \n",
-         Latt.gf_alpha, it, obs[2]);
+  printf("[GF] Tuning :: %f || Iterations :: %zu ||\n[GF] Final Tlink :: %1.15f "
+         "|| Slink :: %1.15f \n[GF] Plaquette :: %1.15f \n",
+         Latt.gf_alpha, it, dg[1], dg[0], obs[2]);
   return it;
 }
 

@@ -179,6 +179,16 @@ int gfix_coulomb_slices_finish(double *d_links, const size_t dims[4],
  * (src/Field/plaqs_links.c:243-265).  out[0..2] in that order. */
 int gfix_observables(const double *links, const size_t dims[4], double *out);
 
+/* GLU's post-fix link diagnostics on host links (output_fixing_info,
+ * src/Gfix/Landau.c:42-66; all_links in Coulomb, Coulomb.c:37-41):
+ * out[0] spatial and out[1] temporal average Re tr / NC (all_links,
+ * src/Field/plaqs_links.c:399-420), out[2] average Re tr / NC of all links
+ * and out[3] the largest Re tr / NC (indivlinks, plaqs_links.c:424-446),
+ * out[4] the temporal constancy, linear definition (const_time,
+ * src/Gfix/gftests.c:35-129; its logarithmic twin is not computed). */
+int gfix_link_diagnostics(const double *links, const size_t dims[4],
+                          double *out);
+
 /* Reunitarise every link (GLU's latt_reunitU, src/Geometry/random_config.c:
  * 42-57) on the GPU, host links in place. */
 int gfix_reunit(double *links, const size_t dims[4]);

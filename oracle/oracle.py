@@ -206,6 +206,12 @@ class Reference:
                   "ref_av_plaquette", "ref_fft_seconds"):
             getattr(L, n).restype = C.c_double
             getattr(L, n).argtypes = []
+        L.ref_all_links.restype = C.c_double
+        L.ref_all_links.argtypes = [_dp, _dp]
+        L.ref_indivlinks.restype = C.c_double
+        L.ref_indivlinks.argtypes = [_dp]
+        L.ref_const_time.restype = None
+        L.ref_const_time.argtypes = [_dp, _dp]
         L.ref_landau_fa.restype = _sz
         L.ref_landau_fa.argtypes = [C.c_int, C.c_double, _sz, _dp, _dp, _dp,
                                     _sz, _szp]
@@ -253,6 +259,16 @@ class Reference:
 
     def plaquette(self):
         return self.lib.ref_av_plaquette()
+
+    def diagnostics(self):
+        """(splink, tlink, all, indivlinks average, indivlinks max,
+        const_time lin, const_time log) of the lattice in place."""
+        sp, t, mx, lin, lg = (np.zeros(1) for _ in range(5))
+        al = self.lib.ref_all_links(_ptr(sp), _ptr(t))
+        avg = self.lib.ref_indivlinks(_ptr(mx))
+        self.lib.ref_const_time(_ptr(lin), _ptr(lg))
+        return (float(sp[0]), float(t[0]), float(al), float(avg), float(mx[0]),
+                float(lin[0]), float(lg[0]))
 
     def landau_fa(self, acc, max_iters, algo="FACG", traj_cap=0):
         th = np.zeros(1)

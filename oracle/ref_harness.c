@@ -126,6 +126,20 @@ double ref_gauge_functional(void) { return gauge_functional(g_lat); }
 double ref_av_plaquette(void) { return av_plaquette(g_lat); }
 void ref_latt_reunitU(void) { latt_reunitU(g_lat); }
 
+/* post-fix diagnostics of GLU's output (Landau.c:42-66, Coulomb.c:37-41):
+ * all_links, indivlinks (src/Field/plaqs_links.c:399-446), const_time
+ * (src/Gfix/gftests.c:35-129) */
+double ref_all_links(double *sp_link, double *t_link) {
+  return all_links(g_lat, sp_link, t_link);
+}
+double ref_indivlinks(double *max) {
+  GLU_real m = 0.0;
+  const double avg = indivlinks(g_lat, &m);
+  *max = (double)m;
+  return avg;
+}
+void ref_const_time(double *lin, double *lg) { const_time(g_lat, lin, lg); }
+
 double ref_fft_seconds(void) { return glu_shim_fft_seconds(); }
 void ref_reset_fft_seconds(void) { glu_shim_reset_fft_seconds(); }
 

@@ -137,7 +137,34 @@ def pack(prefix: str, r: dict, store: dict, links=True):
         store[f"{prefix}_links"] = r["links"]
 
 
+DIAG_KEYS = ("splink", "tlink", "all", "link", "link_max_trace", "const_lin",
+             "const_log")
+
+
+def diagnostics(R: Reference, links) -> np.ndarray:
+    """GLU's all_links, indivlinks and const_time of `links` (the lattice
+    set up in R): the 7 values of Reference.diagnostics."""
+    R.put_links(links)
+    return np.array(R.diagnostics())
+
+
+def add_diagnostics() -> None:
+    """Adds GLU's link diagnostics of the input and of the fixed links to
+    the existing fixtures (lat400: input, Landau FACG, Coulomb FACG links)."""
+    R = Reference()
+    g = dict(np.load(OUT / "lat400.npz"))
+    R.setup(tuple(int(d) for d in g["dims"]), 1, 0.08)
+    for key, links in (("input", g["links"]), ("landau", g["landau_facg_links"]),
+                       ("coulomb", g["coulomb_facg_links"])):
+        g[f"diag_{key}"] = diagnostics(R, links)
+    np.savez(OUT / "lat400.npz", **g)
+    print("lat400 diagnostics:", {k: v for k, v in g.items() if k.startswith("diag")})
+
+
 def main() -> None:
+    if "--diagnostics" in sys.argv:
+        add_diagnostics()
+        return
     R = Reference()
     RSD = Reference(sd_build=True)
 
@@ -157,6 +184,7 @@ def main() -> None:
     pack("coulomb_fasd_sd", coulomb_case(RSD, U, 0.09, "FASD"), st)
     np.savez(OUT / "lat400.npz", **st)
     print("lat400:", {k: v for k, v in st.items() if k.endswith("iters")})
+    add_diagnostics()
 
     # ---- 8^4 heatbath configuration -------------------------------------
     with tempfile.TemporaryDirectory() as td:

@@ -60,6 +60,24 @@ def test_fourier_accelerate3_matches_oracle(oracle, dims):
     assert np.abs(got - ref).max() < 1e-13 * np.abs(ref).max()
 
 
+@pytest.mark.parametrize("which", ["input", "landau", "coulomb"])
+def test_link_diagnostics_match_reference(lat400, which):
+    """all_links, indivlinks and the linear const_time of GLU (fixture values
+    from the reference build) on the input and on the fixed links."""
+    g = lat400
+    links = {"input": g["links"], "landau": g["landau_facg_links"],
+             "coulomb": g["coulomb_facg_links"]}[which]
+    ref = g[f"diag_{which}"]
+    got = gfix.link_diagnostics(links, _dims(g))
+    assert abs(got["splink"] - ref[0]) < 1e-14
+    assert abs(got["tlink"] - ref[1]) < 1e-14
+    assert abs(got["link"] - ref[3]) < 1e-14
+    # GLU prints the maximum trace divided by NC
+    assert abs(got["link_max"] - ref[4] / 3.0) < 1e-14
+    # a difference of slice sums of O(1) entries: rounding floor ~1e-15
+    assert abs(got["const_lin"] - ref[5]) <= 1e-12 * ref[5] + 1e-15
+
+
 def test_reunit_matches_oracle(oracle, lat400):
     g = lat400
     rng = np.random.default_rng(1)
