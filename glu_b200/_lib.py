@@ -39,7 +39,8 @@ EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
            "gfix_batch_add", "gfix_batch_add_device", "gfix_batch_run",
            "gfix_batch_result", "gfix_batch_destroy", "gfix_coulomb_slices",
            "gfix_coulomb_slices_finish", "gfix_fft_tuning", "gfix_fft_plan",
-           "gfix_link_diagnostics",
+           "gfix_link_diagnostics", "gfix_nersc_decode", "gfix_nersc_encode",
+           "gfix_nersc_error",
            "gfix_noalloc_error",
            "gfix_last_error", "gfix_release", "gfix_kernel_launches")
 
@@ -72,6 +73,12 @@ def load(path: Path | str | None = None):
                                      C.POINTER(GfixResult), _dp, _szp]
     lib.gfix_observables.restype = C.c_int
     lib.gfix_observables.argtypes = [C.c_void_p, _szp, _dp]
+    for fn in ("gfix_nersc_decode", "gfix_nersc_encode"):
+        getattr(lib, fn).restype = C.c_int
+        getattr(lib, fn).argtypes = [C.c_void_p, _szp, C.c_int, C.c_int, C.c_int,
+                                     C.c_void_p, C.POINTER(C.c_uint32)]
+    lib.gfix_nersc_error.restype = C.c_char_p
+    lib.gfix_nersc_error.argtypes = []
     lib.gfix_link_diagnostics.restype = C.c_int
     lib.gfix_link_diagnostics.argtypes = [C.c_void_p, _szp, _dp]
     lib.gfix_reunit.restype = C.c_int

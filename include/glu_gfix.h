@@ -27,6 +27,7 @@
 #define GLU_B200_GFIX_H
 
 #include <stddef.h>
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -255,6 +256,25 @@ void gfix_fft_tuning(int on);
  * precision: GFIX_MIXED reports the FP32 workspace. */
 int gfix_fft_plan(const size_t dims[4], int coulomb, int precision, int *plan,
                   float *ms);
+
+/* NERSC configuration payloads on the GPU (GLU's I/O layer,
+ * src/IO/readers.c:169-310, src/IO/writers.c): the binary part of a NERSC
+ * file -- per site (x fastest), per direction, nreal = 12 (4D_SU3_GAUGE, the
+ * top two rows; the third is completed as conj(row0 x row1),
+ * readers.c:50-58) or 18 (4D_SU3_GAUGE_3x3) reals of bytes_per_real = 8
+ * (IEEE64) or 4 (IEEE32), big-endian when big_endian != 0 -- to GLU's
+ * double[V][4][9][2] links and back.  *checksum (may be NULL) receives the
+ * NERSC checksum: the 32-bit wrapping sum over the stored numbers, in host
+ * byte order, of their 32-bit words (readers.c:279-293).  Header lines are
+ * the caller's (glu_b200/nersc.py parses and writes them).  Host pointers;
+ * returns 0 or -1 with the reason in gfix_nersc_error(). */
+int gfix_nersc_decode(const void *payload, const size_t dims[4], int nreal,
+                      int bytes_per_real, int big_endian, double *links,
+                      uint32_t *checksum);
+int gfix_nersc_encode(const double *links, const size_t dims[4], int nreal,
+                      int bytes_per_real, int big_endian, void *payload,
+                      uint32_t *checksum);
+const char *gfix_nersc_error(void);
 
 /* message of the last failed call (thread-local, never NULL) */
 const char *gfix_last_error(void);

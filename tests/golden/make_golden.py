@@ -161,9 +161,41 @@ def add_diagnostics() -> None:
     print("lat400 diagnostics:", {k: v for k, v in g.items() if k.startswith("diag")})
 
 
+def nersc_fixture() -> None:
+    """tests/golden/lat400.nersc: the 4^3x8 fixture links as a NERSC file
+    (4D_SU3_GAUGE, IEEE64BIG), written by this numpy encoder and checked by
+    GLU's own reader (checksum, plaquette and link trace of the header, and
+    every link read back equal to the fixture's)."""
+    g = dict(np.load(OUT / "lat400.npz"))
+    U = g["links"]
+    dims = tuple(int(d) for d in g["dims"])
+    top = np.ascontiguousarray(U[:, :, :2, :]).view(np.float64)
+    ck = int(np.frombuffer(top.astype("<f8").tobytes(), "<u4").sum(dtype=np.uint64)
+             & 0xFFFFFFFF)
+    trace = float(np.trace(U, axis1=-2, axis2=-1).real.mean() / 3.0)
+    hdr = ["BEGIN_HEADER", "HDR_VERSION = 1.0", "DATATYPE = 4D_SU3_GAUGE",
+           "STORAGE_FORMAT = 1.0"]
+    hdr += [f"DIMENSION_{k + 1} = {dims[k]}" for k in range(4)]
+    hdr += ["LINK_TRACE = %1.15f" % trace, "PLAQUETTE = %1.15f" % float(g["plaquette"])]
+    hdr += [f"BOUNDARY_{k + 1} = PERIODIC" for k in range(4)]
+    hdr += ["CHECKSUM = %x" % ck, "ENSEMBLE_ID = glu_b200_fixture",
+            "SEQUENCE_NUMBER = 400", "FLOATING_POINT = IEEE64BIG", "END_HEADER"]
+    path = OUT / "lat400.nersc"
+    with open(path, "wb") as f:
+        f.write(("\n".join(hdr) + "\n").encode("ascii"))
+        f.write(top.astype(">f8").tobytes())
+    R = Reference()
+    back = R.read_file(path)
+    assert np.array_equal(back, U), "GLU read the file differently"
+    print("lat400.nersc: checksum %x accepted by GLU's reader" % ck)
+
+
 def main() -> None:
     if "--diagnostics" in sys.argv:
         add_diagnostics()
+        return
+    if "--nersc" in sys.argv:
+        nersc_fixture()
         return
     R = Reference()
     RSD = Reference(sd_build=True)
@@ -185,6 +217,7 @@ def main() -> None:
     np.savez(OUT / "lat400.npz", **st)
     print("lat400:", {k: v for k, v in st.items() if k.endswith("iters")})
     add_diagnostics()
+    nersc_fixture()
 
     # ---- 8^4 heatbath configuration -------------------------------------
     with tempfile.TemporaryDirectory() as td:
