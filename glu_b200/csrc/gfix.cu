@@ -867,8 +867,11 @@ class Engine {
     }
     for (auto &e : ev) cudaEventDestroy(e);
     const double B = sizeof(cx<R>) * (double)V;  // one complex per site
+    // update: links in and out, the direction; with G (the FP32 phase of
+    // mixed precision) also the accumulated transform in and out
     const double b[7] = {(36 + 4) * B, 8 * B, 8 * B, 12 * B,
-                         (36 + 4 + 4 + 4) * B, (36 + 4 + 36) * B, 0.0};
+                         (36 + 4 + 4 + 4) * B,
+                         (36 + 4 + 36 + (c.G ? 18 : 0)) * B, 0.0};
     for (int k = 0; k < 7; k++) {
       ms[k] = acc[k] / n;
       if (bytes) bytes[k] = b[k];
