@@ -40,7 +40,7 @@ EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
            "gfix_batch_result", "gfix_batch_destroy", "gfix_coulomb_slices",
            "gfix_coulomb_slices_finish", "gfix_fft_tuning", "gfix_fft_plan",
            "gfix_link_diagnostics", "gfix_nersc_decode", "gfix_nersc_encode",
-           "gfix_nersc_error",
+           "gfix_nersc_error", "gfix_scidac_checksum",
            "gfix_noalloc_error",
            "gfix_last_error", "gfix_release", "gfix_kernel_launches")
 
@@ -77,6 +77,9 @@ def load(path: Path | str | None = None):
         getattr(lib, fn).restype = C.c_int
         getattr(lib, fn).argtypes = [C.c_void_p, _szp, C.c_int, C.c_int, C.c_int,
                                      C.c_void_p, C.POINTER(C.c_uint32)]
+    lib.gfix_scidac_checksum.restype = C.c_int
+    lib.gfix_scidac_checksum.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t,
+                                         C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     lib.gfix_nersc_error.restype = C.c_char_p
     lib.gfix_nersc_error.argtypes = []
     lib.gfix_link_diagnostics.restype = C.c_int

@@ -146,6 +146,51 @@ __global__ void k_nersc_encode(const double2 *links, size_t nlinks, int nreal,
   block_add(ck, cksum);
 }
 
+// SCIDAC / ILDG checksums (src/IO/writers.c:210-224, readers.c:256-263):
+// per site the CRC-32 (the zlib / IEEE 802.3 polynomial, reflected) of the
+// site's stored bytes, rotated left by (site % 29) and by (site % 31), all
+// XORed -- exact in any order.  One thread per site, a 256-entry table.
+__constant__ uint32_t c_crc_table[256];
+
+__global__ void k_scidac_crc(const unsigned char *pay, size_t site_bytes,
+                             size_t nsites, uint32_t *sums) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  uint32_t a = 0, b = 0;
+  if (i < nsites) {
+    const unsigned char *p = pay + i * site_bytes;
+    uint32_t crc = 0xFFFFFFFFu;
+    for (size_t k = 0; k < site_bytes; k++)
+      crc = c_crc_table[(crc ^ p[k]) & 0xFFu] ^ (crc >> 8);
+    crc ^= 0xFFFFFFFFu;
+    const uint32_t r29 = (uint32_t)(i % 29), r31 = (uint32_t)(i % 31);
+    a = r29 ? (crc << r29) | (crc >> (32 - r29)) : crc;
+    b = r31 ? (crc << r31) | (crc >> (32 - r31)) : crc;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a ^= __shfl_down_sync(0xffffffffu, a, o);
+    b ^= __shfl_down_sync(0xffffffffu, b, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicXor(sums, a);
+    atomicXor(sums + 1, b);
+  }
+}
+
+int upload_crc_table() {
+  static bool done = false;
+  if (done) return 0;
+  uint32_t t[256];
+  for (uint32_t n = 0; n < 256; n++) {
+    uint32_t c = n;
+    for (int k = 0; k < 8; k++) c = (c & 1) ? 0xEDB88320u ^ (c >> 1) : c >> 1;
+    t[n] = c;
+  }
+  NCK(cudaMemcpyToSymbol(c_crc_table, t, sizeof t));
+  done = true;
+  return 0;
+}
+
 int check_args(const size_t dims[4], int nreal, int bytes, size_t *nlinks) {
   if (!dims) return nfail("null dims");
   if (nreal != 12 && nreal != 18) return nfail("reals per link must be 12 or 18");
@@ -260,6 +305,48 @@ int gfix_nersc_encode(const double *links, const size_t dims[4], int nreal,
   cudaFree(d_p);
   cudaFree(d_l);
   cudaFree(d_c);
+  if (s) cudaStreamDestroy(s);
+  return rc;
+}
+
+int gfix_scidac_checksum(const void *payload, size_t site_bytes, size_t nsites,
+                         uint32_t *suma, uint32_t *sumb) {
+  if (!payload || !site_bytes || !suma || !sumb) return nfail("null argument");
+  if (upload_crc_table()) return -1;
+  const size_t bytes = site_bytes * nsites;
+  unsigned char *d_p = nullptr;
+  uint32_t *d_s = nullptr;
+  int rc = 0;
+  cudaStream_t s = nullptr;
+  do {
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) ||
+        (e = cudaMalloc(&d_p, bytes ? bytes : 1)) ||
+        (e = cudaMalloc(&d_s, 2 * sizeof(uint32_t)))) {
+      rc = nfail("device buffers", e);
+      break;
+    }
+    if ((e = cudaMemsetAsync(d_s, 0, 2 * sizeof(uint32_t), s)) ||
+        (e = cudaMemcpyAsync(d_p, payload, bytes, cudaMemcpyHostToDevice, s))) {
+      rc = nfail("copy in", e);
+      break;
+    }
+    if (nsites) {
+      const unsigned nb = (unsigned)((nsites + 127) / 128);
+      k_scidac_crc<<<nb, 128, 0, s>>>(d_p, site_bytes, nsites, d_s);
+    }
+    uint32_t h[2] = {0, 0};
+    if ((e = cudaGetLastError()) ||
+        (e = cudaMemcpyAsync(h, d_s, sizeof h, cudaMemcpyDeviceToHost, s)) ||
+        (e = cudaStreamSynchronize(s))) {
+      rc = nfail("checksum", e);
+      break;
+    }
+    *suma = h[0];
+    *sumb = h[1];
+  } while (0);
+  cudaFree(d_p);
+  cudaFree(d_s);
   if (s) cudaStreamDestroy(s);
   return rc;
 }

@@ -276,6 +276,14 @@ int gfix_nersc_encode(const double *links, const size_t dims[4], int nreal,
                       uint32_t *checksum);
 const char *gfix_nersc_error(void);
 
+/* SCIDAC / ILDG checksums of a payload of nsites records of site_bytes
+ * bytes each, as stored (src/IO/writers.c:210-224, readers.c:256-263): per
+ * site the CRC-32 of its bytes, rotated left by site % 29 (suma) and by
+ * site % 31 (sumb), XORed over the sites.  The ILDG payload itself decodes
+ * with gfix_nersc_decode (18 reals, big-endian).  Host pointers. */
+int gfix_scidac_checksum(const void *payload, size_t site_bytes, size_t nsites,
+                         uint32_t *suma, uint32_t *sumb);
+
 /* message of the last failed call (thread-local, never NULL) */
 const char *gfix_last_error(void);
 

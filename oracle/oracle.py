@@ -206,6 +206,12 @@ class Reference:
                   "ref_av_plaquette", "ref_fft_seconds"):
             getattr(L, n).restype = C.c_double
             getattr(L, n).argtypes = []
+        L.ref_read_file_as.restype = C.c_int
+        L.ref_read_file_as.argtypes = [C.c_char_p, _szp, C.c_int, C.c_int]
+        L.ref_write_config.restype = C.c_int
+        L.ref_write_config.argtypes = [C.c_char_p, C.c_int, C.c_char_p]
+        L.ref_output_code.restype = C.c_int
+        L.ref_output_code.argtypes = [C.c_char_p]
         L.ref_all_links.restype = C.c_double
         L.ref_all_links.argtypes = [_dp, _dp]
         L.ref_indivlinks.restype = C.c_double
@@ -228,9 +234,10 @@ class Reference:
         if self.lib.ref_setup(_dims(dims), nthreads, alpha, seed) != 0:
             raise RuntimeError("reference lattice allocation failed")
 
-    def read_file(self, path, nthreads=1):
+    def read_file(self, path, nthreads=1, ildg=False):
         d = (C.c_size_t * 4)()
-        if self.lib.ref_read_file(str(path).encode(), d, nthreads) != 0:
+        if self.lib.ref_read_file_as(str(path).encode(), d, nthreads,
+                                     1 if ildg else 0) != 0:
             raise RuntimeError(f"reference could not read {path}")
         self.dims = tuple(d)
         return self.get_links()
@@ -259,6 +266,14 @@ class Reference:
 
     def plaquette(self):
         return self.lib.ref_av_plaquette()
+
+    def write(self, path, storage="ILDG", details="glu_b200 fixture"):
+        """GLU's write_configuration of the lattice in place (which
+        reunitarises it first)."""
+        code = self.lib.ref_output_code(storage.encode())
+        if code < 0 or self.lib.ref_write_config(str(path).encode(), code,
+                                                 details.encode()) != 0:
+            raise RuntimeError(f"reference could not write {path}")
 
     def diagnostics(self):
         """(splink, tlink, all, indivlinks average, indivlinks max,

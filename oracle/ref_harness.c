@@ -29,6 +29,7 @@
 #include "random_config.h"
 
 #include <omp.h>
+#include <string.h>
 
 /* GLU's global lattice description (src/Run/Mainfile.c:30) */
 struct latt_info Latt;
@@ -68,17 +69,21 @@ int ref_setup(const size_t *dims, int nthreads, double gf_alpha,
   return 0;
 }
 
-/* read a configuration file with GLU's own reader; dims are returned */
-int ref_read_file(const char *path, size_t *dims_out, int nthreads) {
+/* read a configuration file with GLU's own reader; dims are returned.
+ * head: 0 NERSC, 1 ILDG (SciDAC LIME) */
+int ref_read_file_as(const char *path, size_t *dims_out, int nthreads, int head) {
   free_lattice();
   set_threads(nthreads);
-  Latt.head = NERSC_HEADER;
+  Latt.head = head == 1 ? ILDG_SCIDAC_HEADER : NERSC_HEADER;
   Latt.Seed[0] = 1;
   struct head_data HEAD;
   g_lat = read_file(&HEAD, path);
   if (g_lat == NULL) return -1;
   for (int mu = 0; mu < ND; mu++) dims_out[mu] = Latt.dims[mu];
   return 0;
+}
+int ref_read_file(const char *path, size_t *dims_out, int nthreads) {
+  return ref_read_file_as(path, dims_out, nthreads, 0);
 }
 
 void ref_set_alpha(double gf_alpha) { Latt.gf_alpha = gf_alpha; }
@@ -139,6 +144,19 @@ double ref_indivlinks(double *max) {
   return avg;
 }
 void ref_const_time(double *lin, double *lg) { const_time(g_lat, lin, lg); }
+
+/* GLU's writer (src/IO/writers.c:329-420, write_configuration): storage
+ * is a GLU_output value (OUTPUT_ILDG, OUTPUT_GAUGE, ...) */
+int ref_write_config(const char *path, int storage, const char *details) {
+  return write_configuration(g_lat, path, (GLU_output)storage, details);
+}
+int ref_output_code(const char *name) {
+  if (!strcmp(name, "ILDG")) return OUTPUT_ILDG;
+  if (!strcmp(name, "SCIDAC")) return OUTPUT_SCIDAC;
+  if (!strcmp(name, "NERSC_GAUGE")) return OUTPUT_GAUGE;
+  if (!strcmp(name, "NERSC_NCxNC")) return OUTPUT_NCxNC;
+  return -1;
+}
 
 double ref_fft_seconds(void) { return glu_shim_fft_seconds(); }
 void ref_reset_fft_seconds(void) { glu_shim_reset_fft_seconds(); }

@@ -190,7 +190,26 @@ def nersc_fixture() -> None:
     print("lat400.nersc: checksum %x accepted by GLU's reader" % ck)
 
 
+def ildg_fixture() -> None:
+    """tests/golden/lat400.ildg: the 4^3x8 fixture links written by GLU's own
+    ILDG writer (which reunitarises them first); the links GLU reads back
+    are stored as lat400.npz["ildg_links"]."""
+    g = dict(np.load(OUT / "lat400.npz"))
+    R = Reference()
+    R.setup(tuple(int(d) for d in g["dims"]), 1, 0.08)
+    R.put_links(g["links"])
+    path = OUT / "lat400.ildg"
+    path.unlink(missing_ok=True)  # GLU's writer does not overwrite
+    R.write(path, "ILDG", "glu_b200 fixture")
+    g["ildg_links"] = Reference().read_file(path, ildg=True)
+    np.savez(OUT / "lat400.npz", **g)
+    print("lat400.ildg written by GLU,", path.stat().st_size, "bytes")
+
+
 def main() -> None:
+    if "--ildg" in sys.argv:
+        ildg_fixture()
+        return
     if "--diagnostics" in sys.argv:
         add_diagnostics()
         return
@@ -218,6 +237,7 @@ def main() -> None:
     print("lat400:", {k: v for k, v in st.items() if k.endswith("iters")})
     add_diagnostics()
     nersc_fixture()
+    ildg_fixture()
 
     # ---- 8^4 heatbath configuration -------------------------------------
     with tempfile.TemporaryDirectory() as td:

@@ -63,3 +63,37 @@ def test_corrupted_payload_fails_the_checksum(tmp_path):
     bad.write_bytes(bytes(data))
     with pytest.raises(nersc.NerscError):
         nersc.read(bad)
+
+
+ILDG = Path(__file__).resolve().parent / "golden" / "lat400.ildg"
+
+
+def test_ildg_read_matches_glu(lat400):
+    from glu_b200 import ildg
+    U, dims, info = ildg.read(ILDG)  # SciDAC checksums verified
+    assert dims == tuple(int(d) for d in lat400["dims"])
+    assert np.array_equal(U, lat400["ildg_links"])
+    assert (info["suma"], info["sumb"]) == (0xD00BA925, 0xC215FD4E)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_ildg_write_round_trip(hb8, tmp_path, precision):
+    from glu_b200 import ildg
+    dims = tuple(int(d) for d in hb8["dims"])
+    out = tmp_path / "w.ildg"
+    ildg.write(out, hb8["links"], dims, precision)
+    U, d2, info = ildg.read(out)
+    assert d2 == dims and info["precision"] == precision
+    tol = 0.0 if precision == 64 else 3e-7
+    assert np.abs(U - hb8["links"]).max() <= tol
+
+
+def test_glu_reads_our_ildg_file(reference, lat400, tmp_path):
+    """GLU's own reader on a file written by ildg.write (the reference build
+    travels with the repository as oracle/_ref)."""
+    from glu_b200 import ildg
+    dims = tuple(int(d) for d in lat400["dims"])
+    out = tmp_path / "ours.ildg"
+    ildg.write(out, lat400["ildg_links"], dims)
+    back = reference.read_file(out, ildg=True)
+    assert np.array_equal(back, lat400["ildg_links"])
