@@ -23,6 +23,12 @@ class GfixParams(C.Structure):
                 ("traj_func", _dp), ("traj_cap", C.c_size_t)]
 
 
+class GfixCutInfo(C.Structure):
+    _fields_ = [("dir", C.c_int), ("type", C.c_int), ("max_mom", C.c_size_t),
+                ("definition", C.c_int), ("angle", C.c_size_t),
+                ("cyl_width", C.c_double)]
+
+
 class GfixResult(C.Structure):
     _fields_ = [("iters", C.c_size_t), ("iters_fp32", C.c_size_t),
                 ("theta", C.c_double), ("traj_len", C.c_size_t),
@@ -40,7 +46,9 @@ EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
            "gfix_batch_result", "gfix_batch_destroy", "gfix_coulomb_slices",
            "gfix_coulomb_slices_finish", "gfix_fft_tuning", "gfix_fft_plan",
            "gfix_link_diagnostics", "gfix_nersc_decode", "gfix_nersc_encode",
-           "gfix_nersc_error", "gfix_scidac_checksum",
+           "gfix_nersc_error", "gfix_scidac_checksum", "gfix_cut_veclist",
+           "gfix_cuts_measure", "gfix_cuts_measure_device", "gfix_cuts_write",
+           "gfix_profile_cuts", "gfix_cuts_error", "gfix_cuts_release",
            "gfix_noalloc_error",
            "gfix_last_error", "gfix_release", "gfix_kernel_launches")
 
@@ -80,6 +88,21 @@ def load(path: Path | str | None = None):
     lib.gfix_scidac_checksum.restype = C.c_int
     lib.gfix_scidac_checksum.argtypes = [C.c_void_p, C.c_size_t, C.c_size_t,
                                          C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    _ci = C.POINTER(GfixCutInfo)
+    lib.gfix_cut_veclist.restype = C.c_long
+    lib.gfix_cut_veclist.argtypes = [_szp, _ci, C.POINTER(C.c_int32), C.c_size_t]
+    for fn in ("gfix_cuts_measure", "gfix_cuts_measure_device"):
+        getattr(lib, fn).restype = C.c_int
+        getattr(lib, fn).argtypes = [C.c_void_p, _szp, _ci, C.c_size_t, _dp, _dp, _dp]
+    lib.gfix_cuts_write.restype = C.c_int
+    lib.gfix_cuts_write.argtypes = [C.c_void_p, _szp, _ci, C.c_char_p, C.c_size_t,
+                                    _dp, C.c_char_p, C.c_size_t]
+    lib.gfix_profile_cuts.restype = C.c_int
+    lib.gfix_profile_cuts.argtypes = [C.c_void_p, _szp, _ci, C.c_int,
+                                      C.POINTER(C.c_float)]
+    lib.gfix_cuts_error.restype = C.c_char_p
+    lib.gfix_cuts_error.argtypes = []
+    lib.gfix_cuts_release.restype = None
     lib.gfix_nersc_error.restype = C.c_char_p
     lib.gfix_nersc_error.argtypes = []
     lib.gfix_link_diagnostics.restype = C.c_int

@@ -135,6 +135,43 @@ __device__ __forceinline__ void dft_reg(cx<R> *v, const cx<R> *tw, int N,
   }
 }
 
+// radices 8, 4, 2, 3, 5, 7 and the Stockham stage table of length n
+// radix orders of the generic passes' stage tables (the autotuner tries
+// them; 0, largest radices first, is the default)
+constexpr int kRadixOrders = 3;
+constexpr int kRadixPref[kRadixOrders][6] = {
+    {8, 4, 2, 3, 5, 7}, {4, 8, 2, 3, 5, 7}, {2, 4, 8, 3, 5, 7}};
+
+static inline int factorize(int n, FftAxis &ax, int order = 0) {
+  ax.n = n;
+  ax.nstages = 0;
+  int m = n;
+  int rad[kMaxStages];
+  int ns = 0;
+  const int *pref = kRadixPref[order];
+  for (int i = 0; i < 6; i++)
+    for (const int r = pref[i]; m % r == 0 && m > 1;) {
+      if (ns == kMaxStages) return -1;
+      rad[ns++] = r;
+      m /= r;
+    }
+  if (m > 1) return -1;  // a prime factor above kMaxRadix
+  if (ns == 0) rad[ns++] = 1;
+  int Ns = 1;
+  for (int k = 0; k < ns; k++) {
+    FftStage &S = ax.st[k];
+    S.r = rad[k];
+    S.nb = n / rad[k];
+    S.Ns = Ns;
+    S.step0 = n / (Ns * rad[k]);
+    S.nb_sh = log2_if_pow2(S.nb);
+    S.ns_sh = log2_if_pow2(Ns);
+    Ns *= rad[k];
+  }
+  ax.nstages = ns;
+  return 0;
+}
+
 // Elements one thread holds per stage (PT): a tile of n elements is handled
 // by at least n / PT threads.  8 in FP64 and 16 in FP32 keep the butterflies
 // in registers; 16 in FP64 serves tiles too large for 512 threads.
@@ -205,5 +242,82 @@ __device__ void smem_fft(cx<R> *buf, const PencilMap &m, const FftAxis &ax,
     }
   }
 }
+
+// ---------------------------------------------------------------------
+// compile-time Stockham stages (every extent, stride and pencil mapping a
+// template constant), used by the compile-time passes
+
+// radix of the next stage for a remaining length m
+__host__ __device__ constexpr int ct_radix(int m) {
+  return (m % 8 == 0) ? 8 : (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2 : 3;
+}
+// can the extent be transformed by the compile-time stages?
+__host__ __device__ constexpr bool ct_ok(int n) {
+  while (n % 2 == 0) n /= 2;
+  while (n % 3 == 0) n /= 3;
+  return n == 1;
+}
+
+// Stockham stages for pencils of length N; pencil p starts at
+// (p / PIN) * PSHI + (p % PIN) * PSLO, elements are JS apart; BD threads.
+// Consecutive threads take consecutive pencils at the same butterfly index:
+// their elements are neighbours in shared memory (no bank conflicts for the
+// tile layouts below) and they share one twiddle factor (a broadcast).
+template <typename R, int N, int Ns, int NP, int PIN, int PSLO, int PSHI,
+          int JS, int BD>
+__device__ __forceinline__ void ct_stages(cx<R> *buf, const cx<R> *tw,
+                                          bool bwd) {
+  if constexpr (Ns < N) {
+    constexpr int RDX = ct_radix(N / Ns);
+    constexpr int NB = N / RDX;
+    constexpr int TOTAL = NP * NB;
+    constexpr int K = (TOTAL + BD - 1) / BD;
+    constexpr int STEP0 = N / (Ns * RDX);
+    cx<R> v[K][RDX];
+    int dst[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      const int idx = threadIdx.x + k * BD;
+      dst[k] = -1;
+      if (TOTAL % BD == 0 || idx < TOTAL) {
+        const int p = idx % NP, j = idx / NP;
+        const int po = (p / PIN) * PSHI + (p % PIN) * PSLO;
+        const int jq = j / Ns, jm = j % Ns;
+#pragma unroll
+        for (int s = 0; s < RDX; s++) {
+          v[k][s] = buf[po + (j + s * NB) * JS];
+          if constexpr (Ns > 1)
+            if (s > 0) v[k][s] = cmul(v[k][s], twiddle(tw, s * jm * STEP0, bwd));
+        }
+        dft_reg<R, RDX>(v[k], tw, N, bwd);
+        dst[k] = po + (jq * Ns * RDX + jm) * JS;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (dst[k] >= 0) {
+#pragma unroll
+        for (int s = 0; s < RDX; s++) buf[dst[k] + s * Ns * JS] = v[k][s];
+      }
+    }
+    __syncthreads();
+    ct_stages<R, N, Ns * RDX, NP, PIN, PSLO, PSHI, JS, BD>(buf, tw, bwd);
+  }
+}
+
+// threads of a tile of n elements: one radix-8 butterfly each (32..1024
+// threads), two for tiles above 8192 elements
+__host__ __device__ constexpr int ct_threads(int n) {
+  return n / 8 < 32 ? 32 : (n / 8 <= 1024 ? n / 8 : n / 16);
+}
+// resident blocks asked of the compiler: 1024 threads per SM at least
+__host__ __device__ constexpr int ct_minb(int n) {
+  return 1024 / ct_threads(n) < 1 ? 1 : 1024 / ct_threads(n);
+}
+// padding of the t-stride of a zt tile of B x columns: t-planes start B
+// elements apart modulo 8, so the z-stage pencils of 8 (FP64) or 16 (FP32)
+// consecutive threads fall in distinct banks
+__host__ __device__ constexpr int zt_pad(int b) { return b < 16 ? b : 0; }
 
 }  // namespace gfix

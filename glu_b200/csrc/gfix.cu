@@ -54,43 +54,6 @@ static int fail(const char *fmt, ...) {
 
 constexpr size_t kSentinel = 123456789;
 
-// radices 8, 4, 2, 3, 5, 7 and the Stockham stage table of length n
-// radix orders of the generic passes' stage tables (the autotuner tries
-// them; 0, largest radices first, is the default)
-constexpr int kRadixOrders = 3;
-static const int kRadixPref[kRadixOrders][6] = {
-    {8, 4, 2, 3, 5, 7}, {4, 8, 2, 3, 5, 7}, {2, 4, 8, 3, 5, 7}};
-
-static int factorize(int n, FftAxis &ax, int order = 0) {
-  ax.n = n;
-  ax.nstages = 0;
-  int m = n;
-  int rad[kMaxStages];
-  int ns = 0;
-  const int *pref = kRadixPref[order];
-  for (int i = 0; i < 6; i++)
-    for (const int r = pref[i]; m % r == 0 && m > 1;) {
-      if (ns == kMaxStages) return -1;
-      rad[ns++] = r;
-      m /= r;
-    }
-  if (m > 1) return -1;  // a prime factor above kMaxRadix
-  if (ns == 0) rad[ns++] = 1;
-  int Ns = 1;
-  for (int k = 0; k < ns; k++) {
-    FftStage &S = ax.st[k];
-    S.r = rad[k];
-    S.nb = n / rad[k];
-    S.Ns = Ns;
-    S.step0 = n / (Ns * rad[k]);
-    S.nb_sh = log2_if_pow2(S.nb);
-    S.ns_sh = log2_if_pow2(Ns);
-    Ns *= rad[k];
-  }
-  ax.nstages = ns;
-  return 0;
-}
-
 // FFT plans: 0 = the default plan per shape (bit-reproducible runs), 1 =
 // autotuned per shape at first use (gfix_fft_tuning, GLU_GFIX_FFT_TUNE=1)
 static int g_fft_tune = -1;
@@ -1660,6 +1623,7 @@ int gfix_fft_plan(const size_t dims[4], int coulomb, int precision, int *plan,
 }
 
 void gfix_release(void) {
+  gfix_cuts_release();
   g_e64.clear();
   g_e32.clear();
   g_ec.clear();

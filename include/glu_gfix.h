@@ -284,6 +284,74 @@ const char *gfix_nersc_error(void);
 int gfix_scidac_checksum(const void *payload, size_t site_bytes, size_t nsites,
                          uint32_t *suma, uint32_t *sumb);
 
+/* Momentum-space gluon measurements (GLU's cuts_struct, src/Cuts/cuts.c:
+ * 110-184, as cuts_wrap_struct calls it for CUTTYPE = GLUON_PROPS,
+ * EXCEPTIONAL and FIELDS, src/Wrappers/CUT_wrap.c:57-63).  The fields of
+ * GLU's struct cut_info (src/Headers/GLU_types.h:94-103) these modes read;
+ * enum values are GLU's (src/Headers/GLU_enum.h:161-195). */
+enum {
+  GFIX_CUT_EXCEPTIONAL = 0,    /* MOMgg g2, g3 (src/Cuts/MOMgg.c) */
+  GFIX_CUT_NONEXCEPTIONAL = 1, /* not provided */
+  GFIX_CUT_FIELDS = 2,         /* the fields at the kept momenta */
+  GFIX_CUT_GLUON_PROPS = 6     /* transverse / longitudinal (glueprop.c) */
+};
+enum {
+  GFIX_CUT_HYPERCUBIC = 0,
+  GFIX_CUT_PSQ = 1, /* SPHERICAL_CUT in the input file */
+  GFIX_CUT_CYLINDER = 2,
+  GFIX_CUT_CONICAL = 3
+};
+enum { GFIX_FIELD_LINEAR = 0, GFIX_FIELD_LOG = 1 };
+
+typedef struct gfix_cut_info {
+  int dir;          /* GFIX_CUT_GLUON_PROPS, _EXCEPTIONAL or _FIELDS */
+  int type;         /* momentum cut, GFIX_CUT_HYPERCUBIC .. _CONICAL */
+  size_t max_mom;   /* MAXMOM: largest (n_mu small/L_mu)^2 kept */
+  int definition;   /* GFIX_FIELD_LINEAR (Hermitian projection) */
+  size_t angle;     /* ANGLE of the conical cut, degrees */
+  double cyl_width; /* CYL_WIDTH in units of 2 pi / min(L) */
+} gfix_cut_info;
+
+/* compute_veclist (src/Cuts/cut_routines.c:459-631) in momentum space: the
+ * number of kept momenta (or -1); with mom, up to cap momenta as 4 ints
+ * each in GLU's order (lexicographic in the -pi..pi zone, x fastest).
+ * Host-only: needs no GPU. */
+long gfix_cut_veclist(const size_t dims[4], const gfix_cut_info *ci,
+                      int32_t *mom, size_t cap);
+
+/* the measurement of cuts_struct without its file: links are GLU's
+ * double[V][4][9][2] (host, or device for _device); nmom must be the count
+ * of gfix_cut_veclist.  GLUON_PROPS: out0 = transverse G(p^2), out1 =
+ * longitudinal F(p^2) (glueprop.c:89-146); EXCEPTIONAL: out0 = g2, out1 =
+ * g3 (MOMgg.c:160-211); FIELDS: out0 = nmom * 4 * 9 complex fields
+ * (interleaved re, im) times e^{i p_mu/2}, out1 unused.  pspace_err
+ * (may be NULL) receives the p-space gauge error GLU prints
+ * (src/Cuts/pspace_landau.c:78-80). */
+int gfix_cuts_measure(const double *links, const size_t dims[4],
+                      const gfix_cut_info *ci, size_t nmom, double *out0,
+                      double *out1, double *pspace_err);
+int gfix_cuts_measure_device(const double *d_links, const size_t dims[4],
+                             const gfix_cut_info *ci, size_t nmom,
+                             double *out0, double *out1, double *pspace_err);
+
+/* cuts_struct itself: measures and writes GLU's output file (big-endian,
+ * src/Cuts/cut_output.c:250-410), named as output_str_struct does
+ * (cut_output.c:121-242) after the prefix `where` (GLU's default build
+ * uses "./"); flow is the configuration number in the name.  The path is
+ * copied to path_out (may be NULL). */
+int gfix_cuts_write(const double *links, const size_t dims[4],
+                    const gfix_cut_info *ci, const char *where, size_t flow,
+                    double *pspace_err, char *path_out, size_t path_cap);
+
+/* per-kernel CUDA-event times (ms, mean of reps after one warm-up) of the
+ * measurement on device links: [0] Lie fields + x,y transforms, [1] z,t
+ * transforms, [2] gather + contraction */
+int gfix_profile_cuts(const double *d_links, const size_t dims[4],
+                      const gfix_cut_info *ci, int reps, float ms[3]);
+
+const char *gfix_cuts_error(void);
+void gfix_cuts_release(void);
+
 /* message of the last failed call (thread-local, never NULL) */
 const char *gfix_last_error(void);
 

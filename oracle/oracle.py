@@ -227,6 +227,15 @@ class Reference:
         L.ref_landau.argtypes = [C.c_double, _sz, C.c_char_p]
         L.ref_coulomb.restype = _sz
         L.ref_coulomb.argtypes = [C.c_double, _sz]
+        L.ref_veclist.restype = C.c_long
+        L.ref_veclist.argtypes = [C.c_int, C.c_int, _sz, _sz, C.c_double,
+                                  C.POINTER(C.c_int), _szp, _sz]
+        L.ref_cut_output_name.restype = C.c_int
+        L.ref_cut_output_name.argtypes = [C.c_int, C.c_int, _sz, C.c_int, _sz,
+                                          C.c_double, _sz, C.c_char_p, _sz]
+        L.ref_cuts.restype = C.c_int
+        L.ref_cuts.argtypes = [C.c_int, C.c_int, _sz, C.c_int, _sz, C.c_double,
+                               _sz, C.c_char_p]
         self.dims = None
 
     def setup(self, dims, nthreads=1, alpha=0.08, seed=1):
@@ -308,6 +317,35 @@ class Reference:
 
     def fft_seconds(self):
         return self.lib.ref_fft_seconds()
+
+    # momentum-space cuts (src/Cuts/cuts.c:110-184)
+    def veclist(self, dir, type, max_mom, angle=0, cyl_width=1.0):
+        """(MOM (n, 4), idx (n,)) of compute_veclist for the current dims."""
+        V = int(np.prod(self.dims))
+        mom = np.zeros((V, 4), dtype=np.int32)
+        idx = np.zeros(V, dtype=np.uint64)
+        n = self.lib.ref_veclist(dir, type, max_mom, angle, cyl_width,
+                                 mom.ctypes.data_as(C.POINTER(C.c_int)),
+                                 idx.ctypes.data_as(_szp), V)
+        return mom[:n].astype(np.int64), idx[:n].astype(np.int64)
+
+    def cut_output_name(self, dir, type, max_mom, definition=0, angle=0,
+                        cyl_width=1.0, flow=0):
+        buf = C.create_string_buffer(1024)
+        self.lib.ref_cut_output_name(dir, type, max_mom, definition, angle,
+                                     cyl_width, flow, buf, 1024)
+        return buf.value.decode()
+
+    def cuts(self, where, dir, type, max_mom, definition=0, angle=0,
+             cyl_width=1.0, flow=0):
+        """GLU's cuts_struct on the lattice in place; returns the path of
+        the file it wrote (the lattice then holds momentum-space fields)."""
+        name = self.cut_output_name(dir, type, max_mom, definition, angle,
+                                    cyl_width, flow)
+        if self.lib.ref_cuts(dir, type, max_mom, definition, angle, cyl_width,
+                             flow, str(where).encode()) != 0:
+            raise RuntimeError("reference cuts_struct failed")
+        return Path(where) / name
 
 
 def available() -> dict:

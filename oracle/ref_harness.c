@@ -20,6 +20,9 @@
 #include "Coulomb.h"
 #include "FACG.h"
 #include "GLUlib_wrap.h"
+#include "cut_output.h"
+#include "cut_routines.h"
+#include "cuts.h"
 #include "Landau.h"
 #include "geometry.h"
 #include "init.h"
@@ -30,6 +33,7 @@
 
 #include <omp.h>
 #include <string.h>
+#include <unistd.h>
 
 /* GLU's global lattice description (src/Run/Mainfile.c:30) */
 struct latt_info Latt;
@@ -270,4 +274,65 @@ size_t ref_landau(double acc, size_t max_iters, const char *infile) {
 
 size_t ref_coulomb(double acc, size_t max_iters) {
   return Coulomb(g_lat, acc, max_iters);
+}
+
+/* momentum-space cuts (src/Cuts/cuts.c:110-184, cuts_struct) */
+static struct cut_info cut_info_of(int dir, int type, size_t max_mom,
+                                   int definition, size_t angle,
+                                   double cyl_width) {
+  struct cut_info c;
+  memset(&c, 0, sizeof c);
+  c.dir = (cut_mode)dir;
+  c.type = (momentum_cut_def)type;
+  c.max_mom = max_mom;
+  c.definition = (lie_field_def)definition;
+  c.angle = angle;
+  c.cyl_width = cyl_width;
+  return c;
+}
+
+/* compute_veclist (src/Cuts/cut_routines.c:459) in momentum space: the
+ * number of momenta; up to cap entries of MOM (4 ints each) and idx */
+long ref_veclist(int dir, int type, size_t max_mom, size_t angle,
+                 double cyl_width, int *mom, size_t *idx, size_t cap) {
+  struct cut_info c = cut_info_of(dir, type, max_mom, LINEAR_DEF, angle,
+                                  cyl_width);
+  if (c.dir == NONEXCEPTIONAL) c.type = PSQ_CUT;
+  size_t n = 0;
+  struct veclist *list = compute_veclist(&n, c, ND, GLU_FALSE);
+  if (list == NULL) return 0;
+  for (size_t i = 0; i < n && i < cap; i++) {
+    for (int mu = 0; mu < ND; mu++) mom[i * ND + mu] = list[i].MOM[mu];
+    idx[i] = list[i].idx;
+  }
+  free(list);
+  return (long)n;
+}
+
+/* GLU's output file name for these cuts (src/Cuts/cut_output.c:121) */
+int ref_cut_output_name(int dir, int type, size_t max_mom, int definition,
+                        size_t angle, double cyl_width, size_t flow,
+                        char *out, size_t cap) {
+  struct cut_info c = cut_info_of(dir, type, max_mom, definition, angle,
+                                  cyl_width);
+  Latt.flow = flow;
+  char *s = output_str_struct(c);
+  snprintf(out, cap, "%s", s);
+  free(s);
+  return 0;
+}
+
+/* the whole measurement: writes GLU's output file into directory `where`
+ * (GLU's default build writes to "./"); the lattice is left holding the
+ * Fourier-transformed Lie fields, as in GLU */
+int ref_cuts(int dir, int type, size_t max_mom, int definition, size_t angle,
+             double cyl_width, size_t flow, const char *where) {
+  struct cut_info c = cut_info_of(dir, type, max_mom, definition, angle,
+                                  cyl_width);
+  Latt.flow = flow;
+  char cwd[4096];
+  if (getcwd(cwd, sizeof cwd) == NULL || chdir(where) != 0) return -1;
+  const int rc = cuts_struct(g_lat, c);
+  if (chdir(cwd) != 0) return -1;
+  return rc == GLU_SUCCESS ? 0 : -1;
 }

@@ -14,6 +14,8 @@ lat400.npz   4^3x8 configuration shipped with the reference (CONF/lat..400),
              read by GLU's own NERSC reader, plus reference results:
                Landau FACG / FASD (line-search SD) / FASD (GLU_GFIX_SD build,
                fixed step), Coulomb FACG / FASD (GLU_GFIX_SD build)
+cuts/        GLU's momentum-space output files (G2F2 / MOMgg / MATS) of the
+             Landau-fixed lat400 links, with cases.json
 hb8.npz      8^4 SU(3) configuration from GLU's heatbath (beta 6.0, cold
              start, seed 1, 500 sweeps of KP heatbath + 4 over-relaxation,
              8 OpenMP threads), plus reference Landau FACG (alpha 0.08,
@@ -206,7 +208,45 @@ def ildg_fixture() -> None:
     print("lat400.ildg written by GLU,", path.stat().st_size, "bytes")
 
 
+# momentum-space cuts of the Landau-fixed 4^3x8 links written by GLU's
+# cuts_struct: (CUTTYPE, MOM_CUT, MAXMOM, ANGLE, CYL_WIDTH)
+CUT_CASES = [("GLUON_PROPS", "SPHERICAL_CUT", 6, 0, 1.0),
+             ("GLUON_PROPS", "HYPERCUBIC_CUT", 2, 0, 1.0),
+             ("GLUON_PROPS", "CYLINDER_CUT", 8, 0, 0.75),
+             ("GLUON_PROPS", "CONICAL_CUT", 8, 40, 1.0),
+             ("EXCEPTIONAL", "SPHERICAL_CUT", 6, 0, 1.0),
+             ("FIELDS", "SPHERICAL_CUT", 2, 0, 1.0)]
+CUT_DIRS = {"EXCEPTIONAL": 0, "FIELDS": 2, "GLUON_PROPS": 6}
+CUT_TYPES = {"HYPERCUBIC_CUT": 0, "SPHERICAL_CUT": 1, "CYLINDER_CUT": 2,
+             "CONICAL_CUT": 3}
+
+
+def cuts_fixture() -> None:
+    """tests/golden/cuts/: GLU's output files of its momentum-space
+    measurements (src/Cuts/cuts.c) on lat400.npz["landau_facg_links"],
+    configuration number 400, and cases.json naming their parameters."""
+    import json
+    g = dict(np.load(OUT / "lat400.npz"))
+    dims = tuple(int(d) for d in g["dims"])
+    out = OUT / "cuts"
+    out.mkdir(exist_ok=True)
+    R = Reference()
+    cases = []
+    for ct, mc, mm, ang, w in CUT_CASES:
+        R.setup(dims, 1, 0.08)
+        R.put_links(g["landau_facg_links"])
+        path = R.cuts(out, CUT_DIRS[ct], CUT_TYPES[mc], mm, 0, ang, w, flow=400)
+        cases.append(dict(file=path.name, cuttype=ct, mom_cut=mc, maxmom=mm,
+                          angle=ang, cyl_width=w, flow=400,
+                          links="landau_facg_links"))
+        print(path.name, path.stat().st_size, "bytes")
+    (out / "cases.json").write_text(json.dumps(cases, indent=1) + "\n")
+
+
 def main() -> None:
+    if "--cuts" in sys.argv:
+        cuts_fixture()
+        return
     if "--ildg" in sys.argv:
         ildg_fixture()
         return
@@ -238,6 +278,7 @@ def main() -> None:
     add_diagnostics()
     nersc_fixture()
     ildg_fixture()
+    cuts_fixture()
 
     # ---- 8^4 heatbath configuration -------------------------------------
     with tempfile.TemporaryDirectory() as td:
