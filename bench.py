@@ -55,10 +55,12 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--workload", default="landau",
-                    choices=["landau", "coulomb", "ensemble"],
+                    choices=["landau", "coulomb", "ensemble", "gluonprop"],
                     help="landau: 32^3x64 Landau FACG (the headline); coulomb: "
                          "64^3x128 Coulomb FACG, all slices batched; ensemble: "
-                         "48 x 16^3x32 + 16 x 24^3x48 Landau FASD in one batch")
+                         "48 x 16^3x32 + 16 x 24^3x48 Landau FASD in one batch; "
+                         "gluonprop: 32^3x64 momentum-space gluon propagators "
+                         "(GLU's cuts_struct, GLUON_PROPS)")
     ap.add_argument("--dims", default=None,
                     help="lattice extents; default 32,32,32,64 (landau) or "
                          "64,64,64,128 (coulomb)")
@@ -1024,10 +1026,215 @@ def ensemble_iters_record():
     return None
 
 
+# ---------------------------------------------------------------------
+# gluon propagators: GLU's cuts_struct (CUTTYPE = GLUON_PROPS) with the cut
+# of GLU's shipped input file (CONF/input_file: CYLINDER_CUT, MAXMOM 4,
+# CYL_WIDTH 2.0, ANGLE 60, FIELD_DEFINITION LINEAR)
+
+G_CUT = dict(cuttype="GLUON_PROPS", mom_cut="CYLINDER_CUT", field_definition="LINEAR",
+             maxmom=4, angle=60, cyl_width=2.0)
+G_UNIT = "measurements/hour"
+
+
+def g_metric_name(dims) -> str:
+    return ("gluon propagator measurements/hour (%dx%dx%dx%d Landau-fixed, "
+            "GLUON_PROPS CYLINDER_CUT MAXMOM 4)" % tuple(dims))
+
+
+def g_workload(dims) -> dict:
+    return {"workload": "gluon propagators %s (cuts_struct GLUON_PROPS)" % "x".join(map(str, dims)),
+            "cut": "CYLINDER_CUT MAXMOM 4 CYL_WIDTH 2.0 ANGLE 60, LINEAR fields"}
+
+
+def g_reference_time(U, dims, nthreads):
+    """seconds of one GLU cuts_struct on the host cores (oracle/_ref)."""
+    import tempfile
+    from oracle import oracle as O
+    R = O.Reference()
+    R.setup(dims, nthreads)
+    R.put_links(U)
+    with tempfile.TemporaryDirectory() as td:
+        t0 = time.perf_counter()
+        R.cuts(td, 6, 2, 4, 0, 60, 2.0, flow=1)
+        return time.perf_counter() - t0
+
+
+def g_input(dims, rank):
+    """the synthetic stand-in, Landau-fixed to theta < 1e-14 on the GPU
+    (outside any timed region)."""
+    from glu_b200 import gfix
+    from glu_b200.workload import tiled_config
+    U = tiled_config(dims, seed=2 + rank)
+    return gfix.landau_fix(U, dims, accuracy=ACC, precision="MIXED").links
+
+
+def gluonprop_main(args, dims, rank, world, local):
+    import ctypes as C
+    import torch
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        from glu_b200.workload import tiled_config
+        U = tiled_config(dims, seed=2)  # the measurement's cost is gauge-independent
+        cores = os.cpu_count() or 1
+        secs = [g_reference_time(U, dims, cores) for _ in range(max(1, min(args.steps, 2)))]
+        t = statistics.median(secs)
+        value = 3600.0 / t
+        emit({"metric": g_metric_name(dims), "value": value, "unit": G_UNIT,
+              "n_gpus": world, "steps": len(secs), "warmup": 0, "ms_per_step": t * 1e3,
+              "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+              "dtype": "f64", "data": "synthetic (8^4 GLU heatbath tiled + random gauge)",
+              "config": dict(g_workload(dims), parallelism="host OpenMP"),
+              "impl": "reference",
+              "cpu_baseline": {"value": value, "unit": G_UNIT, "cores": cores,
+                               "kind": "reference",
+                               "sample": "%d full GLU cuts_struct runs (FFT: the oracle's FFTW stand-in)" % len(secs)},
+              "e2e": {"value": value, "unit": G_UNIT, "h2d_bytes_per_step": 0,
+                      "d2h_bytes_per_step": 0}})
+        return
+    torch.cuda.set_device(local)
+    from glu_b200 import _lib, cuts
+    from glu_b200._lib import check
+    lib = _lib.load()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    if args.profile_only:
+        # a short, bounded launch list for ncu: two measurements, no fix
+        from glu_b200.workload import tiled_config
+        U = tiled_config(dims, seed=2)
+        d = torch.from_numpy(U.view(np.float64).reshape(-1).copy()).cuda()
+        info = cuts.CutInfo(**G_CUT)
+        for _ in range(2):
+            r = cuts.measure_device(d, dims, info)
+        torch.cuda.synchronize()
+        print(json.dumps({"workload": "gluonprop profile-only", "momenta": len(r["mom"]),
+                          "pspace_err": r["pspace_err"]}))
+        return
+    U = g_input(dims, rank)
+    d_links = torch.from_numpy(U.view(np.float64).reshape(-1).copy()).cuda()
+    h_links = torch.from_numpy(U.view(np.float64).reshape(-1).copy()).pin_memory()
+    info = cuts.CutInfo(**G_CUT)
+    ci = info.c()
+    nmom = len(cuts.veclist(dims, info))
+    cd = (C.c_size_t * 4)(*dims)
+    o0, o1, perr = np.zeros(nmom), np.zeros(nmom), C.c_double(0.0)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    V = int(np.prod(dims))
+    # L2 flush between timed steps: the transforms' inputs (1.2 GB of links
+    # at 32^3x64) exceed the 126 MB L2 anyway; a 256 MB write makes it so
+    # for every shape
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def run(mode):
+        ms = 0.0
+        l0 = 0
+        for k in range(args.warmup + args.steps):
+            if k == args.warmup:
+                l0 = lib.gfix_kernel_launches()
+            flush.zero_()
+            barrier()
+            a, e = ev(), ev()
+            a.record()
+            if mode == "device":
+                rc = lib.gfix_cuts_measure_device(d_links.data_ptr(), cd, C.byref(ci), nmom,
+                                                  o0.ctypes.data_as(_lib._dp),
+                                                  o1.ctypes.data_as(_lib._dp), C.byref(perr))
+            else:
+                rc = lib.gfix_cuts_measure(h_links.data_ptr(), cd, C.byref(ci), nmom,
+                                           o0.ctypes.data_as(_lib._dp),
+                                           o1.ctypes.data_as(_lib._dp), C.byref(perr))
+            e.record()
+            if rc != 0:
+                raise RuntimeError(lib.gfix_cuts_error().decode())
+            barrier()
+            if k >= args.warmup:
+                ms += a.elapsed_time(e)
+        return max_over_ranks(ms), lib.gfix_kernel_launches() - l0
+
+    with Clocks(local) as clk:
+        ms_dev, launches = run("device")
+        ms_host, _ = run("host")
+        kms = (C.c_float * 3)()
+        if lib.gfix_profile_cuts(d_links.data_ptr(), cd, C.byref(ci), 10, kms) != 0:
+            raise RuntimeError(lib.gfix_cuts_error().decode())
+        # the same with FIELD_DEFINITION = LOGARITHMIC (eigenvalues and the
+        # exact logarithm of every link inside the xy pass)
+        lms = (C.c_float * 3)()
+        ci_log = cuts.CutInfo(**dict(G_CUT, field_definition="LOGARITHMIC")).c()
+        if lib.gfix_profile_cuts(d_links.data_ptr(), cd, C.byref(ci_log), 10, lms) != 0:
+            raise RuntimeError(lib.gfix_cuts_error().decode())
+    steps = args.steps
+    hbm, peak_src = peaks()
+    # algorithmic bytes per launch: xy pass reads the links (4 x 9 complex
+    # FP64 per site) and writes 16 complex fields; zt pass reads and writes
+    # the 16 fields
+    xy_bytes = V * (4 * 9 * 16 + 16 * 16)
+    zt_bytes = V * (2 * 16 * 16)
+    xy_ms, zt_ms, rest_ms = (float(x) for x in kms)
+    dom = ("k_cut_xy", xy_bytes, xy_ms) if xy_ms >= zt_ms else ("k_cut_zt", zt_bytes, zt_ms)
+    achieved = dom[1] / (dom[2] * 1e-3) / 1e9
+    traffic = traffic_from_profiles(dom[0], "fp64", dims)
+    line = {
+        "metric": g_metric_name(dims), "value": world * steps * 3600e3 / ms_dev,
+        "unit": G_UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": ms_dev / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled + seeded random gauge, "
+                "Landau-fixed to theta<1e-14 before timing)",
+        "config": dict(g_workload(dims), momenta=nmom,
+                       l2="256 MB flush between steps; %.2f GB of links" % (V * 576 / 1e9),
+                       kernel_ms={"xy (Lie fields + x,y transforms)": xy_ms,
+                                  "zt (z,t transforms)": zt_ms,
+                                  "gather + contraction": rest_ms},
+                       log_kernel_ms={"xy (logarithms + x,y transforms)": float(lms[0]),
+                                      "zt": float(lms[1]), "gather + contraction": float(lms[2])},
+                       parallelism="one configuration per GPU" if world > 1 else "single GPU"),
+        "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                     "peak_source": peak_src,
+                     "other": {"k_cut_zt" if dom[0] == "k_cut_xy" else "k_cut_xy":
+                               ((zt_bytes / zt_ms if dom[0] == "k_cut_xy" else xy_bytes / xy_ms)
+                                / 1e6 / hbm)}},
+        "e2e": {"value": world * steps * 3600e3 / ms_host, "unit": G_UNIT,
+                "h2d_bytes_per_step": V * 576, "d2h_bytes_per_step": 2 * nmom * 8},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            t = g_reference_time(U, dims, os.cpu_count() or 1)
+            line["cpu_baseline"] = {"value": 3600.0 / t, "unit": G_UNIT,
+                                    "cores": os.cpu_count() or 1, "kind": "reference",
+                                    "sample": "one full GLU cuts_struct (%.1f s; FFT: the oracle's FFTW stand-in)" % t}
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": G_UNIT, "kind": "unavailable",
+                                    "sample": str(e)}
+    if rank == 0:
+        emit(line)
+
+
 def main():
     args = parse()
     if args.dims is None:
-        args.dims = "32,32,32,64" if args.workload == "landau" else "64,64,64,128"
+        args.dims = ("32,32,32,64" if args.workload in ("landau", "gluonprop")
+                     else "64,64,64,128")
     dims = tuple(int(x) for x in args.dims.split(","))
     rank, world, local = dist_env()
     if args.workload == "coulomb":
@@ -1035,6 +1242,9 @@ def main():
         return
     if args.workload == "ensemble":
         ensemble_main(args, rank, world, local)
+        return
+    if args.workload == "gluonprop":
+        gluonprop_main(args, dims, rank, world, local)
         return
     if args.profile_only:
         profile_only(args, dims)

@@ -4,13 +4,17 @@
 // default build (SIN_MOM, backward transform, matrix contraction).
 //
 // Pipeline (FP64 throughout):
-//   k_cut_xy      Lie field of every link (Hermitian_proj, exactQ.c:358-385)
-//                 packed per direction in 4 complex fields -- (A00 + i A11,
-//                 A01, A02, A12), the traceless Hermitian matrix's 8 reals --
-//                 then the x and y transforms of one xy plane per block.
-//                 The block computes its field straight from the links:
-//                 each of the 4 components reads its own subset of the 9
-//                 link elements, so the links are read once.
+//   k_cut_xy4_ct  Lie field of every link -- FIELD_DEFINITION LINEAR
+//                 (Hermitian_proj, exactQ.c:358-385) or LOGARITHMIC
+//                 (exact_log_slow, exactQ.c:157-240) -- packed per direction
+//                 in 4 complex fields (A00 + i A11, A01, A02, A12: the
+//                 traceless Hermitian matrix's 8 reals), then the x and y
+//                 transforms of the four fields of one direction of one xy
+//                 plane per block.  The links are read once, straight into
+//                 the transform.
+//   k_cut_xy      the same per field (planes too large for four tiles, and
+//                 the generic extents); with the logarithm, k_cut_log_pack
+//                 writes the packed fields first
 //   k_cut_zt      z and t transforms of tiles of x columns
 //                 (both also as k_cut_*_ct with compile-time extents)
 //   k_cut_gather  per listed momentum: A_mu(p) for all 9 colour entries
@@ -44,6 +48,7 @@
 #include "fft.cuh"
 
 namespace gfix {
+void count_launches(unsigned long long n);  // gfix.cu
 namespace cuts {
 
 thread_local std::string t_err;
@@ -93,6 +98,109 @@ __device__ __forceinline__ C2 lin_component(const C2 *u, int k) {
   if (k == 1) return off_diag(u[1], u[3]);
   if (k == 2) return off_diag(u[2], u[6]);
   return off_diag(u[5], u[7]);
+}
+
+// ---- the logarithmic definition (exact_log_slow, src/Matrix_Ops/exactQ.c:
+// 157-240): eigenvalues of the link from its characteristic cubic
+// (Eigenvalues_suNC, src/Matrix_Ops/evalues.c:317-349, and the
+// near-identity form Eigenvalues_su3_stab, evalues.c:185-202), their
+// phases, and Q = log(U)/i from the su(3) f-constants
+// (f_hermitian_log_suNC, src/Matrix_Ops/effs.c:63-95).
+
+__device__ __forceinline__ C2 cadd2(C2 a, C2 b) { return mk<double>(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ C2 csub2(C2 a, C2 b) { return mk<double>(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ C2 cscal(C2 a, double s) { return mk<double>(a.x * s, a.y * s); }
+__device__ __forceinline__ C2 cconj(C2 a) { return mk<double>(a.x, -a.y); }
+__device__ __forceinline__ C2 cdiv(C2 a, C2 b) {
+  const double d = b.x * b.x + b.y * b.y;
+  return mk<double>((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+
+// GLU's squarert keeps the real part of the root only (its result is a
+// double); for an SU(3) link the argument -- minus the cubic's
+// discriminant over 108 -- is real and non-negative, so this is the root
+__device__ __forceinline__ double sq_root(C2 z, C2 R) {
+  const double t = sqrt(hypot(z.x, z.y)) * cos(atan2(z.y, z.x) * 0.5);
+  return (R.x * t < 0) ? -t : t;
+}
+
+__device__ __forceinline__ C2 cube_root(C2 z) {
+  const double r = cbrt(hypot(z.x, z.y));
+  const double a = atan2(z.y, z.x) / 3.;
+  return mk<double>(r * cos(a), r * sin(a));
+}
+
+__device__ void su3_eigenvalues(const C2 *U, C2 z[3]) {
+  const C2 rr3 = mk<double>(0., 1.7320508075688772);  // i sqrt(3)
+  const C2 tr = cadd2(cadd2(U[0], U[4]), U[8]);
+  if (1.0 - (U[0].x + U[4].x + U[8].x) / 3. < 1E-12) {
+    // eigenvalues of 1 - U near the identity
+    const C2 a = mk<double>(1.0 - tr.x / 3., -(tr.y / 3.));
+    const C2 b = mk<double>(-a.x, a.y);
+    const C2 p = cadd2(b, cm(a, mk<double>(2.0 - a.x, -a.y)));
+    const C2 t1 = mk<double>(1.0 - a.x / 3., -(a.y / 3.));
+    const C2 inner = csub2(csub2(mk<double>(1.0, 0.0), b), cm(cscal(a, 2.0), t1));
+    const C2 q = cscal(cadd2(cm(a, inner), b), 1.5);
+    const double res = sq_root(cadd2(cm(q, q), cm(cm(p, p), p)), p);
+    const C2 u1 = cube_root(mk<double>(res - q.x, -q.y));
+    const C2 u2 = (u1.x != 0.0) ? cdiv(mk<double>(-p.x, -p.y), u1) : mk<double>(0., 0.);
+    const C2 plus = cadd2(u1, u2);
+    const C2 minus = cm(rr3, csub2(u1, u2));
+    z[0] = csub2(cadd2(mk<double>(1.0, 0.0), plus), a);
+    z[1] = csub2(cadd2(mk<double>(1.0, 0.0), cscal(csub2(minus, plus), 0.5)), a);
+    z[2] = csub2(z[1], minus);
+    return;
+  }
+  const C2 a = mk<double>(-tr.x / 3., -tr.y / 3.);
+  const C2 ca = cconj(a);
+  const C2 Q = cadd2(cm(a, a), ca);
+  const C2 R = csub2(cm(a, cadd2(Q, cscal(ca, 0.5))), mk<double>(0.5, 0.0));
+  const C2 temp = csub2(cm(R, R), cm(cm(Q, Q), Q));
+  const double res = sq_root(temp, R);
+  const C2 A = cscal(cube_root(mk<double>(R.x + res, R.y)), -1.0);
+  const C2 B = (A.x != 0.0 || A.y != 0.0) ? cdiv(Q, A) : mk<double>(0., 0.);
+  const C2 plus = cadd2(A, B);
+  const C2 minus = cm(rr3, csub2(A, B));
+  z[0] = csub2(plus, a);
+  z[1] = csub2(cscal(csub2(minus, plus), 0.5), a);
+  z[2] = csub2(z[1], minus);
+}
+
+// the four packed components of exact_log_slow(U); zero where GLU's
+// routine returns without writing (all three phases equal, i.e. U = 1)
+__device__ void log_components(const C2 *U, C2 out[4]) {
+  C2 ev[3];
+  su3_eigenvalues(U, ev);
+  const double z0 = atan2(ev[0].y, ev[0].x), z1 = atan2(ev[1].y, ev[1].x);
+  const double z2 = -(z0 - z1);
+  if (z0 == z1 && z1 == z2) {
+    for (int k = 0; k < 4; k++) out[k] = mk<double>(0., 0.);
+    return;
+  }
+  const double u = 0.5 * z0, w = z1 + u;
+  const double cw = cos(w), cu = cos(u), su = sin(u);
+  const C2 one1 = mk<double>(cu, -su);
+  const C2 two1 = cm(cconj(one1), cconj(one1));
+  const double uu = u * u, ww = w * w;
+  const double denom = 1.0 / (9. * uu - ww);
+  const double E0 = fabs(w) < 1E-13 ? 1 - ww / 6. * (1 - ww / 20. * (1 - ww / 42.)) : sin(w) / w;
+  C2 f0 = cadd2(cscal(two1, uu - ww),
+                cm(one1, mk<double>(8. * uu * cw, 2. * u * (3. * uu + ww) * E0)));
+  C2 f1 = csub2(cscal(two1, 2 * u), cm(one1, mk<double>(2. * u * cw, -((3. * uu - ww) * E0))));
+  C2 f2 = csub2(two1, cm(one1, mk<double>(cw, 3. * u * E0)));
+  f0 = cscal(f0, denom);
+  f1 = cscal(f1, denom);
+  f2 = cscal(f2, denom);
+  const C2 con = cconj(f2);
+  const double mod = 1.0 / (f1.y * f2.x - f1.x * f2.y);
+  const double imf = (f0.y * f2.x - f0.x * f2.y) * mod;
+  const C2 trce = mk<double>(0., -mod / 2.);
+  auto entry = [&](C2 uab, C2 uba) { return cm(trce, csub2(cm(con, uab), cm(f2, cconj(uba)))); };
+  const C2 q0 = entry(U[0], U[0]), q4 = entry(U[4], U[4]);
+  out[0] = mk<double>(q0.x - imf, q4.x - imf);
+  out[1] = entry(U[1], U[3]);
+  out[2] = entry(U[2], U[6]);
+  out[3] = entry(U[5], U[7]);
 }
 
 struct CutCtx {
@@ -283,28 +391,103 @@ __global__ void __launch_bounds__(ct_threads(B *LZ *LT), ct_minb(B *LZ *LT))
   }
 }
 
+// all four packed fields of one direction of one xy plane per block: each
+// thread reads whole 144-byte link records (the element pairs of a 32-byte
+// sector meet in L1), and the four tiles are transformed together
+template <int LX, int LY, bool LOG>
+__global__ void __launch_bounds__(ct_threads(4 * LX * LY), ct_minb(4 * LX * LY))
+    k_cut_xy4_ct(CutCtx c) {
+  constexpr int P = LX + 1, N = LX * LY, T = P * LY, BD = ct_threads(4 * N);
+  constexpr int SPT = (N + BD - 1) / BD;  // sites per thread
+  constexpr int EPT = (4 * N + BD - 1) / BD;
+  extern __shared__ unsigned char smem_raw[];
+  C2 *A = reinterpret_cast<C2 *>(smem_raw);
+  C2 *twx = A + 4 * T;
+  C2 *twy = twx + LX;
+  for (int k = threadIdx.x; k < LX; k += BD) twx[k] = c.tw[c.ax[0].tw_off + k];
+  for (int k = threadIdx.x; k < LY; k += BD) twy[k] = c.tw[c.ax[1].tw_off + k];
+  const int mu = blockIdx.x, plane = blockIdx.y;
+  const size_t base = (size_t)plane * N;
+#pragma unroll
+  for (int k = 0; k < SPT; k++) {
+    const int e = threadIdx.x + k * BD;
+    if (N % BD == 0 || e < N) {
+      const C2 *u = c.links + ((base + e) * 4 + mu) * 9;
+      C2 r[9];
+#pragma unroll
+      for (int j = 0; j < 9; j++) r[j] = u[j];
+      const int o = (e / LX) * P + e % LX;
+      if constexpr (LOG) {
+        C2 q4[4];
+        log_components(r, q4);
+#pragma unroll
+        for (int q = 0; q < 4; q++) A[q * T + o] = q4[q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; q++) A[q * T + o] = lin_component(r, q);
+      }
+    }
+  }
+  __syncthreads();
+  ct_stages<double, LX, 1, 4 * LY, 1, 0, P, 1, BD>(A, twx, true);       // rows
+  ct_stages<double, LY, 1, 4 * LX, LX, 1, T, P, BD>(A, twy, true);      // columns
+#pragma unroll
+  for (int k = 0; k < EPT; k++) {
+    const int e = threadIdx.x + k * BD;
+    if ((4 * N) % BD == 0 || e < 4 * N) {
+      const int q = e / N, r = e % N;
+      c.F[(size_t)(mu * 4 + q) * c.V + base + r] = A[q * T + (r / LX) * P + r % LX];
+    }
+  }
+}
+
+// the logarithmic Lie fields packed into F, one thread per site and
+// direction (for the per-field xy passes)
+__global__ void __launch_bounds__(128) k_cut_log_pack(CutCtx c) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)c.V * 4) return;
+  const size_t site = t >> 2;
+  const int mu = (int)(t & 3);
+  C2 r[9];
+  const C2 *u = c.links + t * 9;
+#pragma unroll
+  for (int j = 0; j < 9; j++) r[j] = u[j];
+  C2 q4[4];
+  log_components(r, q4);
+#pragma unroll
+  for (int q = 0; q < 4; q++) c.F[(size_t)(mu * 4 + q) * c.V + site] = q4[q];
+}
+
 using CutFn = void (*)(CutCtx);
 
-static CutFn xy_ct(int lx, int ly) {
+static CutFn xy4_ct(int lx, int ly, bool log) {
+#define GFIX_CXY4(n) \
+  if (lx == n && ly == n) return log ? k_cut_xy4_ct<n, n, true> : k_cut_xy4_ct<n, n, false>;
+  GFIX_CXY4(8) GFIX_CXY4(16) GFIX_CXY4(24) GFIX_CXY4(32) GFIX_CXY4(48)
+#undef GFIX_CXY4
+  return nullptr;
+}
+
+static CutFn xy_ct(int lx, int ly, bool links) {
 #define GFIX_CXY(n) \
-  if (lx == n && ly == n) return k_cut_xy_ct<n, n, true>;
+  if (lx == n && ly == n) return links ? k_cut_xy_ct<n, n, true> : k_cut_xy_ct<n, n, false>;
   GFIX_CXY(8) GFIX_CXY(16) GFIX_CXY(24) GFIX_CXY(32) GFIX_CXY(48) GFIX_CXY(64)
 #undef GFIX_CXY
   return nullptr;
 }
 
-// (Lz, Lt) -> the tile width it is compiled for
-static CutFn zt_ct(int lz, int lt, int lx, int *b) {
-#define GFIX_CZT(z, t, bb)                   \
-  if (lz == z && lt == t && lx % bb == 0) { \
-    *b = bb;                                 \
-    return k_cut_zt_ct<z, t, bb>;            \
-  }
+// compiled zt passes of (Lz, Lt): (tile width, kernel) candidates; the
+// width only regroups pencils, so every candidate gives the same bits
+static std::vector<std::pair<int, CutFn>> zt_ct(int lz, int lt, int lx) {
+  std::vector<std::pair<int, CutFn>> v;
+#define GFIX_CZT(z, t, bb) \
+  if (lz == z && lt == t && lx % bb == 0) v.push_back({bb, k_cut_zt_ct<z, t, bb>});
   GFIX_CZT(8, 8, 8) GFIX_CZT(8, 16, 4) GFIX_CZT(16, 16, 4) GFIX_CZT(16, 32, 2)
-  GFIX_CZT(24, 48, 2) GFIX_CZT(32, 32, 2) GFIX_CZT(32, 64, 2) GFIX_CZT(48, 96, 1)
-  GFIX_CZT(64, 128, 1)
+  GFIX_CZT(16, 32, 4) GFIX_CZT(24, 48, 1) GFIX_CZT(24, 48, 2) GFIX_CZT(32, 32, 2)
+  GFIX_CZT(32, 32, 4) GFIX_CZT(32, 64, 1) GFIX_CZT(32, 64, 2) GFIX_CZT(32, 64, 4)
+  GFIX_CZT(48, 96, 1) GFIX_CZT(48, 96, 2) GFIX_CZT(64, 128, 1)
 #undef GFIX_CZT
-  return nullptr;
+  return v;
 }
 
 // per listed momentum i: G[i][mu][9] = A_mu(p) e^{i p_mu / 2} and the
@@ -615,7 +798,9 @@ struct Work {
   int pt_xy = 8, pt_zt = 8, bd_xy = 128, bd_zt = 128;
   size_t sm_xy = 0, sm_zt = 0;
   bool odd = false;
-  CutFn xy_fn = nullptr, zt_fn = nullptr;  // compile-time passes, if any
+  // compile-time passes, if any: xy_fn[definition] (LINEAR, LOG)
+  CutFn xy_fn[2] = {nullptr, nullptr}, zt_fn = nullptr;
+  bool xy4 = false;  // xy_fn are k_cut_xy4_ct (the Lie fields computed inside)
   std::map<CutKey, MomList> lists;
   const MomList *cur = nullptr;  // list on the device
 
@@ -666,19 +851,22 @@ struct Work {
     pt_zt = (b * nzt <= 4096 && !odd) ? 8 : 16;
     bd_zt = (int)threads(b * nzt, pt_zt);
     sm_zt = ((size_t)(L[2] * b + 1) * L[3] + L[2] + L[3]) * sizeof(C2);
+    CCK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     // compile-time passes where the extents have them
     if (!odd) {
-      xy_fn = xy_ct(L[0], L[1]);
-      if (xy_fn) bd_xy = ct_threads(L[0] * L[1]);
-      int bc = 0;
-      zt_fn = zt_ct(L[2], L[3], L[0], &bc);
-      if (zt_fn) {
-        c.zt_b = bc;
-        bd_zt = ct_threads(bc * L[2] * L[3]);
-        sm_zt = ((size_t)(L[2] * bc + zt_pad(bc)) * L[3] + L[2] + L[3]) * sizeof(C2);
+      const size_t sm4 = (4 * (size_t)(L[0] + 1) * L[1] + L[0] + L[1]) * sizeof(C2);
+      if (xy4_ct(L[0], L[1], false) && sm4 <= 200u * 1024u) {
+        xy4 = true;
+        xy_fn[0] = xy4_ct(L[0], L[1], false);
+        xy_fn[1] = xy4_ct(L[0], L[1], true);
+        bd_xy = ct_threads(4 * L[0] * L[1]);
+        sm_xy = sm4;
+      } else if (xy_ct(L[0], L[1], true)) {
+        xy_fn[0] = xy_ct(L[0], L[1], true);
+        xy_fn[1] = xy_ct(L[0], L[1], false);  // on the packed logarithms
+        bd_xy = ct_threads(L[0] * L[1]);
       }
     }
-    CCK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     std::vector<C2> tw;
     for (int a = 0; a < 4; a++) {
       c.ax[a].tw_off = (int)tw.size();
@@ -694,7 +882,47 @@ struct Work {
     c.V = V;
     c.tw = d_tw;
     c.F = d_F;
-    return set_attrs();
+    if (set_attrs()) return -1;
+    return odd ? 0 : pick_zt();
+  }
+
+  // the fastest compiled zt pass for this shape (timed once on zeroed
+  // fields; all candidates give identical results)
+  int pick_zt() {
+    const auto cands = zt_ct(L[2], L[3], L[0]);
+    if (cands.empty()) return 0;
+    CCK(cudaMemsetAsync(d_F, 0, (size_t)kNF * V * sizeof(C2), s));
+    cudaEvent_t a, b;
+    CCK(cudaEventCreate(&a));
+    CCK(cudaEventCreate(&b));
+    float best = 1e30f;
+    for (const auto &cd : cands) {
+      const int bw = cd.first;
+      const size_t sm = ((size_t)(L[2] * bw + zt_pad(bw)) * L[3] + L[2] + L[3]) * sizeof(C2);
+      if (sm > 200u * 1024u || attr(cd.second, sm)) continue;
+      CutCtx cc = c;
+      cc.zt_b = bw;
+      const int bd = ct_threads(bw * L[2] * L[3]);
+      const dim3 g((L[0] / bw) * L[1], kNF);
+      cd.second<<<g, bd, sm, s>>>(cc);
+      CCK(cudaEventRecord(a, s));
+      for (int r = 0; r < 3; r++) cd.second<<<g, bd, sm, s>>>(cc);
+      CCK(cudaEventRecord(b, s));
+      CCK(cudaEventSynchronize(b));
+      float ms = 0.f;
+      CCK(cudaEventElapsedTime(&ms, a, b));
+      if (ms < best) {
+        best = ms;
+        zt_fn = cd.second;
+        c.zt_b = bw;
+        bd_zt = bd;
+        sm_zt = sm;
+      }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CCK(cudaGetLastError());
+    return 0;
   }
 
   template <typename K>
@@ -709,8 +937,8 @@ struct Work {
         attr(k_cut_zt<8, false>, sm_zt) || attr(k_cut_zt<16, false>, sm_zt) ||
         attr(k_cut_zt<16, true>, sm_zt))
       return -1;
-    if (xy_fn && attr(xy_fn, sm_xy)) return -1;
-    if (zt_fn && attr(zt_fn, sm_zt)) return -1;
+    for (CutFn f : xy_fn)
+      if (f && attr(f, sm_xy)) return -1;
     return 0;
   }
 
@@ -770,18 +998,26 @@ struct Work {
     return 0;
   }
 
-  // the transforms of the linear Lie fields of c.links into d_F; `mid`
-  // (may be null) is recorded between the xy and the zt pass
-  void transform(cudaEvent_t mid = nullptr) {
-    const dim3 gxy(kNF, L[2] * L[3]);
-    if (xy_fn)
-      xy_fn<<<gxy, bd_xy, sm_xy, s>>>(c);
+  // the transforms of the Lie fields (definition def) of c.links into
+  // d_F; `mid` (may be null) is recorded between the xy and the zt pass
+  void transform(int def, cudaEvent_t mid = nullptr) {
+    const bool log = def == GFIX_FIELD_LOG;
+    const dim3 gxy(xy4 ? 4 : kNF, L[2] * L[3]);
+    if (log && !xy4) {
+      k_cut_log_pack<<<(unsigned)(((size_t)V * 4 + 127) / 128), 128, 0, s>>>(c);
+      count_launches(1);
+    }
+    if (xy_fn[log])
+      xy_fn[log]<<<gxy, bd_xy, sm_xy, s>>>(c);
     else if (odd)
-      k_cut_xy<16, true, true><<<gxy, bd_xy, sm_xy, s>>>(c);
+      log ? k_cut_xy<16, true, false><<<gxy, bd_xy, sm_xy, s>>>(c)
+          : k_cut_xy<16, true, true><<<gxy, bd_xy, sm_xy, s>>>(c);
     else if (pt_xy == 8)
-      k_cut_xy<8, false, true><<<gxy, bd_xy, sm_xy, s>>>(c);
+      log ? k_cut_xy<8, false, false><<<gxy, bd_xy, sm_xy, s>>>(c)
+          : k_cut_xy<8, false, true><<<gxy, bd_xy, sm_xy, s>>>(c);
     else
-      k_cut_xy<16, false, true><<<gxy, bd_xy, sm_xy, s>>>(c);
+      log ? k_cut_xy<16, false, false><<<gxy, bd_xy, sm_xy, s>>>(c)
+          : k_cut_xy<16, false, true><<<gxy, bd_xy, sm_xy, s>>>(c);
     if (mid) cudaEventRecord(mid, s);
     const dim3 gzt((L[0] / c.zt_b) * L[1], kNF);
     if (zt_fn)
@@ -792,6 +1028,7 @@ struct Work {
       k_cut_zt<8, false><<<gzt, bd_zt, sm_zt, s>>>(c);
     else
       k_cut_zt<16, false><<<gzt, bd_zt, sm_zt, s>>>(c);
+    count_launches(2);
   }
 
   Norms norms() const {
@@ -810,6 +1047,7 @@ struct Work {
       k_cut_props<<<nb, 128, 0, s>>>(d_G, n >> 1, d_pmu, d_psq, norms(), d_o0, d_o1);
     else if (dir == GFIX_CUT_EXCEPTIONAL)
       k_cut_momgg<<<nb, 128, 0, s>>>(d_G, n, d_pmu, d_psq, norms(), d_o0, d_o1);
+    count_launches(dir == GFIX_CUT_FIELDS ? 1 : 2);
   }
 
   // results to the host, as GLU fills them
@@ -861,8 +1099,8 @@ static int check_info(const size_t *dims, const gfix_cut_info *ci) {
     return cfail("cut mode %d not supported (GLUON_PROPS, EXCEPTIONAL, FIELDS)", ci->dir);
   if (ci->type < GFIX_CUT_HYPERCUBIC || ci->type > GFIX_CUT_CONICAL)
     return cfail("momentum cut type %d unknown", ci->type);
-  if (ci->definition != GFIX_FIELD_LINEAR)
-    return cfail("field definition %d not supported (LINEAR)", ci->definition);
+  if (ci->definition != GFIX_FIELD_LINEAR && ci->definition != GFIX_FIELD_LOG)
+    return cfail("field definition %d unknown", ci->definition);
   return 0;
 }
 
@@ -874,7 +1112,7 @@ static int run(Work *w, const gfix_cut_info *ci, size_t nmom, double *out0,
   if (nmom != ml->n())
     return cfail("%zu momenta given, the cut keeps %zu", nmom, ml->n());
   if (w->upload(ml)) return -1;
-  w->transform();
+  w->transform(ci->definition);
   w->measure(ci->dir);
   CCK(cudaGetLastError());
   return w->fetch(ci->dir, out0, out1, perr);
@@ -1027,7 +1265,7 @@ int gfix_profile_cuts(const double *d_links, const size_t dims[4], const gfix_cu
   float acc[3] = {0, 0, 0};
   for (int r = 0; r < reps + 1; r++) {
     CCK(cudaEventRecord(ev[0], w->s));
-    w->transform(ev[1]);
+    w->transform(ci->definition, ev[1]);
     CCK(cudaEventRecord(ev[2], w->s));
     w->measure(ci->dir);
     CCK(cudaEventRecord(ev[3], w->s));

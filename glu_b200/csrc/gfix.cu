@@ -52,6 +52,9 @@ static int fail(const char *fmt, ...) {
 
 #define LAUNCHED(n) g_launches.fetch_add((n), std::memory_order_relaxed)
 
+// kernels launched by the other translation units of the library
+void count_launches(unsigned long long n) { LAUNCHED(n); }
+
 constexpr size_t kSentinel = 123456789;
 
 // FFT plans: 0 = the default plan per shape (bit-reproducible runs), 1 =

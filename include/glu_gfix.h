@@ -307,7 +307,8 @@ typedef struct gfix_cut_info {
   int dir;          /* GFIX_CUT_GLUON_PROPS, _EXCEPTIONAL or _FIELDS */
   int type;         /* momentum cut, GFIX_CUT_HYPERCUBIC .. _CONICAL */
   size_t max_mom;   /* MAXMOM: largest (n_mu small/L_mu)^2 kept */
-  int definition;   /* GFIX_FIELD_LINEAR (Hermitian projection) */
+  int definition;   /* GFIX_FIELD_LINEAR (Hermitian projection) or
+                       GFIX_FIELD_LOG (exact logarithm) */
   size_t angle;     /* ANGLE of the conical cut, degrees */
   double cyl_width; /* CYL_WIDTH in units of 2 pi / min(L) */
 } gfix_cut_info;

@@ -5,7 +5,9 @@ it as the checker of the GPU path; the product package never imports it.
 Followed, in GLU's default build (SIN_MOM on, CUT_FORWARD off, CONDOR_MODE,
 matrix contraction for the three-gluon vertex):
 
-* lie fields       src/Matrix_Ops/exactQ.c:358-385 (Hermitian_proj, LINEAR)
+* lie fields       src/Matrix_Ops/exactQ.c:358-385 (Hermitian_proj, LINEAR),
+                   exactQ.c:157-240 with evalues.c:136-202, 317-349 and
+                   effs.c:63-95 (exact_log_slow, LOGARITHMIC)
 * Fourier step     src/Cuts/cuts.c:35-97 (backward, unnormalised transform
                    of each colour component: sum_x A(x) e^{+ipx})
 * momentum list    src/Cuts/cut_routines.c:60-81 (simorb_ratios), 84-104
@@ -49,12 +51,91 @@ def hermitian_proj(U: np.ndarray) -> np.ndarray:
     return Q
 
 
-def momentum_fields(links: np.ndarray, dims) -> np.ndarray:
+def _sq_root(z, R):
+    """GLU's squarert (evalues.c:136-143): the real part of the root only."""
+    t = np.sqrt(np.abs(z)) * np.cos(np.angle(z) * 0.5)
+    return np.where((np.conj(R) * t).real < 0, -t, t)
+
+
+def _cube_root(z):
+    return np.cbrt(np.abs(z)) * (np.cos(np.angle(z) / 3.0) + 1j * np.sin(np.angle(z) / 3.0))
+
+
+def su3_eigenvalues(U):
+    """Eigenvalues_suNC (evalues.c:317-349) with Eigenvalues_su3_stab
+    (evalues.c:185-202) near the identity, for U (..., 3, 3)."""
+    rr3 = 1j * 1.7320508075688772
+    tr = U[..., 0, 0] + U[..., 1, 1] + U[..., 2, 2]
+    # generic branch
+    a = -tr / 3.0
+    ca = np.conj(a)
+    Q = a * a + ca
+    R = a * (Q + ca * 0.5) - 0.5
+    res = _sq_root(R * R - Q * Q * Q, R)
+    A = -_cube_root(R + res)
+    with np.errstate(all="ignore"):
+        B = np.where(A != 0, Q / np.where(A != 0, A, 1), 0)
+    plus, minus = A + B, rr3 * (A - B)
+    z0, z1 = plus - a, (minus - plus) * 0.5 - a
+    # near-identity branch
+    a2 = 1.0 - tr / 3.0
+    b2 = -np.conj(a2)
+    p = b2 + a2 * (2.0 - a2)
+    q = (a2 * (1.0 - b2 - a2 * 2.0 * (1.0 - a2 / 3.0)) + b2) * 1.5
+    r2 = _sq_root(q * q + p * p * p, p)
+    u1 = _cube_root(r2 - q)
+    with np.errstate(all="ignore"):
+        u2 = np.where(u1.real != 0, -p / np.where(u1 != 0, u1, 1), 0)
+    plus2, minus2 = u1 + u2, rr3 * (u1 - u2)
+    s0, s1 = 1.0 + plus2 - a2, 1.0 + 0.5 * (minus2 - plus2) - a2
+    stab = 1.0 - tr.real / 3.0 < 1e-12
+    return np.where(stab, s0, z0), np.where(stab, s1, z1)
+
+
+def exact_log(U: np.ndarray) -> np.ndarray:
+    """Q with U = exp(iQ), Q traceless Hermitian (exact_log_slow,
+    exactQ.c:157-240, f-constants effs.c:63-95); zero where GLU's routine
+    returns without writing (all phases equal)."""
+    e0, e1 = su3_eigenvalues(U)
+    z0, z1 = np.angle(e0), np.angle(e1)
+    z2 = -(z0 - z1)
+    u = 0.5 * z0
+    w = z1 + u
+    cw, cu, su = np.cos(w), np.cos(u), np.sin(u)
+    one1 = cu - 1j * su
+    two1 = np.conj(one1) ** 2
+    uu, ww = u * u, w * w
+    with np.errstate(all="ignore"):
+        denom = 1.0 / (9.0 * uu - ww)
+        E0 = np.where(np.abs(w) < 1e-13, 1 - ww / 6.0 * (1 - ww / 20.0 * (1 - ww / 42.0)),
+                      np.sin(w) / np.where(w != 0, w, 1))
+        f0 = ((uu - ww) * two1 + one1 * (8.0 * uu * cw + 1j * 2.0 * u * (3.0 * uu + ww) * E0)) * denom
+        f1 = (2 * u * two1 - one1 * (2.0 * u * cw - 1j * (3.0 * uu - ww) * E0)) * denom
+        f2 = (two1 - one1 * (cw + 3.0 * 1j * u * E0)) * denom
+        con = np.conj(f2)
+        mod = 1.0 / (f1.imag * f2.real - f1.real * f2.imag)
+        imf = (f0.imag * f2.real - f0.real * f2.imag) * mod
+    trce = -1j * mod / 2.0
+    Qm = np.zeros_like(U)
+    for a, b in ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2)):
+        Qm[..., a, b] = trce * (con * U[..., a, b] - f2 * np.conj(U[..., b, a]))
+    Qm[..., 0, 0] -= imf
+    Qm[..., 1, 1] -= imf
+    for a, b in ((0, 1), (0, 2), (1, 2)):
+        Qm[..., b, a] = np.conj(Qm[..., a, b])
+    Qm[..., 2, 2] = -(Qm[..., 0, 0] + Qm[..., 1, 1])
+    same = (z0 == z1) & (z1 == z2)
+    Qm[same] = 0
+    return Qm
+
+
+def momentum_fields(links: np.ndarray, dims, definition=LINEAR_DEF) -> np.ndarray:
     """A_mu(p) = sum_x A_mu(x) e^{+ipx} for every p of the 0..2pi zone,
     (V, 4, 3, 3), site order x fastest."""
     Lx, Ly, Lz, Lt = (int(d) for d in dims)
     V = Lx * Ly * Lz * Lt
-    Q = hermitian_proj(np.asarray(links).reshape(V, 4, 3, 3))
+    U = np.asarray(links).reshape(V, 4, 3, 3)
+    Q = exact_log(U) if definition == LOG_DEF else hermitian_proj(U)
     A = Q.reshape(Lt, Lz, Ly, Lx, 4, 3, 3)
     A = np.fft.ifftn(A, axes=(0, 1, 2, 3)) * V
     return A.reshape(V, 4, 3, 3)
@@ -241,12 +322,12 @@ def exceptional(B, moms, dims):
 
 
 def measure(links, dims, dir=GLUON_PROPS, type=PSQ_CUT, max_mom=20, angle=0,
-            cyl_width=1.0):
+            cyl_width=1.0, definition=LINEAR_DEF):
     """dict(mom, out0, out1, pspace_err) as GLU's cuts_struct computes
     them; out0/out1 = transverse/longitudinal, g2/g3, or for FIELDS the
     corrected fields (n, 4, 3, 3) and None."""
     moms, idx = veclist(dims, dir, type, max_mom, angle, cyl_width)
-    A = momentum_fields(links, dims)
+    A = momentum_fields(links, dims, definition)
     B, err = correct_pspace(A, moms, idx, dims)
     if dir == GLUON_PROPS:
         o0, o1 = gluon_props(B, moms, dims)

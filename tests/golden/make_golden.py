@@ -209,13 +209,15 @@ def ildg_fixture() -> None:
 
 
 # momentum-space cuts of the Landau-fixed 4^3x8 links written by GLU's
-# cuts_struct: (CUTTYPE, MOM_CUT, MAXMOM, ANGLE, CYL_WIDTH)
-CUT_CASES = [("GLUON_PROPS", "SPHERICAL_CUT", 6, 0, 1.0),
-             ("GLUON_PROPS", "HYPERCUBIC_CUT", 2, 0, 1.0),
-             ("GLUON_PROPS", "CYLINDER_CUT", 8, 0, 0.75),
-             ("GLUON_PROPS", "CONICAL_CUT", 8, 40, 1.0),
-             ("EXCEPTIONAL", "SPHERICAL_CUT", 6, 0, 1.0),
-             ("FIELDS", "SPHERICAL_CUT", 2, 0, 1.0)]
+# cuts_struct: (CUTTYPE, MOM_CUT, MAXMOM, ANGLE, CYL_WIDTH, FIELD_DEFINITION)
+CUT_CASES = [("GLUON_PROPS", "SPHERICAL_CUT", 6, 0, 1.0, "LINEAR"),
+             ("GLUON_PROPS", "HYPERCUBIC_CUT", 2, 0, 1.0, "LINEAR"),
+             ("GLUON_PROPS", "CYLINDER_CUT", 8, 0, 0.75, "LINEAR"),
+             ("GLUON_PROPS", "CONICAL_CUT", 8, 40, 1.0, "LINEAR"),
+             ("EXCEPTIONAL", "SPHERICAL_CUT", 6, 0, 1.0, "LINEAR"),
+             ("FIELDS", "SPHERICAL_CUT", 2, 0, 1.0, "LINEAR"),
+             ("GLUON_PROPS", "SPHERICAL_CUT", 6, 0, 1.0, "LOGARITHMIC"),
+             ("EXCEPTIONAL", "CONICAL_CUT", 8, 40, 1.0, "LOGARITHMIC")]
 CUT_DIRS = {"EXCEPTIONAL": 0, "FIELDS": 2, "GLUON_PROPS": 6}
 CUT_TYPES = {"HYPERCUBIC_CUT": 0, "SPHERICAL_CUT": 1, "CYLINDER_CUT": 2,
              "CONICAL_CUT": 3}
@@ -232,12 +234,13 @@ def cuts_fixture() -> None:
     out.mkdir(exist_ok=True)
     R = Reference()
     cases = []
-    for ct, mc, mm, ang, w in CUT_CASES:
+    for ct, mc, mm, ang, w, fd in CUT_CASES:
         R.setup(dims, 1, 0.08)
         R.put_links(g["landau_facg_links"])
-        path = R.cuts(out, CUT_DIRS[ct], CUT_TYPES[mc], mm, 0, ang, w, flow=400)
+        path = R.cuts(out, CUT_DIRS[ct], CUT_TYPES[mc], mm,
+                      1 if fd == "LOGARITHMIC" else 0, ang, w, flow=400)
         cases.append(dict(file=path.name, cuttype=ct, mom_cut=mc, maxmom=mm,
-                          angle=ang, cyl_width=w, flow=400,
+                          angle=ang, cyl_width=w, field_definition=fd, flow=400,
                           links="landau_facg_links"))
         print(path.name, path.stat().st_size, "bytes")
     (out / "cases.json").write_text(json.dumps(cases, indent=1) + "\n")

@@ -22,7 +22,8 @@ OUT_KEYS = {"GLUON_PROPS": ("transverse", "longitudinal"),
 def _oracle(links, dims, case):
     return CO.measure(links, dims, cuts.CUTTYPES[case["cuttype"]],
                       cuts.MOM_CUTS[case["mom_cut"]], case["maxmom"],
-                      case["angle"], case["cyl_width"])
+                      case["angle"], case["cyl_width"],
+                      cuts.FIELD_DEFINITIONS[case.get("field_definition", "LINEAR")])
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c["file"] for c in CASES])
@@ -48,15 +49,17 @@ def _random_links(dims, seed):
 
 @pytest.mark.parametrize("dims", [(4, 4, 4, 8), (6, 6, 6, 12), (8, 8, 8, 8)])
 @pytest.mark.parametrize("cuttype", ["GLUON_PROPS", "EXCEPTIONAL", "FIELDS"])
-def test_oracle_matches_glu_runs(reference, dims, cuttype):
+@pytest.mark.parametrize("definition", ["LINEAR", "LOGARITHMIC"])
+def test_oracle_matches_glu_runs(reference, dims, cuttype, definition):
     U = _random_links(dims, 11)
     case = dict(cuttype=cuttype, mom_cut="CONICAL_CUT", maxmom=12, angle=45,
-                cyl_width=1.5)
+                cyl_width=1.5, field_definition=definition)
     reference.setup(dims)
     reference.put_links(U)
     import tempfile
     with tempfile.TemporaryDirectory() as td:
-        p = reference.cuts(td, cuts.CUTTYPES[cuttype], 3, 12, 0, 45, 1.5, flow=3)
+        p = reference.cuts(td, cuts.CUTTYPES[cuttype], 3, 12,
+                           cuts.FIELD_DEFINITIONS[definition], 45, 1.5, flow=3)
         ref = cuts.read_output(p, cuttype)
     o = _oracle(U, dims, case)
     assert np.array_equal(ref["mom"], o["mom"])
@@ -96,3 +99,32 @@ def test_library_veclist_of_the_fixture_cases(lat400):
 def test_unsupported_modes_raise():
     with pytest.raises(cuts.CutsError):
         cuts.CutInfo("NON_EXCEPTIONAL").c()
+
+
+def _near_identity(V, eps, rng):
+    """links exp(i eps H) with H random traceless Hermitian"""
+    from scipy.linalg import expm
+    out = np.empty((V, 3, 3), dtype=np.complex128)
+    for i in range(V):
+        a = rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3))
+        h = (a + a.conj().T) / 2
+        h -= np.trace(h) / 3 * np.eye(3)
+        out[i] = expm(1j * eps * h)
+    return out
+
+
+def test_oracle_log_near_identity_matches_glu(reference):
+    """GLU's near-identity eigenvalue branch (1 - Re tr U / 3 < 1e-12)."""
+    dims = (4, 4, 4, 4)
+    V = 256
+    rng = np.random.default_rng(5)
+    U = _near_identity(V * 4, 3e-7, rng).reshape(V, 4, 3, 3)
+    assert (1.0 - np.trace(U, axis1=-2, axis2=-1).real / 3.0 < 1e-12).mean() > 0.5
+    reference.setup(dims)
+    reference.put_links(U)
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        p = reference.cuts(td, 2, 1, 3, 1, 0, 1.0, flow=1)
+        ref = cuts.read_output(p, "FIELDS")
+    o = CO.measure(U, dims, 2, 1, 3, 0, 1.0, definition=1)
+    assert np.abs(ref["fields"] - o["out0"]).max() <= 1e-10 * np.abs(ref["fields"]).max()

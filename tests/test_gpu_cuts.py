@@ -40,8 +40,8 @@ def test_files_match_glu(lat400, tmp_path, case):
     """cuts_struct's file: GLU's name, momentum list bit for bit, values to
     rounding."""
     dims = tuple(int(d) for d in lat400["dims"])
-    info = cuts.CutInfo(case["cuttype"], case["mom_cut"], "LINEAR", case["maxmom"],
-                        case["angle"], case["cyl_width"])
+    info = cuts.CutInfo(case["cuttype"], case["mom_cut"], case["field_definition"],
+                        case["maxmom"], case["angle"], case["cyl_width"])
     path, _ = cuts.cuts_struct(lat400[case["links"]], dims, info,
                                where=str(tmp_path) + "/", flow=case["flow"])
     assert path.name == case["file"]
@@ -64,12 +64,14 @@ CUTS = [("SPHERICAL_CUT", 12, 0, 1.0), ("HYPERCUBIC_CUT", 3, 0, 1.0),
 
 @pytest.mark.parametrize("dims", DIMS)
 @pytest.mark.parametrize("cuttype", ["GLUON_PROPS", "EXCEPTIONAL", "FIELDS"])
-def test_measure_matches_oracle(dims, cuttype):
+@pytest.mark.parametrize("definition", ["LINEAR", "LOGARITHMIC"])
+def test_measure_matches_oracle(dims, cuttype, definition):
     U = _links(dims)
     for mc, mm, ang, w in CUTS:
-        info = cuts.CutInfo(cuttype, mc, "LINEAR", mm, ang, w)
+        info = cuts.CutInfo(cuttype, mc, definition, mm, ang, w)
         r = cuts.measure(U, dims, info)
-        o = CO.measure(U, dims, cuts.CUTTYPES[cuttype], cuts.MOM_CUTS[mc], mm, ang, w)
+        o = CO.measure(U, dims, cuts.CUTTYPES[cuttype], cuts.MOM_CUTS[mc], mm, ang, w,
+                       cuts.FIELD_DEFINITIONS[definition])
         assert np.array_equal(r["mom"], o["mom"])
         k0, k1 = OUT_KEYS[cuttype]
         scale = np.abs(o["out0"]).max()
@@ -77,6 +79,30 @@ def test_measure_matches_oracle(dims, cuttype):
         if k1:
             assert _close(r[k1], o["out1"], scale), (mc, k1)
         assert abs(r["pspace_err"] - o["pspace_err"]) <= 1e-12 * o["pspace_err"]
+
+
+def test_log_of_identity_and_near_identity_links():
+    """The logarithm's near-identity eigenvalue branch, and exact identity
+    links (log 0; GLU's routine leaves its output unwritten there)."""
+    from scipy.linalg import expm
+    dims = (8, 8, 8, 8)
+    V = int(np.prod(dims))
+    U = _links(dims, 13)
+    rng = np.random.default_rng(4)
+    sel = rng.choice(V * 4, V // 2, replace=False)
+    flat = U.reshape(V * 4, 3, 3)
+    for k, i in enumerate(sel):
+        if k % 4 == 0:
+            flat[i] = np.eye(3)
+        else:
+            a = rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3))
+            h = (a + a.conj().T) / 2
+            h -= np.trace(h) / 3 * np.eye(3)
+            flat[i] = expm(1j * 3e-7 * h)
+    info = cuts.CutInfo("FIELDS", "SPHERICAL_CUT", "LOGARITHMIC", 6)
+    r = cuts.measure(U, dims, info)
+    o = CO.measure(U, dims, 2, 1, 6, 0, 1.0, 1)
+    assert _close(r["fields"], o["out0"], np.abs(o["out0"]).max())
 
 
 def test_device_entry_matches_host_entry():
@@ -108,6 +134,6 @@ def test_landau_fixed_fields_are_transverse():
 def test_bad_arguments_raise():
     U = _links((4, 4, 4, 8))
     with pytest.raises(cuts.CutsError):
-        cuts.measure(U, (4, 4, 4, 8), cuts.CutInfo(field_definition="LOGARITHMIC"))
+        cuts.measure(U, (4, 4, 4, 8), cuts.CutInfo(cuttype="STATIC_POTENTIAL"))
     with pytest.raises(cuts.CutsError):
         cuts.measure(_links((4, 4, 4, 11)), (4, 4, 4, 11), cuts.CutInfo())  # prime 11
