@@ -37,7 +37,7 @@ class GfixResult(C.Structure):
 
 # every symbol include/glu_gfix.h declares
 EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
-           "Coulomb_FA", "FOURIER_ACCELERATE2", "gfix_landau",
+           "Coulomb_FA", "FOURIER_ACCELERATE2", "cuts_struct", "gfix_landau",
            "gfix_landau_device", "gfix_coulomb", "gfix_coulomb_device",
            "gfix_observables", "gfix_reunit", "gfix_fourier_accelerate",
            "gfix_profile_landau", "gfix_profile_coulomb",

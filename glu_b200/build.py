@@ -19,7 +19,7 @@ LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libglu_gfix.so"
 SOURCES = ["gfix.cu", "glu_abi.cu", "noalloc.cu", "nersc.cu", "cuts.cu"]
 HEADERS = ["su3.cuh", "fft.cuh", "fft_pass.cuh", "fft_ct.cuh", "kernels.cuh", "extra_kernels.cuh",
-           "coulomb.cuh", "glu_compat.h"]
+           "coulomb.cuh", "glu_compat.h", "su3_log.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

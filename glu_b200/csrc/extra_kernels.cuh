@@ -2,6 +2,7 @@
 #pragma once
 
 #include "kernels.cuh"
+#include "su3_log.cuh"
 
 namespace gfix {
 
@@ -63,9 +64,10 @@ __global__ void k_reunit_links(cx<R> *U, size_t nlinks, size_t V) {
 // (grid (blocks per slice, Lt)): Re tr of the spatial and of the temporal
 // links, the largest Re tr of any link, and the sum over the slice of the
 // Hermitian projection of the temporal links (entries 00, 01, 02, 11, 12 of
-// Hermitian_proj, exactQ.c:358-371: 8 reals).  Partials: 11 per block.
+// Hermitian_proj, exactQ.c:358-371: 8 reals), and the same 8 reals of their
+// logarithm (exact_log_slow, exactQ.c:157-240).  Partials: 19 per block.
 constexpr int kDiagThreads = 128;
-constexpr int kDiagVals = 11;
+constexpr int kDiagVals = 19;
 
 template <typename R>
 __global__ void __launch_bounds__(kDiagThreads) k_link_diag(Ctx<R> c, int lcu,
@@ -99,6 +101,18 @@ __global__ void __launch_bounds__(kDiagThreads) k_link_diag(Ctx<R> c, int lcu,
         v[8] += (2 * i4 - i0 - i8) / 3.;
         v[9] += 0.5 * ((double)u[5].y + (double)u[7].y);
         v[10] += -0.5 * ((double)u[5].x - (double)u[7].x);
+        cx<double> ud[9], q[4];
+#pragma unroll
+        for (int e = 0; e < 9; e++) ud[e] = mk<double>((double)u[e].x, (double)u[e].y);
+        su3log::log_components(ud, q);  // (Q00 + i Q11, Q01, Q02, Q12)
+        v[11] += q[0].x;
+        v[12] += q[1].x;
+        v[13] += q[1].y;
+        v[14] += q[2].x;
+        v[15] += q[2].y;
+        v[16] += q[0].y;
+        v[17] += q[3].x;
+        v[18] += q[3].y;
       }
     }
   }

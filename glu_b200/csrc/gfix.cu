@@ -1724,7 +1724,7 @@ int gfix_link_diagnostics(const double *links, const size_t dims[4],
   // fixed-order sums; const_time: per slice t >= 1 the differences of the
   // Hermitian-projection sums from slice 0 (gftests.c:84-95)
   double sp = 0.0, tl = 0.0, mx = -1e300;
-  std::vector<std::array<double, 8>> hs(T);
+  std::vector<std::array<double, 16>> hs(T);  // linear 8 reals, log 8 reals
   for (int t = 0; t < T; t++) {
     hs[t].fill(0.0);
     for (int b = 0; b < nbs; b++) {
@@ -1732,24 +1732,28 @@ int gfix_link_diagnostics(const double *links, const size_t dims[4],
       sp += q[0];
       tl += q[1];
       mx = std::max(mx, q[2]);
-      for (int k = 0; k < 8; k++) hs[t][k] += q[3 + k];
+      for (int k = 0; k < 16; k++) hs[t][k] += q[3 + k];
     }
   }
-  double av = 0.0;
+  double av = 0.0, avlog = 0.0;
   for (int t = 1; t < T; t++) {
-    const auto &a = hs[0], &b = hs[t];
-    av += std::fabs(a[0] - b[0]);
-    av += std::hypot(a[1] - b[1], a[2] - b[2]);
-    av += std::hypot(a[3] - b[3], a[4] - b[4]);
-    av += std::fabs(a[5] - b[5]);
-    av += std::hypot(a[6] - b[6], a[7] - b[7]);
+    for (int d = 0; d < 2; d++) {
+      const double *a = hs[0].data() + 8 * d, *b = hs[t].data() + 8 * d;
+      double x = std::fabs(a[0] - b[0]);
+      x += std::hypot(a[1] - b[1], a[2] - b[2]);
+      x += std::hypot(a[3] - b[3], a[4] - b[4]);
+      x += std::fabs(a[5] - b[5]);
+      x += std::hypot(a[6] - b[6], a[7] - b[7]);
+      (d ? avlog : av) += x;
+    }
   }
   const double V = (double)e->V;
   out[0] = sp / (3.0 * 3.0 * V);        // all_links: spatial
   out[1] = tl / (3.0 * V);              //            temporal
   out[2] = (sp + tl) / (4.0 * 3.0 * V); // indivlinks average
   out[3] = mx / 3.0;                    // largest Re tr / NC
-  out[4] = T > 1 ? av / (9.0 * (T - 1)) : 0.0;  // const_time, linear
+  out[4] = T > 1 ? av / (9.0 * (T - 1)) : 0.0;     // const_time, linear
+  out[5] = T > 1 ? avlog / (9.0 * (T - 1)) : 0.0;  //             logarithmic
   return 0;
 }
 

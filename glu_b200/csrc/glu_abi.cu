@@ -182,13 +182,13 @@ size_t Landau(struct site *lat, const double accuracy, const size_t iter,
   double obs[3] = {0, 0, 0};
   gfix_observables(buf.p, d, obs);
   scatter(L, buf.p, V);
-  double dg[5] = {0, 0, 0, 0, 0};
+  double dg[6] = {0, 0, 0, 0, 0, 0};
   gfix_link_diagnostics(buf.p, d, dg);
   printf("[GF] Plaquette :: %1.15f \n[GF] Accuracy :: %1.4e\n", obs[2],
          r.theta);
   printf("[GF] Iters :: %zu\n[GF] Link trace :: %1.15f || Maximum :: %1.15f\n",
          r.iters, dg[2], dg[3]);
-  printf("[GF] Temporal constance || Lin %e || Log (not computed)\n", dg[4]);
+  printf("[GF] Temporal constance || Lin %e || Log %e \n", dg[4], dg[5]);
   printf("[GF] Functional :: %1.15f\n", obs[1]);
   return r.iters;
 }
@@ -241,7 +241,7 @@ size_t Coulomb(struct site *lat, const double accuracy, const size_t iter) {
   if (!buf.p) return it;
   gather(L, buf.p, V);
   gfix_reunit(buf.p, d);
-  double obs[3] = {0, 0, 0}, dg[5] = {0, 0, 0, 0, 0};
+  double obs[3] = {0, 0, 0}, dg[6] = {0, 0, 0, 0, 0, 0};
   gfix_observables(buf.p, d, obs);
   gfix_link_diagnostics(buf.p, d, dg);
   scatter(L, buf.p, V);
@@ -267,6 +267,44 @@ void FOURIER_ACCELERATE2(struct fftw_stuff *FFTW) {
   }
   for (int k = 0; k < 4; k++)
     memcpy(F->in[k], f.data() + (size_t)k * lcu * 2, lcu * 2 * sizeof(double));
+}
+
+}  // extern "C"
+
+extern "C" {
+
+/* GLU's momentum-space measurements (src/Cuts/cuts.c:110-184) for CUTTYPE =
+ * GLUON_PROPS, EXCEPTIONAL and FIELDS: the output file is written to the
+ * working directory under output_str_struct's name (GLU's default build),
+ * configuration number Latt.flow.  GLU leaves the transformed Lie fields in
+ * A; here A is left unchanged.  Other modes return GLU_FAILURE (-1). */
+int cuts_struct(struct site *lat, const struct cut_info CUTINFO) {
+  glu_site *A = reinterpret_cast<glu_site *>(lat);
+  size_t d[4];
+  dims_of(d);
+  const size_t V = volume();
+  gfix_cut_info ci;
+  ci.dir = CUTINFO.dir;
+  ci.type = CUTINFO.type;
+  ci.max_mom = CUTINFO.max_mom;
+  ci.definition = CUTINFO.definition;
+  ci.angle = CUTINFO.angle;
+  ci.cyl_width = CUTINFO.cyl_width;
+  Pinned buf(V * 72);
+  if (!buf.p) {
+    fprintf(stderr, "[CUTS] allocation of temporaries failed\n");
+    return -1;
+  }
+  gather(A, buf.p, V);
+  double err = 0.0;
+  char path[1024];
+  if (gfix_cuts_write(buf.p, d, &ci, "./", Latt.flow, &err, path, sizeof path) != 0) {
+    fprintf(stderr, "[CUTS] %s\n", gfix_cuts_error());
+    return -1;
+  }
+  fprintf(stdout, "\n[CUTS] P-Space gauge fixing error :: %1.5e \n\n", err);
+  fprintf(stdout, "[CUTS] Writing finished...\n[CUTS] Outputting to %s\n", path);
+  return 0;
 }
 
 }  // extern "C"

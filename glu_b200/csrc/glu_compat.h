@@ -43,3 +43,16 @@ struct glu_latt_info {
 };
 
 }  // namespace gfix
+
+// struct cut_info (src/Headers/GLU_types.h:94-103), under GLU's own name: it
+// is passed by value to cuts_struct, whose C declaration names it
+struct cut_info {
+  int dir;          // cut_mode
+  int type;         // momentum_cut_def
+  size_t max_mom;
+  size_t max_t;
+  char where[256];
+  int definition;   // lie_field_def
+  size_t angle;
+  double cyl_width;
+};

@@ -247,15 +247,16 @@ def fourier_accelerate(fields, dims, ndim=4):
 def link_diagnostics(links, dims) -> dict:
     """GLU's post-fix link diagnostics (gfix_link_diagnostics): spatial and
     temporal average link trace (all_links), average and largest link trace
-    (indivlinks, both / NC) and the linear temporal constancy (const_time)."""
+    (indivlinks, both / NC) and the linear and logarithmic temporal
+    constancy (const_time)."""
     lib = _lib.load()
     cd, d = _dims(dims)
     U = _links(links, d)
-    out = np.zeros(5)
+    out = np.zeros(6)
     check(lib.gfix_link_diagnostics(U.ctypes.data, cd,
                                     out.ctypes.data_as(C.POINTER(C.c_double))))
     return dict(splink=out[0], tlink=out[1], link=out[2], link_max=out[3],
-                const_lin=out[4])
+                const_lin=out[4], const_log=out[5])
 
 
 def fft_tuning(on: bool):

@@ -36,6 +36,7 @@ extern "C" {
 /* GLU types, by reference only (src/Headers/GLU_types.h) */
 struct site;
 struct fftw_stuff;
+struct cut_info;
 
 /* ---------------------------------------------------------------------
  * GLU entry points
@@ -78,6 +79,14 @@ size_t Coulomb_FA(struct site *lat, struct fftw_stuff *FFTW,
 /* 3D version of FOURIER_ACCELERATE3 over one slice of Lx*Ly*Lz sites.
  * Replaces src/Gfix/CFACG.c:69-88. */
 void FOURIER_ACCELERATE2(struct fftw_stuff *FFTW);
+
+/* Momentum-space gluon measurements: CUTTYPE = GLUON_PROPS, EXCEPTIONAL or
+ * FIELDS, either field definition, every momentum cut.  Replaces
+ * src/Cuts/cuts.c:110-184 (src/Headers/cuts.h:40-42): writes GLU's output
+ * file into the working directory (named by output_str_struct, configuration
+ * number Latt.flow) and returns GLU_SUCCESS (0), or GLU_FAILURE (-1) for
+ * the other modes.  A is left unchanged. */
+int cuts_struct(struct site *A, const struct cut_info CUTINFO);
 
 /* ---------------------------------------------------------------------
  * flat interface
@@ -185,8 +194,8 @@ int gfix_observables(const double *links, const size_t dims[4], double *out);
  * out[0] spatial and out[1] temporal average Re tr / NC (all_links,
  * src/Field/plaqs_links.c:399-420), out[2] average Re tr / NC of all links
  * and out[3] the largest Re tr / NC (indivlinks, plaqs_links.c:424-446),
- * out[4] the temporal constancy, linear definition (const_time,
- * src/Gfix/gftests.c:35-129; its logarithmic twin is not computed). */
+ * out[4] and out[5] the temporal constancy, linear and logarithmic
+ * definitions (const_time, src/Gfix/gftests.c:35-129).  out holds 6. */
 int gfix_link_diagnostics(const double *links, const size_t dims[4],
                           double *out);
 

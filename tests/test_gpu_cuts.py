@@ -137,3 +137,67 @@ def test_bad_arguments_raise():
         cuts.measure(U, (4, 4, 4, 8), cuts.CutInfo(cuttype="STATIC_POTENTIAL"))
     with pytest.raises(cuts.CutsError):
         cuts.measure(_links((4, 4, 4, 11)), (4, 4, 4, 11), cuts.CutInfo())  # prime 11
+
+
+class _Site(__import__("ctypes").Structure):
+    """GLU's struct site (src/Headers/GLU_types.h:269-273)"""
+    import ctypes as C
+    _fields_ = [("O", C.POINTER(C.POINTER(C.c_double))),
+                ("neighbor", C.c_size_t * 4), ("back", C.c_size_t * 4)]
+
+
+class _Latt(__import__("ctypes").Structure):
+    """GLU's struct latt_info (src/Headers/GLU_types.h:229-243)"""
+    import ctypes as C
+    _fields_ = [("dims", C.c_size_t * 4), ("Lsq", C.c_size_t), ("Lcu", C.c_size_t),
+                ("Volume", C.c_size_t), ("flow", C.c_size_t), ("gf_alpha", C.c_double),
+                ("sm_alpha", C.c_double * 3), ("head", C.c_int), ("Seed", C.c_uint32 * 1),
+                ("twiddles", C.c_double * 4), ("Nthreads", C.c_uint32),
+                ("su2_data", C.c_void_p), ("argc", C.c_int)]
+
+
+class _CutInfo(__import__("ctypes").Structure):
+    """GLU's struct cut_info (src/Headers/GLU_types.h:94-103)"""
+    import ctypes as C
+    _fields_ = [("dir", C.c_int), ("type", C.c_int), ("max_mom", C.c_size_t),
+                ("max_t", C.c_size_t), ("where", C.c_char * 256), ("definition", C.c_int),
+                ("angle", C.c_size_t), ("cyl_width", C.c_double)]
+
+
+def test_glu_named_cuts_struct_writes_glus_file(lat400, tmp_path, monkeypatch):
+    """cuts_struct called as GLU calls it: a struct site lattice, Latt set,
+    the file written into the working directory."""
+    import ctypes as C
+    from glu_b200 import _lib
+    lib = _lib.load()
+    case = next(c for c in CASES if c["cuttype"] == "GLUON_PROPS"
+                and c["field_definition"] == "LOGARITHMIC")
+    dims = tuple(int(d) for d in lat400["dims"])
+    V = int(np.prod(dims))
+    U = np.ascontiguousarray(lat400[case["links"]])
+    rows = [(C.c_double * 18).from_buffer(U[i, mu]) for i in range(V) for mu in range(4)]
+    ptrs = [(C.POINTER(C.c_double) * 4)(*[C.cast(rows[i * 4 + mu], C.POINTER(C.c_double))
+                                          for mu in range(4)]) for i in range(V)]
+    sites = (_Site * V)()
+    for i in range(V):
+        sites[i].O = C.cast(ptrs[i], C.POINTER(C.POINTER(C.c_double)))
+    latt = _Latt.in_dll(lib, "Latt")
+    for mu in range(4):
+        latt.dims[mu] = dims[mu]
+    latt.Volume = V
+    latt.flow = case["flow"]
+    ci = _CutInfo(cuts.CUTTYPES[case["cuttype"]], cuts.MOM_CUTS[case["mom_cut"]],
+                  case["maxmom"], 0, b"./", 1, case["angle"], case["cyl_width"])
+    lib.cuts_struct.restype = C.c_int
+    lib.cuts_struct.argtypes = [C.POINTER(_Site), _CutInfo]
+    monkeypatch.chdir(tmp_path)
+    before = U.copy()
+    assert lib.cuts_struct(sites, ci) == 0
+    assert np.array_equal(U, before)  # the lattice is left as it was
+    got = cuts.read_output(tmp_path / case["file"], "GLUON_PROPS")
+    ref = cuts.read_output(GOLD / case["file"], "GLUON_PROPS")
+    assert np.array_equal(got["mom"], ref["mom"])
+    assert _close(got["transverse"], ref["transverse"], np.abs(ref["transverse"]).max())
+    assert _close(got["longitudinal"], ref["longitudinal"], np.abs(ref["transverse"]).max())
+    ci.dir = 1  # NON_EXCEPTIONAL: not provided
+    assert lib.cuts_struct(sites, ci) == -1

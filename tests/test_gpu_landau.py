@@ -62,8 +62,8 @@ def test_fourier_accelerate3_matches_oracle(oracle, dims):
 
 @pytest.mark.parametrize("which", ["input", "landau", "coulomb"])
 def test_link_diagnostics_match_reference(lat400, which):
-    """all_links, indivlinks and the linear const_time of GLU (fixture values
-    from the reference build) on the input and on the fixed links."""
+    """all_links, indivlinks and both const_time definitions of GLU (fixture
+    values from the reference build) on the input and on the fixed links."""
     g = lat400
     links = {"input": g["links"], "landau": g["landau_facg_links"],
              "coulomb": g["coulomb_facg_links"]}[which]
@@ -76,6 +76,8 @@ def test_link_diagnostics_match_reference(lat400, which):
     assert abs(got["link_max"] - ref[4] / 3.0) < 1e-14
     # a difference of slice sums of O(1) entries: rounding floor ~1e-15
     assert abs(got["const_lin"] - ref[5]) <= 1e-12 * ref[5] + 1e-15
+    # the same with the exact logarithm of every temporal link
+    assert abs(got["const_log"] - ref[6]) <= 1e-11 * ref[6] + 1e-13
 
 
 def test_reunit_matches_oracle(oracle, lat400):
