@@ -55,12 +55,13 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--workload", default="landau",
-                    choices=["landau", "coulomb", "ensemble", "gluonprop"],
+                    choices=["landau", "coulomb", "ensemble", "gluonprop", "heatbath"],
                     help="landau: 32^3x64 Landau FACG (the headline); coulomb: "
                          "64^3x128 Coulomb FACG, all slices batched; ensemble: "
                          "48 x 16^3x32 + 16 x 24^3x48 Landau FASD in one batch; "
                          "gluonprop: 32^3x64 momentum-space gluon propagators "
-                         "(GLU's cuts_struct, GLUON_PROPS)")
+                         "(GLU's cuts_struct, GLUON_PROPS); heatbath: 32^3x64 "
+                         "heatbath + over-relaxation updates at beta 6.0")
     ap.add_argument("--dims", default=None,
                     help="lattice extents; default 32,32,32,64 (landau) or "
                          "64,64,64,128 (coulomb)")
@@ -1230,10 +1231,165 @@ def gluonprop_main(args, dims, rank, world, local):
         emit(line)
 
 
+# ---------------------------------------------------------------------
+# configuration generation: GLU's heatbath + over-relaxation update
+# (hb_update's update_lattice: one heatbath sweep and four over-relaxation
+# sweeps per step), beta 6.0
+
+H_BETA, H_NOR = 6.0, 4
+H_UNIT = "update steps/hour"
+
+
+def h_metric_name(dims) -> str:
+    return ("heatbath + 4 over-relaxation update steps/hour (%dx%dx%dx%d, beta 6.0)"
+            % tuple(dims))
+
+
+def h_reference_seconds(dims, nthreads, steps=2):
+    """seconds per update step of GLU's own heatbath (oracle/_ref) on the
+    host cores, from a thermalised-like start: a bounded sample of steps"""
+    from oracle import oracle as O
+    from glu_b200.workload import tiled_config
+    R = O.Reference()
+    R.setup(dims, nthreads, 0.08, 11)
+    R.put_links(tiled_config(dims, seed=2))
+    t0 = time.perf_counter()
+    R.heatbath(H_BETA, steps, H_NOR)
+    return (time.perf_counter() - t0) / steps, steps
+
+
+def heatbath_main(args, dims, rank, world, local):
+    import torch
+    cfg = {"workload": "heatbath %s beta %.1f, 1 HB + %d OR sweeps per step"
+                       % ("x".join(map(str, dims)), H_BETA, H_NOR),
+           "generator": "Philox4x32-10, seed 1 + rank"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cores = os.cpu_count() or 1
+        t, n = h_reference_seconds(dims, cores)
+        value = 3600.0 / t
+        emit({"metric": h_metric_name(dims), "value": value, "unit": H_UNIT,
+              "n_gpus": world, "steps": n, "warmup": 0, "ms_per_step": t * 1e3,
+              "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+              "dtype": "f64", "data": "synthetic (8^4 GLU heatbath tiled + random gauge)",
+              "config": dict(cfg, parallelism="host OpenMP"), "impl": "reference",
+              "cpu_baseline": {"value": value, "unit": H_UNIT, "cores": cores,
+                               "kind": "reference",
+                               "sample": "%d GLU update steps (hb_lattice + 4 OR_lattice)" % n},
+              "e2e": {"value": value, "unit": H_UNIT, "h2d_bytes_per_step": 0,
+                      "d2h_bytes_per_step": 0}})
+        return
+    torch.cuda.set_device(local)
+    import ctypes as C
+    from glu_b200 import _lib
+    from glu_b200.workload import tiled_config
+    lib = _lib.load()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    U = tiled_config(dims, seed=2 + rank)
+    V = int(np.prod(dims))
+    d = torch.from_numpy(U.view(np.float64).reshape(-1).copy()).cuda()
+    h = torch.from_numpy(U.view(np.float64).reshape(-1).copy()).pin_memory()
+    cd = (C.c_size_t * 4)(*dims)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    seed = 1 + rank
+
+    def run(mode, it0):
+        ms, l0 = 0.0, 0
+        for k in range(args.warmup + args.steps):
+            if k == args.warmup:
+                l0 = lib.gfix_kernel_launches()
+            barrier()
+            a, e = ev(), ev()
+            a.record()
+            if mode == "device":
+                rc = lib.gfix_heatbath_device(d.data_ptr(), cd, H_BETA, 1, H_NOR, seed,
+                                              it0 + k, None)
+            else:
+                rc = lib.gfix_heatbath(h.data_ptr(), cd, H_BETA, 1, H_NOR, seed, it0 + k, None)
+            e.record()
+            if rc != 0:
+                raise RuntimeError(lib.gfix_update_error().decode())
+            barrier()
+            if k >= args.warmup:
+                ms += a.elapsed_time(e)
+        return max_over_ranks(ms), lib.gfix_kernel_launches() - l0
+
+    with Clocks(local) as clk:
+        ms_dev, launches = run("device", 0)
+        ms_host, _ = run("host", 1000)
+        # one step's kernels alone: the layout conversion is part of the
+        # device call; time 10 steps in one call to see the sweeps
+        a, e = ev(), ev()
+        barrier()
+        a.record()
+        if lib.gfix_heatbath_device(d.data_ptr(), cd, H_BETA, 10, H_NOR, seed, 5000, None):
+            raise RuntimeError(lib.gfix_update_error().decode())
+        e.record()
+        barrier()
+        ms10 = a.elapsed_time(e) / 10
+    steps = args.steps
+    hbm, peak_src = peaks()
+    # algorithmic bytes of one (direction, colour) launch: the updated links
+    # read and written (2 x 144 B x V/2), the other colour's links of that
+    # direction and all links of the other three directions read for the
+    # staples (144 B x (V/2 + 3 V)): 648 B per site; 8 launches per sweep
+    sweep_bytes = 8 * 648 * V
+    sweeps = 1 + H_NOR
+    achieved = sweep_bytes * sweeps / (ms10 * 1e-3) / 1e9
+    line = {
+        "metric": h_metric_name(dims), "value": world * steps * 3600e3 / ms_dev,
+        "unit": H_UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": ms_dev / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled + seeded random gauge)",
+        "config": dict(cfg, ms_per_step_in_10_step_call=ms10,
+                       l2="%.2f GB of links, larger than the 126 MB L2" % (V * 576 / 1e9),
+                       parallelism="one lattice per GPU" if world > 1 else "single GPU"),
+        "roofline": {"bound": "hbm", "kernel": "k_update", "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic_from_profiles("k_update_hb", "fp64", dims),
+                     "peak_source": peak_src},
+        "e2e": {"value": world * steps * 3600e3 / ms_host, "unit": H_UNIT,
+                "h2d_bytes_per_step": V * 576, "d2h_bytes_per_step": V * 576},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            t, n = h_reference_seconds(dims, os.cpu_count() or 1)
+            line["cpu_baseline"] = {"value": 3600.0 / t, "unit": H_UNIT,
+                                    "cores": os.cpu_count() or 1, "kind": "reference",
+                                    "sample": "%d GLU update steps, %.2f s each" % (n, t)}
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": H_UNIT, "kind": "unavailable",
+                                    "sample": str(e)}
+    if rank == 0:
+        emit(line)
+
+
 def main():
     args = parse()
     if args.dims is None:
-        args.dims = ("32,32,32,64" if args.workload in ("landau", "gluonprop")
+        args.dims = ("32,32,32,64" if args.workload in ("landau", "gluonprop", "heatbath")
                      else "64,64,64,128")
     dims = tuple(int(x) for x in args.dims.split(","))
     rank, world, local = dist_env()
@@ -1245,6 +1401,9 @@ def main():
         return
     if args.workload == "gluonprop":
         gluonprop_main(args, dims, rank, world, local)
+        return
+    if args.workload == "heatbath":
+        heatbath_main(args, dims, rank, world, local)
         return
     if args.profile_only:
         profile_only(args, dims)

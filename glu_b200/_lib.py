@@ -49,6 +49,8 @@ EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
            "gfix_nersc_error", "gfix_scidac_checksum", "gfix_cut_veclist",
            "gfix_cuts_measure", "gfix_cuts_measure_device", "gfix_cuts_write",
            "gfix_profile_cuts", "gfix_cuts_error", "gfix_cuts_release",
+           "gfix_heatbath", "gfix_heatbath_device", "gfix_overrelax",
+           "gfix_philox4x32_10", "gfix_update_error", "gfix_update_release",
            "gfix_noalloc_error",
            "gfix_last_error", "gfix_release", "gfix_kernel_launches")
 
@@ -100,6 +102,18 @@ def load(path: Path | str | None = None):
     lib.gfix_profile_cuts.restype = C.c_int
     lib.gfix_profile_cuts.argtypes = [C.c_void_p, _szp, _ci, C.c_int,
                                       C.POINTER(C.c_float)]
+    for fn in ("gfix_heatbath", "gfix_heatbath_device"):
+        getattr(lib, fn).restype = C.c_int
+        getattr(lib, fn).argtypes = [C.c_void_p, _szp, C.c_double, C.c_size_t,
+                                     C.c_size_t, C.c_uint64, C.c_uint64, _dp]
+    lib.gfix_overrelax.restype = C.c_int
+    lib.gfix_overrelax.argtypes = [C.c_void_p, _szp, C.c_size_t]
+    _u32p = C.POINTER(C.c_uint32)
+    lib.gfix_philox4x32_10.restype = None
+    lib.gfix_philox4x32_10.argtypes = [_u32p, _u32p, _u32p]
+    lib.gfix_update_error.restype = C.c_char_p
+    lib.gfix_update_error.argtypes = []
+    lib.gfix_update_release.restype = None
     lib.gfix_cuts_error.restype = C.c_char_p
     lib.gfix_cuts_error.argtypes = []
     lib.gfix_cuts_release.restype = None

@@ -17,7 +17,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libglu_gfix.so"
-SOURCES = ["gfix.cu", "glu_abi.cu", "noalloc.cu", "nersc.cu", "cuts.cu"]
+SOURCES = ["gfix.cu", "glu_abi.cu", "noalloc.cu", "nersc.cu", "cuts.cu", "update.cu"]
 HEADERS = ["su3.cuh", "fft.cuh", "fft_pass.cuh", "fft_ct.cuh", "kernels.cuh", "extra_kernels.cuh",
            "coulomb.cuh", "glu_compat.h", "su3_log.cuh"]
 

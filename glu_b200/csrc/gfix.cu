@@ -1627,6 +1627,7 @@ int gfix_fft_plan(const size_t dims[4], int coulomb, int precision, int *plan,
 
 void gfix_release(void) {
   gfix_cuts_release();
+  gfix_update_release();
   g_e64.clear();
   g_e32.clear();
   g_ec.clear();

@@ -362,6 +362,35 @@ int gfix_profile_cuts(const double *d_links, const size_t dims[4],
 const char *gfix_cuts_error(void);
 void gfix_cuts_release(void);
 
+/* Quenched SU(3) configurations by heatbath and over-relaxation (GLU's
+ * hb_update, src/Update/KPHB.c:123-257, MODE = HEATBATH): each of
+ * `iterations` steps is one heatbath sweep (hb_lattice, src/Update/hb.c:
+ * 146-194: Kennedy-Pendleton per SU(2) subgroup, links reunitarised) and
+ * n_or over-relaxation sweeps (OR_lattice, src/Update/relax.c:83-114), in
+ * GLU's order (per direction, per draughtboard colour).  beta is the Wilson
+ * coupling; random numbers are Philox4x32-10 keyed by `seed`, the counter
+ * holding the step number first_iteration + i, so a run continued from
+ * (seed, first_iteration) equals the uninterrupted one.  plaquettes (may be
+ * NULL) receives the average plaquette after every step.  Even extents
+ * only.  Links as everywhere: double[V][4][9][2], host or device. */
+int gfix_heatbath(double *links, const size_t dims[4], double beta,
+                  size_t iterations, size_t n_or, uint64_t seed,
+                  uint64_t first_iteration, double *plaquettes);
+int gfix_heatbath_device(double *d_links, const size_t dims[4], double beta,
+                         size_t iterations, size_t n_or, uint64_t seed,
+                         uint64_t first_iteration, double *plaquettes);
+
+/* `sweeps` over-relaxation sweeps alone (deterministic: no random numbers) */
+int gfix_overrelax(double *links, const size_t dims[4], size_t sweeps);
+
+/* the generator's block function: Philox4x32-10 of counter ctr under key
+ * (host only) */
+void gfix_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2],
+                        uint32_t out[4]);
+
+const char *gfix_update_error(void);
+void gfix_update_release(void);
+
 /* message of the last failed call (thread-local, never NULL) */
 const char *gfix_last_error(void);
 

@@ -233,6 +233,10 @@ class Reference:
         L.ref_cut_output_name.restype = C.c_int
         L.ref_cut_output_name.argtypes = [C.c_int, C.c_int, _sz, C.c_int, _sz,
                                           C.c_double, _sz, C.c_char_p, _sz]
+        L.ref_overrelax.restype = C.c_int
+        L.ref_overrelax.argtypes = [_sz]
+        L.ref_heatbath.restype = C.c_int
+        L.ref_heatbath.argtypes = [C.c_double, _sz, _sz, _dp]
         L.ref_cuts.restype = C.c_int
         L.ref_cuts.argtypes = [C.c_int, C.c_int, _sz, C.c_int, _sz, C.c_double,
                                _sz, C.c_char_p]
@@ -317,6 +321,20 @@ class Reference:
 
     def fft_seconds(self):
         return self.lib.ref_fft_seconds()
+
+    # configuration generation (src/Update)
+    def overrelax(self, sweeps):
+        """GLU's OR_lattice sweeps on the lattice in place."""
+        if self.lib.ref_overrelax(sweeps) != 0:
+            raise RuntimeError("reference over-relaxation failed")
+
+    def heatbath(self, beta, iterations, n_or=0):
+        """GLU's heatbath steps on the lattice in place (its own generator,
+        seeded by setup's seed); the plaquette after every step."""
+        plaq = np.zeros(max(iterations, 1))
+        if self.lib.ref_heatbath(beta, iterations, n_or, _ptr(plaq)) != 0:
+            raise RuntimeError("reference heatbath failed")
+        return plaq[:iterations]
 
     # momentum-space cuts (src/Cuts/cuts.c:110-184)
     def veclist(self, dir, type, max_mom, angle=0, cyl_width=1.0):

@@ -21,6 +21,10 @@
 #include "FACG.h"
 #include "GLUlib_wrap.h"
 #include "cut_output.h"
+#include "draughtboard.h"
+#include "hb.h"
+#include "par_rng.h"
+#include "relax.h"
 #include "cut_routines.h"
 #include "cuts.h"
 #include "Landau.h"
@@ -335,4 +339,44 @@ int ref_cuts(int dir, int type, size_t max_mom, int definition, size_t angle,
   const int rc = cuts_struct(g_lat, c);
   if (chdir(cwd) != 0) return -1;
   return rc == GLU_SUCCESS ? 0 : -1;
+}
+
+/* configuration generation: GLU's over-relaxation sweeps (OR_lattice,
+ * src/Update/relax.c:83-114) and heatbath steps (update_lattice,
+ * src/Update/KPHB.c:83-99: hb_lattice then n_or OR_lattice) on the lattice
+ * in place, with GLU's draughtboard (src/Geometry/draughtboard.c) and its
+ * own generator seeded from Latt.Seed; plaq (may be NULL) receives the
+ * average plaquette after every step */
+/* GLU's sweeps use orphaned `omp for` loops: as in hb_update
+ * (KPHB.c:193-250) they run inside one parallel region */
+int ref_overrelax(size_t sweeps) {
+  struct draughtboard db;
+  if (!g_lat || init_cb(&db, LVOLUME, ND) == GLU_FAILURE) return -1;
+#pragma omp parallel
+  {
+    for (size_t k = 0; k < sweeps; k++) OR_lattice(g_lat, db);
+  }
+  free_cb(&db);
+  return 0;
+}
+
+int ref_heatbath(double beta, size_t iterations, size_t n_or, double *plaq) {
+  struct draughtboard db;
+  if (!g_lat || initialise_par_rng(NULL) == GLU_FAILURE) return -1;
+  if (init_cb(&db, LVOLUME, ND) == GLU_FAILURE) return -1;
+  const double inverse_beta = NC / beta;
+#pragma omp parallel
+  {
+    for (size_t i = 0; i < iterations; i++) {
+      hb_lattice(g_lat, inverse_beta, db);
+      for (size_t k = 0; k < n_or; k++) OR_lattice(g_lat, db);
+#pragma omp single
+      {
+        if (plaq) plaq[i] = av_plaquette(g_lat);
+      }
+    }
+  }
+  free_cb(&db);
+  free_par_rng();
+  return 0;
 }

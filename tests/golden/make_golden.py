@@ -16,6 +16,9 @@ lat400.npz   4^3x8 configuration shipped with the reference (CONF/lat..400),
                fixed step), Coulomb FACG / FASD (GLU_GFIX_SD build)
 cuts/        GLU's momentum-space output files (G2F2 / MOMgg / MATS) of the
              Landau-fixed lat400 links, with cases.json
+heatbath_glu.json  GLU's heatbath + over-relaxation plaquette statistics
+             (8^4, unit start) at beta 6.0 and 5.7; lat400.npz["or2_links"]
+             holds the fixture links after two of GLU's over-relaxation sweeps
 hb8.npz      8^4 SU(3) configuration from GLU's heatbath (beta 6.0, cold
              start, seed 1, 500 sweeps of KP heatbath + 4 over-relaxation,
              8 OpenMP threads), plus reference Landau FACG (alpha 0.08,
@@ -246,7 +249,53 @@ def cuts_fixture() -> None:
     (out / "cases.json").write_text(json.dumps(cases, indent=1) + "\n")
 
 
+# GLU's heatbath statistics (hb_update's update_lattice): 8^4 from the unit
+# configuration, (beta, OR sweeps per heatbath, thermalisation, measured)
+HB_RUNS = [(6.0, 4, 100, 1000), (5.7, 4, 100, 600)]
+HB_BIN = 20
+
+
+def binned(x, b):
+    """mean and its error from bins of b consecutive measurements"""
+    n = len(x) // b
+    m = np.asarray(x[: n * b]).reshape(n, b).mean(axis=1)
+    return float(m.mean()), float(m.std(ddof=1) / np.sqrt(n))
+
+
+def update_fixture() -> None:
+    """lat400.npz["or2_links"]: the fixture links after two of GLU's
+    over-relaxation sweeps; tests/golden/heatbath_glu.json: GLU's average
+    plaquette (binned mean and error) at each HB_RUNS point."""
+    import json
+    g = dict(np.load(OUT / "lat400.npz"))
+    dims = tuple(int(d) for d in g["dims"])
+    R = Reference()
+    R.setup(dims, 1, 0.08)
+    R.put_links(g["links"])
+    R.overrelax(2)
+    g["or2_links"] = R.get_links()
+    np.savez(OUT / "lat400.npz", **g)
+    runs = []
+    d8 = (8, 8, 8, 8)
+    unit = np.zeros((8 ** 4, 4, 3, 3), dtype=np.complex128)
+    for k in range(3):
+        unit[..., k, k] = 1.0
+    for beta, n_or, therm, iters in HB_RUNS:
+        R.setup(d8, 1, 0.08, 11)
+        R.put_links(unit)
+        p = R.heatbath(beta, therm + iters, n_or)
+        mean, err = binned(p[therm:], HB_BIN)
+        runs.append(dict(beta=beta, n_or=n_or, therm=therm, iterations=iters,
+                         bin=HB_BIN, mean=mean, err=err))
+        print("GLU heatbath beta %.2f: <P> = %.6f +- %.6f" % (beta, mean, err))
+    (OUT / "heatbath_glu.json").write_text(
+        json.dumps(dict(dims=list(d8), start="unit", runs=runs), indent=1) + "\n")
+
+
 def main() -> None:
+    if "--update" in sys.argv:
+        update_fixture()
+        return
     if "--cuts" in sys.argv:
         cuts_fixture()
         return
@@ -282,6 +331,7 @@ def main() -> None:
     nersc_fixture()
     ildg_fixture()
     cuts_fixture()
+    update_fixture()
 
     # ---- 8^4 heatbath configuration -------------------------------------
     with tempfile.TemporaryDirectory() as td:
