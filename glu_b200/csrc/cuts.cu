@@ -1112,7 +1112,8 @@ long gfix_cut_veclist(const size_t dims[4], const gfix_cut_info *ci, int32_t *mo
 int gfix_cuts_measure_device(const double *d_links, const size_t dims[4],
                              const gfix_cut_info *ci, size_t nmom, double *out0,
                              double *out1, double *pspace_err) {
-  if (check_info(dims, ci) || !d_links) return d_links ? -1 : cfail("null links");
+  if (!d_links) return cfail("null links");
+  if (check_info(dims, ci)) return -1;
   Work *w = work_for(dims);
   if (!w) return -1;
   w->c.links = reinterpret_cast<const C2 *>(d_links);
@@ -1121,7 +1122,8 @@ int gfix_cuts_measure_device(const double *d_links, const size_t dims[4],
 
 int gfix_cuts_measure(const double *links, const size_t dims[4], const gfix_cut_info *ci,
                       size_t nmom, double *out0, double *out1, double *pspace_err) {
-  if (check_info(dims, ci) || !links) return links ? -1 : cfail("null links");
+  if (!links) return cfail("null links");
+  if (check_info(dims, ci)) return -1;
   Work *w = work_for(dims);
   if (!w || w->ensure_links()) return -1;
   CCK(cudaMemcpyAsync(w->d_links, links, (size_t)w->V * 36 * sizeof(C2),
@@ -1134,8 +1136,6 @@ int gfix_cuts_write(const double *links, const size_t dims[4], const gfix_cut_in
                     const char *where, size_t flow, double *pspace_err, char *path_out,
                     size_t path_cap) {
   if (check_info(dims, ci)) return -1;
-  int L[4];
-  for (int i = 0; i < 4; i++) L[i] = (int)dims[i];
   Work *w = work_for(dims);
   if (!w) return -1;
   const MomList *ml = w->list(*ci);
@@ -1153,8 +1153,8 @@ int gfix_cuts_write(const double *links, const size_t dims[4], const gfix_cut_in
 
 int gfix_profile_cuts(const double *d_links, const size_t dims[4], const gfix_cut_info *ci,
                       int reps, float ms[3]) {
-  if (check_info(dims, ci) || !d_links || !ms || reps < 1)
-    return cfail("bad arguments to gfix_profile_cuts");
+  if (!d_links || !ms || reps < 1) return cfail("bad arguments to gfix_profile_cuts");
+  if (check_info(dims, ci)) return -1;
   Work *w = work_for(dims);
   if (!w) return -1;
   w->c.links = reinterpret_cast<const C2 *>(d_links);

@@ -99,8 +99,7 @@ __host__ __device__ __forceinline__ void mulhilo(uint32_t a, uint32_t b, uint32_
 __host__ __device__ __forceinline__ U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
   constexpr uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
   constexpr uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
-#pragma unroll
-  for (int r = 0; r < 10; r++) {
+  for (int r = 0; r < 10; r++) {  // constant trip count: unrolled by nvcc
     uint32_t h0, l0, h1, l1;
     mulhilo(M0, c.x, &h0, &l0);
     mulhilo(M1, c.z, &h1, &l1);
