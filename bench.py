@@ -5,22 +5,25 @@ hour.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                     [--precision mixed|fp64] [--dims 32,32,32,64]
 
-A step is one complete gauge fix (GLU's FACG to theta < 1e-14) of one
-configuration.  `value` is measured with the links resident in HBM (the
-device entry point gfix_landau_device); `e2e` is the same fix through the
-host entry point gfix_landau from pinned host memory, host->device and
-device->host copies inside the timed region.  Both run the mixed FP32->FP64
-path by default and report the plain FP64 path beside it.
+A step is four complete gauge fixes (GLU's FACG to theta < 1e-14).
+`value` is measured with the links resident in HBM (the device entry point
+gfix_landau_device); `e2e` is the same fixes through the host entry point
+gfix_landau from pinned host memory, host->device and device->host copies
+inside the timed region.  Both run the mixed FP32->FP64 path by default and
+report the plain FP64 path beside it.
 
-Input: the seeded synthetic stand-in of glu_b200.workload (the committed
-8^4 beta 6.0 GLU heatbath configuration repeated to 32^3x64, then a seeded
-random gauge transformation).  At N > 1 every rank fixes its own
-configuration (seed 2 + rank): weak scaling, no collective on the data path.
+Input: beta 6.0 heatbath configurations generated on the GPU before any
+timed region (glu_b200.workload.heatbath_config: GLU's heatbath algorithm,
+1000 iterations of one heatbath and four over-relaxation sweeps from the unit
+start).  A step fixes four of them (seeds 2..5; rank r: 2 + 4r ..): on
+thermalised fields the iteration count of a fix varies twofold between
+configurations, so the throughput is that of a set.  At N > 1 every rank
+fixes its own set: weak scaling, no collective on the data path.
 
 The reference arm (--impl reference) times GLU itself, compiled from its
 sources (oracle/_ref), on the host cores: a bounded sample of FACG
-iterations on the same configuration, scaled by the iteration count of a
-full fix.
+iterations on the first configuration, scaled by the iteration counts of
+GLU's full fixes of the four (profiles/reference_full_fix.json).
 """
 from __future__ import annotations
 
@@ -137,9 +140,24 @@ def dist_env():
     return rank, world, local
 
 
-def workload(dims, rank):
-    from glu_b200.workload import tiled_config
-    return tiled_config(dims, seed=2 + rank)
+# the input of the Landau workload: beta 6.0 heatbath configurations, 1000
+# iterations of one heatbath and four over-relaxation sweeps from the unit
+# start, generated on the GPU before any timed region.  One step fixes
+# E_CONFIGS of them (seeds 2 + E_CONFIGS rank + i): the iteration count of a
+# fix on a thermalised configuration varies twofold between configurations
+# (and between summation orders), so throughput is measured over a set.
+H_INPUT = dict(beta=6.0, iterations=1000, n_or=4)
+INPUT_NAME = "heatbath beta 6.0, 1000 x (HB + 4 OR), unit start, seed %d"
+E_CONFIGS = 4
+
+
+def seeds(rank):
+    return [2 + E_CONFIGS * rank + i for i in range(E_CONFIGS)]
+
+
+def workload(dims, rank, i=0):
+    from glu_b200.workload import heatbath_config
+    return heatbath_config(dims, seed=seeds(rank)[i], **H_INPUT)
 
 
 def _params(prec: str, cap: int = 0):
@@ -207,17 +225,19 @@ def gpu_arm(args, dims, rank, world, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    U = workload(dims, rank)
-    flat = U.view(np.float64).reshape(-1)
-    host = torch.from_numpy(flat).pin_memory()
-    hwork = torch.empty_like(host).pin_memory()
-    dpristine = host.to("cuda")
-    dwork = torch.empty_like(dpristine)
+    Us = [workload(dims, rank, i) for i in range(E_CONFIGS)]
+    U = Us[0]
+    hosts = [torch.from_numpy(u.view(np.float64).reshape(-1)).pin_memory() for u in Us]
+    hwork = torch.empty_like(hosts[0]).pin_memory()
+    dpristine = [h.to("cuda") for h in hosts]
+    dwork = torch.empty_like(dpristine[0])
     cd = (C.c_size_t * 4)(*dims)
     V = int(np.prod(dims))
 
-    def dev_fix(prec):
-        dwork.copy_(dpristine)
+    def dev_fix(prec, i):
+        # the copy of the pristine input is device work inside the step; the
+        # library runs on its own stream, so the copy must be complete
+        dwork.copy_(dpristine[i])
         torch.cuda.synchronize()
         r = GfixResult()
         p = _params(prec)
@@ -236,34 +256,38 @@ def gpu_arm(args, dims, rank, world, local):
         for prec in ([args.precision, "fp64"] if args.precision == "mixed"
                      else ["fp64"]):
             for _ in range(args.warmup):
-                r = dev_fix(prec)
-            # resident inputs: K steps bracketed by barrier + sync
+                for i in range(E_CONFIGS):
+                    dev_fix(prec, i)
+            # resident inputs: K steps (each E_CONFIGS fixes) bracketed by
+            # barrier + sync
             launches0 = lib.gfix_kernel_launches()
             barrier()
             a, b = ev(), ev()
             a.record()
-            iters = []
+            per = []
             for _ in range(args.steps):
-                r = dev_fix(prec)
-                iters.append(r.iters)
+                per = []
+                for i in range(E_CONFIGS):
+                    r = dev_fix(prec, i)
+                    per.append((int(r.iters), int(r.iters_fp32), float(r.theta)))
             b.record()
             barrier()
             launches = lib.gfix_kernel_launches() - launches0
             ms = max_over_ranks(a.elapsed_time(b))
-            # end to end: pinned host buffers, H2D + D2H inside each step
+            # end to end: pinned host buffers, H2D + D2H inside each fix
             e_ms = 0.0
             for _ in range(args.steps):
-                hwork.copy_(host)
-                barrier()
-                a2, b2 = ev(), ev()
-                a2.record()
-                r2 = host_fix(prec)
-                b2.record()
-                torch.cuda.synchronize()
-                e_ms += a2.elapsed_time(b2)
+                for i in range(E_CONFIGS):
+                    hwork.copy_(hosts[i])
+                    barrier()
+                    a2, b2 = ev(), ev()
+                    a2.record()
+                    host_fix(prec)
+                    b2.record()
+                    torch.cuda.synchronize()
+                    e_ms += a2.elapsed_time(b2)
             e_ms = max_over_ranks(e_ms)
-            out[prec] = dict(ms=ms, e2e_ms=e_ms, iters=iters, iters_fp32=r.iters_fp32,
-                             theta=r.theta, launches=launches, e2e_iters=r2.iters)
+            out[prec] = dict(ms=ms, e2e_ms=e_ms, per=per, launches=launches)
     clocks = clk.summary()
     res = dict(out=out, clocks=clocks, V=V)
     # per-kernel device times for the roofline (events on the launch stream)
@@ -272,7 +296,7 @@ def gpu_arm(args, dims, rank, world, local):
         ms = np.zeros(7)
         by = np.zeros(7)
         check(lib.gfix_profile_landau(
-            dpristine.data_ptr(), cd, C.byref(_params(prec)), args.profile_iters,
+            dpristine[0].data_ptr(), cd, C.byref(_params(prec)), args.profile_iters,
             ms.ctypes.data_as(C.POINTER(C.c_double)),
             by.ctypes.data_as(C.POINTER(C.c_double))))
         prof["fp32" if prec == "mixed" else "fp64"] = (ms, by)
@@ -283,14 +307,16 @@ def gpu_arm(args, dims, rank, world, local):
 
 
 def reference_iters(dims):
-    """Iteration count of the reference's own full fix of this workload
-    (a property of algorithm and input), from the committed measurement."""
+    """Iteration counts of the reference's own full fixes of the step's
+    configurations (rank 0 seeds), from the committed measurements; None if
+    any is missing."""
     f = ROOT / "profiles" / "reference_full_fix.json"
-    if f.exists():
-        for e in json.loads(f.read_text()):
-            if tuple(e["dims"]) == tuple(dims):
-                return int(e["iters"]), e
-    return None, None
+    if not f.exists():
+        return None
+    rec = {e.get("input"): int(e["iters"]) for e in json.loads(f.read_text())
+           if tuple(e["dims"]) == tuple(dims)}
+    its = [rec.get(INPUT_NAME % sd) for sd in seeds(0)]
+    return None if any(i is None for i in its) else its
 
 
 def cpu_sample(U, dims, sample_s: float, nthreads: int, algo: str = "FACG"):
@@ -335,7 +361,7 @@ def reference_arm(args, dims, rank, world):
     if rank != 0:
         return
     U = workload(dims, 0)
-    n_ref, meta = reference_iters(dims)
+    n_ref = reference_iters(dims)
     cores = os.cpu_count() or 1
     for _ in range(max(args.warmup, 0) and 1):
         cpu_sample(U, dims, min(args.cpu_sample_s, 5.0), cores)
@@ -345,24 +371,27 @@ def reference_arm(args, dims, rank, world):
     fixed = statistics.median(s["fixed_s"] for s in samples)
     if n_ref is None:
         emit({"impl": "reference", "unavailable":
-              "no recorded full-fix iteration count for dims %s" % (dims,)})
+              "no recorded full-fix iteration counts for dims %s" % (dims,)})
         return
-    t_fix = fixed + s_iter * n_ref
-    value = 3600.0 / t_fix
+    # one step: the E_CONFIGS fixes, each GLU's recorded iteration count
+    t_set = E_CONFIGS * fixed + s_iter * sum(n_ref)
+    value = E_CONFIGS * 3600.0 / t_set
     s0 = samples[0]
     emit({"metric": metric_name(dims), "value": value, "unit": UNIT, "n_gpus": world,
           "steps": args.steps, "warmup": args.warmup,
-          "ms_per_step": t_fix * 1e3, "higher_is_better": True,
+          "ms_per_step": t_set * 1e3, "higher_is_better": True,
           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-          "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled + random gauge)",
-          "config": {"workload": "Landau FACG theta<1e-14, %s" % "x".join(map(str, dims)),
+          "data": "synthetic: %d configurations, %s (generated on the GPU)"
+                  % (E_CONFIGS, (INPUT_NAME % 2).replace("seed 2", "seeds 2..5")),
+          "config": {"workload": "Landau FACG theta<1e-14, %s, %d configurations per step"
+                                 % ("x".join(map(str, dims)), E_CONFIGS),
                      "dims": list(dims), "gf_alpha": ALPHA, "accuracy": ACC,
                      "full_fix_iters": n_ref, "parallelism": "host OpenMP"},
           "impl": "reference",
           "cpu_baseline": {"value": value, "unit": UNIT, "cores": s0["cores"],
                            "kind": s0["kind"],
                            "sample": "%d x %d FACG iterations per step, "
-                                     "%.3f s/iteration x %d iterations" %
+                                     "%.3f s/iteration x %s iterations" %
                                      (len(samples), s0["sample_iters"], s_iter, n_ref)},
           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                   "d2h_bytes_per_step": 0}})
@@ -371,15 +400,17 @@ def reference_arm(args, dims, rank, world):
 def gpu_line(args, dims, world, res, cpu):
     prec = args.precision
     o = res["out"][prec]
+    o64 = res["out"]["fp64"]
     steps = args.steps
     ms_step = o["ms"] / steps
-    value = world * steps * 3600e3 / o["ms"]
-    e2e = world * steps * 3600e3 / o["e2e_ms"]
+    nfix = world * steps * E_CONFIGS
+    value = nfix * 3600e3 / o["ms"]
+    e2e = nfix * 3600e3 / o["e2e_ms"]
     V = res["V"]
-    # dominant kernel over a whole fix: per-launch time x launches
+    # dominant kernel over the step's fixes: per-launch time x launches
     peak, peak_src = peaks()
-    it32 = o["iters_fp32"] if prec == "mixed" else 0
-    it64 = o["iters"][-1] - it32
+    it32 = sum(x[1] for x in o["per"]) if prec == "mixed" else 0
+    it64 = sum(x[0] for x in o["per"]) - it32
     share = []
     for tag, n in (("fp32", it32), ("fp64", it64)):
         ms, by = res["prof"][tag]
@@ -398,20 +429,25 @@ def gpu_line(args, dims, world, res, cpu):
         "steps": steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if prec == "mixed" else "f64",
-        "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled + seeded random gauge transform)",
-        "config": {"workload": "Landau FACG theta<1e-14, %s" % "x".join(map(str, dims)),
+        "data": "synthetic: %d configurations per step, %s (generated on the GPU "
+                "before timing)" % (E_CONFIGS, (INPUT_NAME % 2).replace(
+                    "seed 2", "seeds 2 + %d rank .. 5 + %d rank" % (E_CONFIGS, E_CONFIGS))),
+        "config": {"workload": "Landau FACG theta<1e-14, %s, %d configurations per step"
+                               % ("x".join(map(str, dims)), E_CONFIGS),
                    "dims": list(dims), "gf_alpha": ALPHA, "accuracy": ACC,
                    "precision": prec, "switch_theta": 1e-9 if prec == "mixed" else None,
-                   "iters": o["iters"][-1], "iters_fp32": it32,
-                   "final_theta": o["theta"],
-                   "fp64_only": {"value": world * steps * 3600e3 / res["out"]["fp64"]["ms"],
-                                 "ms_per_step": res["out"]["fp64"]["ms"] / steps,
-                                 "iters": res["out"]["fp64"]["iters"][-1],
-                                 "e2e": world * steps * 3600e3 / res["out"]["fp64"]["e2e_ms"]},
-                   "l2": "inputs (%.2f GB of links) larger than the 126 MB L2" % (V * 576 / 1e9),
+                   "iters_per_config": [x[0] for x in o["per"]],
+                   "iters_fp32_per_config": [x[1] for x in o["per"]],
+                   "final_theta_max": max(x[2] for x in o["per"]),
+                   "ms_per_config": ms_step / E_CONFIGS,
+                   "fp64_only": {"value": nfix * 3600e3 / o64["ms"],
+                                 "ms_per_step": o64["ms"] / steps,
+                                 "iters_per_config": [x[0] for x in o64["per"]],
+                                 "e2e": nfix * 3600e3 / o64["e2e_ms"]},
+                   "l2": "inputs (%.2f GB of links each) larger than the 126 MB L2" % (V * 576 / 1e9),
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": V * 576,
-                "d2h_bytes_per_step": V * 576},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": E_CONFIGS * V * 576,
+                "d2h_bytes_per_step": E_CONFIGS * V * 576},
         "roofline": {"bound": "hbm", "kernel": f"{KERNELS[k]} ({tag})",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src,
@@ -432,7 +468,10 @@ def profile_only(args, dims):
     from glu_b200 import _lib
     from glu_b200._lib import check
     lib = _lib.load()
-    U = workload(dims, 0)
+    # the per-iteration kernel costs do not depend on the configuration: the
+    # tiled stand-in keeps this launch list short (no heatbath generation)
+    from glu_b200.workload import tiled_config
+    U = tiled_config(dims, seed=2)
     d = torch.from_numpy(U.view(np.float64).reshape(-1)).to("cuda")
     cd = (C.c_size_t * 4)(*dims)
     ms = np.zeros(7)
@@ -1415,15 +1454,18 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            n_ref, _ = reference_iters(dims)
+            n_ref = reference_iters(dims)
             s = cpu_sample(U, dims, args.cpu_sample_s, os.cpu_count() or 1)
-            n_full = n_ref or res["out"]["fp64"]["iters"][-1]
-            t_fix = s["fixed_s"] + s["s_iter"] * n_full
-            cpu = {"value": 3600.0 / t_fix, "unit": UNIT, "cores": s["cores"],
+            src = "GLU's recorded full fixes"
+            if n_ref is None:  # our FP64 counts stand in for GLU's
+                n_ref = [x[0] for x in res["out"]["fp64"]["per"]]
+                src = "our FP64 fixes' counts"
+            t_set = E_CONFIGS * s["fixed_s"] + s["s_iter"] * sum(n_ref)
+            cpu = {"value": E_CONFIGS * 3600.0 / t_set, "unit": UNIT, "cores": s["cores"],
                    "kind": s["kind"],
-                   "sample": "%d FACG iterations (%.1f s); %.3f s/iteration x %d "
-                             "iterations of a full fix; FFT stand-in %.3f thread-s/iteration"
-                             % (s["sample_iters"], s["sample_s"], s["s_iter"], n_full,
+                   "sample": "%d FACG iterations (%.1f s); %.3f s/iteration x %s "
+                             "iterations (%s); FFT stand-in %.3f thread-s/iteration"
+                             % (s["sample_iters"], s["sample_s"], s["s_iter"], n_ref, src,
                                 s["fft_thread_s_iter"])}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "kind": "unavailable", "sample": str(e)}

@@ -107,7 +107,34 @@ struct Params {
   int algo = GFIX_CG, sd_fixed = 0;
   double *traj_theta = nullptr, *traj_func = nullptr;
   size_t traj_cap = 0;
+  // stall rule (DevState), set for mixed-precision FP32 phases only
+  long long stall_window = 0;
+  double stall_floor = 0.0, blowup = 0.0;
 };
+
+// The FP32 phase of a mixed-precision solve hands over to FP64 at
+// switch_theta, or earlier when it stops making progress: on thermalised
+// fields theta crosses long plateaus on which FP32 arithmetic can lose the
+// ground it had gained (theta jumping by orders of magnitude), so once the
+// best theta is below 1e-4 the phase ends after 15 iterations without a
+// 10% improvement or on a jump above 30x the best (the window of the best
+// mean over four beta 6.0 heatbath configurations of 32^3x64 among 15, 25
+// and 40; on smoothly converging inputs the rule never fires).
+// GLU_GFIX_STALL="window,floor,blowup" overrides it ("0": switch at
+// switch_theta only).
+static void stall_rule(Params &p) {
+  p.stall_window = 15;
+  p.stall_floor = 1e-4;
+  p.blowup = 30.0;
+  if (const char *e = getenv("GLU_GFIX_STALL")) {
+    long long w = 0;
+    double f = 0.0, b = 0.0;
+    const int n = sscanf(e, "%lld,%lf,%lf", &w, &f, &b);
+    p.stall_window = n >= 1 ? w : 0;
+    if (n >= 2) p.stall_floor = f;
+    if (n >= 3) p.blowup = b;
+  }
+}
 
 template <typename R>
 class Engine {
@@ -645,6 +672,10 @@ class Engine {
     // FP32 phase keeps its line search down to the precision switch
     st.cg_tol = 5E-11;
     st.hp_below = 1E-5;
+    st.best_tr = 1e300;
+    st.stall_window = p.stall_window;
+    st.stall_floor = p.stall_floor;
+    st.blowup = p.blowup;
     st.traj_cap = p.traj_cap ? (long long)p.traj_cap : 0;
     st.traj_theta = p.traj_cap ? d_traj : nullptr;
     st.traj_func = p.traj_cap ? d_traj + p.traj_cap : nullptr;
@@ -1322,6 +1353,7 @@ static int landau_staged(Engine<double> *e64, const gfix_params *gp,
     LAUNCHED(2);
     Params p32 = p;
     p32.acc = std::max(gp->switch_theta, gp->accuracy);
+    stall_rule(p32);
     size_t it32 = 0;
     double th32 = 0.0;
     if (e32->solve(p32, &it32, &th32)) return -1;
@@ -1534,6 +1566,7 @@ static int batch_run(Batch *b) {
     }
     Params p32 = p64;
     p32.acc = std::max(b->p.switch_theta, b->p.accuracy);
+    stall_rule(p32);
     if (batch_solve(e32, p32, it32, th32, b->bs)) return -1;
     for (size_t i = 0; i < n; i++) {
       int restart = 0;

@@ -66,6 +66,11 @@ struct DevState {
   int sd_fixed;       // GLU_GFIX_SD: fixed step gf_alpha in SD steps
   double cg_tol;      // CG_TOL (GLU_definitions.h:451-455)
   double hp_below;    // FP32 storage: probes in FP64 arithmetic once tr < this
+  // stall rule of a mixed-precision FP32 phase (stall_window 0: off): once
+  // the best theta is below stall_floor, the run ends when theta has not
+  // improved on it by 10% for stall_window iterations or exceeds blowup x it
+  double best_tr, stall_floor, blowup;
+  long long since_best, stall_window;
 };
 
 // which arithmetic variant of a kernel runs this step (FP32 storage: FP32
@@ -443,6 +448,17 @@ __global__ void __launch_bounds__(kScalarThreads)
         // the top of a loop iteration zeroes GLU's reduction slots
         st->ls_last[0] = st->ls_last[1] = 0.0;
         st->stop = !((st->tr > st->acc) && (st->iter + 1 < st->max_iters));
+        if (st->stall_window > 0) {
+          if (st->tr < 0.9 * st->best_tr) {
+            st->best_tr = st->tr;
+            st->since_best = 0;
+          } else {
+            st->since_best++;
+          }
+          if (st->best_tr < st->stall_floor &&
+              (st->since_best >= st->stall_window || st->tr > st->blowup * st->best_tr))
+            st->stop = 1;
+        }
       }
       break;
     }
