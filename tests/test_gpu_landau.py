@@ -165,6 +165,29 @@ def test_mixed_precision_reaches_fp64_accuracy(hb8):
     assert abs(fn - gfix.gauge_functional(r64.links, d)) < 1e-8
 
 
+def test_mixed_precision_on_a_thermalised_configuration(monkeypatch):
+    """A genuine beta 6.0 heatbath configuration (16^3x32, generated on the
+    GPU): theta crosses a plateau, on which the FP32 phase hands over by the
+    stall rule; both the default rule and the threshold-only switch reach
+    theta < 1e-14 on the input's gauge orbit."""
+    from glu_b200.workload import heatbath_config
+    d = (16, 16, 16, 32)
+    U = heatbath_config(d, seed=7, iterations=300)
+    plaq = gfix.av_plaquette(U, d)
+    for stall in (None, "0"):
+        if stall is None:
+            monkeypatch.delenv("GLU_GFIX_STALL", raising=False)
+        else:
+            monkeypatch.setenv("GLU_GFIX_STALL", stall)
+        r = gfix.landau_fix(U, d, 0.08, 1e-14, 20000, "FACG", precision="MIXED",
+                            switch_theta=1e-9)
+        assert r.iters != gfix.SENTINEL
+        assert r.theta < 1e-14
+        assert 0 < r.iters_fp32 < r.iters
+        assert abs(gfix.av_plaquette(r.links, d) - plaq) < 1e-12
+        assert gfix.observables(r.links, d)[0] < 1e-13
+
+
 def test_nonconvergence_sentinel(lat400):
     g = lat400
     r = gfix.landau_fix(g["links"], _dims(g), 0.08, 1e-14, 4, "FACG")
