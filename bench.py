@@ -22,8 +22,9 @@ fixes its own set: weak scaling, no collective on the data path.
 
 The reference arm (--impl reference) times GLU itself, compiled from its
 sources (oracle/_ref), on the host cores: a bounded sample of FACG
-iterations on the first configuration, scaled by the iteration counts of
-GLU's full fixes of the four (profiles/reference_full_fix.json).
+iterations (on the host-built tiled stand-in: the cost of an iteration does
+not depend on the configuration), scaled by the iteration counts of GLU's
+full fixes of the four configurations (profiles/reference_full_fix.json).
 """
 from __future__ import annotations
 
@@ -360,7 +361,12 @@ def emit(d):
 def reference_arm(args, dims, rank, world):
     if rank != 0:
         return
-    U = workload(dims, 0)
+    # GLU's per-iteration cost does not depend on the configuration: it is
+    # sampled on the tiled stand-in (built on the host, so this arm loads
+    # nothing of ours), the iteration counts are those of GLU's own full
+    # fixes of the heatbath configurations
+    from glu_b200.workload import tiled_config
+    U = tiled_config(dims, seed=2)
     n_ref = reference_iters(dims)
     cores = os.cpu_count() or 1
     for _ in range(max(args.warmup, 0) and 1):
