@@ -888,16 +888,28 @@ def e_metric_name() -> str:
             "Landau FASD, theta<1e-12)")
 
 
-def ensemble_configs(rank: int = 0):
-    """(dims, links) per configuration: the 8^4 heatbath stand-in tiled to
-    the shape, each with its own seeded gauge transformation (seeds
-    100..163, offset by 64 per rank)."""
-    from glu_b200.workload import tiled_config
-    out, seed = [], 100 + 64 * rank
+E_HB_ITERS = 500  # heatbath steps (1 HB + 4 OR) generating each configuration
+
+
+def ensemble_configs(rank: int = 0, tiled: bool = False):
+    """(dims, links) per configuration: heatbath configurations generated on
+    the GPU, beta spread evenly over 5.9 .. 6.1 across the 64, seeds
+    100..163 (offset by 64 per rank), E_HB_ITERS steps of one heatbath and
+    four over-relaxation sweeps from the unit start.  tiled: the host-built
+    stand-in of the same shapes (the 8^4 heatbath configuration tiled, with
+    a seeded gauge transformation), for timing the reference's iterations,
+    whose cost does not depend on the configuration."""
+    from glu_b200.workload import heatbath_config, tiled_config
+    ntot = sum(n for n, _ in E_GROUPS)
+    out, k = [], 0
     for n, dims in E_GROUPS:
         for _ in range(n):
-            out.append((dims, tiled_config(dims, seed=seed)))
-            seed += 1
+            seed = 100 + 64 * rank + k
+            beta = 5.9 + 0.2 * k / (ntot - 1)
+            U = (tiled_config(dims, seed=seed) if tiled else
+                 heatbath_config(dims, seed=seed, iterations=E_HB_ITERS, beta=beta))
+            out.append((dims, U))
+            k += 1
     return out
 
 
@@ -914,7 +926,7 @@ def ensemble_main(args, rank, world, local):
     if args.impl == "reference":
         if rank != 0:
             return
-        cfgs = ensemble_configs(0)
+        cfgs = ensemble_configs(0, tiled=True)
         rec = ensemble_iters_record()
         if rec is None:
             emit({"impl": "reference", "unavailable":
@@ -1025,7 +1037,8 @@ def ensemble_main(args, rank, world, local):
         "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": args.warmup,
         "ms_per_step": o["ms"] / steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64" if prec == "mixed" else "f64",
-        "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled to each shape + seeded random gauge transforms, seeds 100-163)",
+        "data": "synthetic: heatbath configurations generated on the GPU before timing, "
+                "beta 5.9-6.1, seeds 100-163, %d x (HB + 4 OR) from the unit start" % E_HB_ITERS,
         "config": {"workload": "ensemble 48x16^3x32 + 16x24^3x48 Landau FASD theta<1e-12",
                    "configs": n, "sites": sites, "precision": prec,
                    "switch_theta": 1e-9 if prec == "mixed" else None,
@@ -1035,6 +1048,11 @@ def ensemble_main(args, rank, world, local):
                    "fp64_only": {"value": world * n * steps * 3600e3 / out["fp64"]["device"]["ms"],
                                  "ms_per_step": out["fp64"]["device"]["ms"] / steps,
                                  "iters_total": sum(x[0] for x in out["fp64"]["device"]["iters"]),
+                                 "iters_by_group": {
+                                     str(d[0]): sum(x[0] for x, (dd, _) in
+                                                    zip(out["fp64"]["device"]["iters"], cfgs)
+                                                    if dd == d)
+                                     for _, d in E_GROUPS},
                                  "e2e": world * n * steps * 3600e3 / out["fp64"]["host"]["ms"]},
                    "l2": "inputs (%.2f GB of links) larger than the 126 MB L2" % (nbytes / 1e9),
                    "parallelism": "one batch per GPU" if world > 1 else "single GPU, one batch"},
