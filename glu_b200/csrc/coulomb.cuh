@@ -40,6 +40,8 @@ struct Slice {
   int bad;            // set when the unitarity check fails
   int trans;          // GLU's trans_flag: survives a continuation run
   int traj_len;
+  double best_tr;     // stall rule (mixed-precision FP32 phase)
+  long long since_best;
 };
 
 struct CoulState {
@@ -55,6 +57,12 @@ struct CoulState {
   int *done_mask;     // [nslices], 1 once a slice has finished (FFT passes skip it)
   double prec_tol;    // PREC_TOL of the unitarity check
   double hp_below;    // FP32 storage: FP64 arithmetic for slices below this theta
+  // stall rule of a mixed-precision FP32 phase (stall_window 0: off): a
+  // slice whose best theta is below stall_floor ends its run after
+  // stall_window iterations without a 10% improvement on it, or on a jump
+  // above blowup x it; the FP64 phase then continues it
+  long long stall_window;
+  double stall_floor, blowup;
 };
 
 template <typename R>
@@ -443,6 +451,19 @@ __global__ void k_cscalar(CoulState *cs, Slice *sl, const double *part,
             break;
           }
           S.iter++;
+          if (cs->stall_window > 0 && S.tr > cs->acc) {
+            if (S.tr < 0.9 * S.best_tr) {
+              S.best_tr = S.tr;
+              S.since_best = 0;
+            } else {
+              S.since_best++;
+            }
+            if (S.best_tr < cs->stall_floor &&
+                (S.since_best >= cs->stall_window || S.tr > cs->blowup * S.best_tr)) {
+              S.sd = -1;  // ends the run, no restart: the FP64 phase goes on
+              break;
+            }
+          }
           if ((S.tr > cs->acc) && (S.iter < cs->max_iters)) break;
           S.reunit = S.tr < cs->acc;  // run ended: adequate_solution first
           S.sd = -1;                  // marks "ended" for C_END2

@@ -1024,6 +1024,9 @@ class Engine {
     // rounding of FP32 rotated links slows the slices' convergence (measured
     // on 32^3x64 and 64^3x128 slices), unlike the Landau probes (1e-5)
     cst.hp_below = 1E-2;
+    cst.stall_window = p.stall_window;
+    cst.stall_floor = p.stall_floor;
+    cst.blowup = p.blowup;
     CK(cudaMemsetAsync(d_cmask, 0, sizeof(int) * T, s));
     CK(cudaMemcpyAsync(d_cst, &cst, sizeof cst, cudaMemcpyHostToDevice, s));
     std::vector<Slice> sl(T);
@@ -1031,6 +1034,7 @@ class Engine {
     for (auto &x : sl) {
       x.sd = 1;
       x.mode = SL_RUN;
+      x.best_tr = 1e300;
     }
     CK(cudaMemcpyAsync(d_sl, sl.data(), sizeof(Slice) * T,
                        cudaMemcpyHostToDevice, s));
@@ -1904,6 +1908,7 @@ static int coulomb_staged(Engine<double> *e, const gfix_params *gp,
     p32.acc = gp->switch_theta;
     p32.traj_cap = 0;
     p32.traj_theta = p32.traj_func = nullptr;
+    stall_rule(p32);  // per slice (FACG)
     if (f->csolve(p32, &n32, th32.data(), it32.data(), nullptr, true, 0))
       return -1;
     bool finite = true;
