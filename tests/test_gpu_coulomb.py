@@ -209,6 +209,27 @@ def test_mixed_precision_reaches_fp64_accuracy(case, request):
     assert abs(fs(r.links) - fs(r64.links)) < 1e-13
 
 
+def test_mixed_precision_on_a_thermalised_configuration(monkeypatch):
+    """A genuine beta 6.0 heatbath configuration (16^3x32, generated on the
+    GPU): slices stuck on a theta plateau in FP32 hand over to FP64 by the
+    per-slice stall rule; with it and without it every slice reaches
+    theta < 1e-14 on the input's gauge orbit."""
+    from glu_b200.workload import heatbath_config
+    d = (16, 16, 16, 32)
+    U = heatbath_config(d, seed=9, iterations=300)
+    p0 = gfix.observables(U, d)[2]
+    for stall in (None, "0"):
+        if stall is None:
+            monkeypatch.delenv("GLU_GFIX_STALL", raising=False)
+        else:
+            monkeypatch.setenv("GLU_GFIX_STALL", stall)
+        r = gfix.coulomb_fix(U, d, 0.08, ACC, 20000, "FACG", precision="MIXED",
+                             switch_theta=1e-9)
+        assert np.all(r.slice_theta < ACC)
+        assert 0 < r.iters_fp32 < r.iters
+        assert abs(gfix.observables(r.links, d)[2] - p0) < 1e-12
+
+
 @pytest.mark.parametrize("blocks", [[(0, 4), (4, 8)], [(0, 2), (2, 5), (5, 8)]])
 def test_slice_blocks_equal_whole_lattice(lat400, blocks):
     """gfix_coulomb_slices on blocks of slices (one per rank in a sharded
