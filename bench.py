@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--dims", default=None,
                     help="lattice extents; default 32,32,32,64 (landau) or "
                          "64,64,64,128 (coulomb)")
+    ap.add_argument("--beta", type=float, default=6.0,
+                    help="landau: coupling of the generated heatbath inputs")
+    ap.add_argument("--configs", type=int, default=4,
+                    help="landau: configurations fixed per step")
     ap.add_argument("--profile-iters", type=int, default=20)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -150,6 +154,16 @@ def dist_env():
 H_INPUT = dict(beta=6.0, iterations=1000, n_or=4)
 INPUT_NAME = "heatbath beta 6.0, 1000 x (HB + 4 OR), unit start, seed %d"
 E_CONFIGS = 4
+
+
+def set_input(beta: float, configs: int):
+    """--beta / --configs of the Landau workload (defaults 6.0, 4)"""
+    global INPUT_NAME, E_CONFIGS
+    H_INPUT["beta"] = beta
+    INPUT_NAME = "heatbath beta %g, 1000 x (HB + 4 OR), unit start, seed %%d" % beta
+    if beta == 6.0:
+        INPUT_NAME = "heatbath beta 6.0, 1000 x (HB + 4 OR), unit start, seed %d"
+    E_CONFIGS = max(1, int(configs))
 
 
 def seeds(rank):
@@ -388,7 +402,8 @@ def reference_arm(args, dims, rank, world):
           "ms_per_step": t_set * 1e3, "higher_is_better": True,
           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
           "data": "synthetic: %d configurations, %s (generated on the GPU)"
-                  % (E_CONFIGS, (INPUT_NAME % 2).replace("seed 2", "seeds 2..5")),
+                  % (E_CONFIGS, (INPUT_NAME % 2).replace(
+                      "seed 2", "seeds 2..%d" % (1 + E_CONFIGS))),
           "config": {"workload": "Landau FACG theta<1e-14, %s, %d configurations per step"
                                  % ("x".join(map(str, dims)), E_CONFIGS),
                      "dims": list(dims), "gf_alpha": ALPHA, "accuracy": ACC,
@@ -437,7 +452,8 @@ def gpu_line(args, dims, world, res, cpu):
         "dtype": "f32+f64" if prec == "mixed" else "f64",
         "data": "synthetic: %d configurations per step, %s (generated on the GPU "
                 "before timing)" % (E_CONFIGS, (INPUT_NAME % 2).replace(
-                    "seed 2", "seeds 2 + %d rank .. 5 + %d rank" % (E_CONFIGS, E_CONFIGS))),
+                    "seed 2", "seeds 2 + %d rank .. %d + %d rank"
+                    % (E_CONFIGS, 1 + E_CONFIGS, E_CONFIGS))),
         "config": {"workload": "Landau FACG theta<1e-14, %s, %d configurations per step"
                                % ("x".join(map(str, dims)), E_CONFIGS),
                    "dims": list(dims), "gf_alpha": ALPHA, "accuracy": ACC,
@@ -1468,6 +1484,7 @@ def main():
     if args.workload == "heatbath":
         heatbath_main(args, dims, rank, world, local)
         return
+    set_input(args.beta, args.configs)
     if args.profile_only:
         profile_only(args, dims)
         return
