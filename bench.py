@@ -15,10 +15,11 @@ report the plain FP64 path beside it.
 Input: beta 6.0 heatbath configurations generated on the GPU before any
 timed region (glu_b200.workload.heatbath_config: GLU's heatbath algorithm,
 1000 iterations of one heatbath and four over-relaxation sweeps from the unit
-start).  A step fixes four of them (seeds 2..5; rank r: 2 + 4r ..): on
-thermalised fields the iteration count of a fix varies twofold between
-configurations, so the throughput is that of a set.  At N > 1 every rank
-fixes its own set: weak scaling, no collective on the data path.
+start).  A step fixes four of them (seeds 2..5): on thermalised fields the
+iteration count of a fix varies twofold between configurations, so the
+throughput is that of a set.  At N > 1 every rank fixes the same set on its
+own GPU (the same work per GPU): weak scaling, no collective on the data
+path.
 
 The reference arm (--impl reference) times GLU itself, compiled from its
 sources (oracle/_ref), on the host cores: a bounded sample of FACG
@@ -148,9 +149,10 @@ def dist_env():
 # the input of the Landau workload: beta 6.0 heatbath configurations, 1000
 # iterations of one heatbath and four over-relaxation sweeps from the unit
 # start, generated on the GPU before any timed region.  One step fixes
-# E_CONFIGS of them (seeds 2 + E_CONFIGS rank + i): the iteration count of a
+# E_CONFIGS of them (seeds 2 .. 1 + E_CONFIGS): the iteration count of a
 # fix on a thermalised configuration varies twofold between configurations
-# (and between summation orders), so throughput is measured over a set.
+# (and between summation orders), so throughput is measured over a set,
+# the same set on every rank.
 H_INPUT = dict(beta=6.0, iterations=1000, n_or=4)
 INPUT_NAME = "heatbath beta 6.0, 1000 x (HB + 4 OR), unit start, seed %d"
 E_CONFIGS = 4
@@ -167,7 +169,10 @@ def set_input(beta: float, configs: int):
 
 
 def seeds(rank):
-    return [2 + E_CONFIGS * rank + i for i in range(E_CONFIGS)]
+    """every rank fixes the same configurations: with iteration counts that
+    vary twofold between configurations, distinct sets per rank would make
+    the slowest rank's set, not the hardware, set a weak-scaling step"""
+    return [2 + i for i in range(E_CONFIGS)]
 
 
 def workload(dims, rank, i=0):
@@ -452,8 +457,7 @@ def gpu_line(args, dims, world, res, cpu):
         "dtype": "f32+f64" if prec == "mixed" else "f64",
         "data": "synthetic: %d configurations per step, %s (generated on the GPU "
                 "before timing)" % (E_CONFIGS, (INPUT_NAME % 2).replace(
-                    "seed 2", "seeds 2 + %d rank .. %d + %d rank"
-                    % (E_CONFIGS, 1 + E_CONFIGS, E_CONFIGS))),
+                    "seed 2", "seeds 2..%d on every rank" % (1 + E_CONFIGS))),
         "config": {"workload": "Landau FACG theta<1e-14, %s, %d configurations per step"
                                % ("x".join(map(str, dims)), E_CONFIGS),
                    "dims": list(dims), "gf_alpha": ALPHA, "accuracy": ACC,
