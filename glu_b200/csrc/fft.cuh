@@ -251,6 +251,36 @@ __device__ void smem_fft(cx<R> *buf, const PencilMap &m, const FftAxis &ax,
 __host__ __device__ constexpr int ct_radix(int m) {
   return (m % 8 == 0) ? 8 : (m % 4 == 0) ? 4 : (m % 2 == 0) ? 2 : 3;
 }
+// radix of the last stage of a length m (the first of the mirrored order)
+__host__ __device__ constexpr int ct_radix_last(int m) {
+  int r = ct_radix(m);
+  while (m / r > 1) {
+    m /= r;
+    r = ct_radix(m);
+  }
+  return r;
+}
+// number of stages of a length n
+__host__ __device__ constexpr int ct_nstages(int n) {
+  int k = 0;
+  while (n > 1) {
+    n /= ct_radix(n);
+    k++;
+  }
+  return k;
+}
+// the mirrored order (radix ct_radix_last of the remaining length at each
+// stage) is the forward radix sequence reversed
+__host__ __device__ constexpr bool ct_mirror_ok(int n) {
+  int fwd[kMaxStages] = {}, k = 0;
+  for (int m = n; m > 1 && k < kMaxStages; m /= fwd[k++]) fwd[k] = ct_radix(m);
+  int ns = 1;
+  for (int i = k - 1; i >= 0; i--) {
+    if (ct_radix_last(n / ns) != fwd[i]) return false;
+    ns *= fwd[i];
+  }
+  return ns == n;
+}
 // can the extent be transformed by the compile-time stages?
 __host__ __device__ constexpr bool ct_ok(int n) {
   while (n % 2 == 0) n /= 2;
@@ -263,12 +293,15 @@ __host__ __device__ constexpr bool ct_ok(int n) {
 // Consecutive threads take consecutive pencils at the same butterfly index:
 // their elements are neighbours in shared memory (no bank conflicts for the
 // tile layouts below) and they share one twiddle factor (a broadcast).
+// The stages run from Ns up to (not including) END; MIR selects the
+// mirrored radix order (any order of the radices is a valid Stockham
+// sequence: the twiddle of a stage depends only on Ns and its radix).
 template <typename R, int N, int Ns, int NP, int PIN, int PSLO, int PSHI,
-          int JS, int BD>
+          int JS, int BD, bool MIR = false, int END = N>
 __device__ __forceinline__ void ct_stages(cx<R> *buf, const cx<R> *tw,
                                           bool bwd) {
-  if constexpr (Ns < N) {
-    constexpr int RDX = ct_radix(N / Ns);
+  if constexpr (Ns < END) {
+    constexpr int RDX = MIR ? ct_radix_last(N / Ns) : ct_radix(N / Ns);
     constexpr int NB = N / RDX;
     constexpr int TOTAL = NP * NB;
     constexpr int K = (TOTAL + BD - 1) / BD;
@@ -302,8 +335,96 @@ __device__ __forceinline__ void ct_stages(cx<R> *buf, const cx<R> *tw,
       }
     }
     __syncthreads();
-    ct_stages<R, N, Ns * RDX, NP, PIN, PSLO, PSHI, JS, BD>(buf, tw, bwd);
+    ct_stages<R, N, Ns * RDX, NP, PIN, PSLO, PSHI, JS, BD, MIR, END>(buf, tw,
+                                                                    bwd);
   }
+}
+
+// One Stockham stage (length N, product of the earlier radices Ns, radix
+// RDX) over NP pencils whose element i is read by ld(p, i) and written by
+// st(p, i, value): the first stage of a pass reading its pencils from
+// global memory, or the last one writing them there.  No barrier between
+// the loads and the stores (source and destination differ); AFTER puts one
+// after the stores.
+template <typename R, int N, int Ns, int RDX, int NP, int BD, bool AFTER,
+          class Ld, class St>
+__device__ __forceinline__ void ct_stage_io(const cx<R> *tw, bool bwd, Ld ld,
+                                            St st) {
+  constexpr int NB = N / RDX;
+  constexpr int TOTAL = NP * NB;
+  constexpr int K = (TOTAL + BD - 1) / BD;
+  constexpr int STEP0 = N / (Ns * RDX);
+  cx<R> v[K][RDX];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const int idx = threadIdx.x + k * BD;
+    if (TOTAL % BD == 0 || idx < TOTAL) {
+      const int p = idx % NP, j = idx / NP;
+      const int jq = j / Ns, jm = j % Ns;
+#pragma unroll
+      for (int s = 0; s < RDX; s++) v[k][s] = ld(p, j + s * NB);
+#pragma unroll
+      for (int s = 1; s < RDX; s++)
+        if constexpr (Ns > 1) v[k][s] = cmul(v[k][s], twiddle(tw, s * jm * STEP0, bwd));
+      dft_reg<R, RDX>(v[k], tw, N, bwd);
+#pragma unroll
+      for (int s = 0; s < RDX; s++) st(p, jq * Ns * RDX + jm + s * Ns, v[k][s]);
+    }
+  }
+  if constexpr (AFTER) __syncthreads();
+}
+
+// The last forward stage of a length N, a scale sc(p, i) of every output
+// element and the first backward stage of the mirrored radix order, in
+// registers: the forward stage leaves element j + s * N / RL of each pencil
+// with the thread that the mirrored backward stage (radix RL, Ns = 1) reads
+// it from, so the pair costs one shared-memory round trip instead of three
+// (two stages and the scaling pass).
+// a product rounded on its own (never contracted into a following add), so
+// that a scale applied in registers rounds as one applied in a separate pass
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
+template <typename R, int N, int NP, int PIN, int PSLO, int PSHI, int JS,
+          int BD, class Sc>
+__device__ __forceinline__ void ct_mid(cx<R> *buf, const cx<R> *tw, Sc sc) {
+  constexpr int RL = ct_radix_last(N);
+  constexpr int NB = N / RL;  // the forward stage's Ns
+  constexpr int TOTAL = NP * NB;
+  constexpr int K = (TOTAL + BD - 1) / BD;
+  cx<R> v[K][RL];
+  int dst[K];
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    const int idx = threadIdx.x + k * BD;
+    dst[k] = -1;
+    if (TOTAL % BD == 0 || idx < TOTAL) {
+      const int p = idx % NP, j = idx / NP;
+      const int po = (p / PIN) * PSHI + (p % PIN) * PSLO;
+#pragma unroll
+      for (int s = 0; s < RL; s++) v[k][s] = buf[po + (j + s * NB) * JS];
+#pragma unroll
+      for (int s = 1; s < RL; s++)
+        if constexpr (NB > 1) v[k][s] = cmul(v[k][s], twiddle(tw, s * j, false));
+      dft_reg<R, RL>(v[k], tw, N, false);
+#pragma unroll
+      for (int s = 0; s < RL; s++) {
+        const R f = sc(p, j + s * NB);
+        v[k][s] = mk<R>(mul_rn(v[k][s].x, f), mul_rn(v[k][s].y, f));
+      }
+      dft_reg<R, RL>(v[k], tw, N, true);
+      dst[k] = po + j * RL * JS;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    if (dst[k] >= 0) {
+#pragma unroll
+      for (int s = 0; s < RL; s++) buf[dst[k] + s * JS] = v[k][s];
+    }
+  }
+  __syncthreads();
 }
 
 // threads of a tile of n elements: one radix-8 butterfly each (32..1024

@@ -91,6 +91,57 @@ __global__ void __launch_bounds__(ct_threads(B *LZ *NT), ct_minb(B *LZ *NT))
   const int x0 = xb * B;
   const size_t sz = (size_t)Lx * Ly;
   const size_t base = (size_t)x0 + (size_t)Lx * y + sz * LZ * tslice;
+  const double D = FOUR ? 4.0 : 3.0;
+  const double cxy = c.cs[1 * c.cs_ld + y];
+  if constexpr (FOUR || ct_nstages(LZ) >= 2) {
+    // Fused form: the first forward z stage reads the columns from global
+    // memory, the last forward stage of the innermost transform (t, or z
+    // for Coulomb), psq and the first backward stage share registers (the
+    // backward stages of that transform run in the mirrored radix order),
+    // and the last backward z stage writes global memory.  z pencil p:
+    // column b = p % B of t-plane p / B; t pencil p: column b = p % B at
+    // z = p / B.
+    static_assert(ct_mirror_ok(LZ) && ct_mirror_ok(NT), "radix order");
+    constexpr int NPZ = NT * B, R1 = ct_radix(LZ), RLZ = ct_radix_last(LZ);
+    auto gidx = [&](int p, int z) {
+      return base + (p % B) + sz * (z + LZ * (p / B));
+    };
+    auto sidx = [&](int p, int z) { return (p / B) * TS + (p % B) + z * B; };
+    auto psq = [&](int b, int z, int t) -> R {
+      double kcos = 0.0;
+      kcos += c.cs[x0 + b];
+      kcos += cxy;
+      kcos += c.cs[2 * c.cs_ld + z];
+      if constexpr (FOUR) kcos += c.cs[3 * c.cs_ld + t];
+      const double p2 = (kcos == D) ? 1.0 : 2.0 * (D - kcos);
+      return (R)(c.maxp * __drcp_rn(p2));
+    };
+    __syncthreads();  // twiddles staged
+    ct_stage_io<R, LZ, 1, R1, NPZ, BD, true>(
+        twz, false, [&](int p, int z) { return data[gidx(p, z)]; },
+        [&](int p, int z, cx<R> v) { A[sidx(p, z)] = v; });
+    if constexpr (FOUR) {
+      constexpr int RLT = ct_radix_last(NT);
+      ct_stages<R, LZ, R1, NPZ, B, 1, TS, B, BD>(A, twz, false);
+      ct_stages<R, NT, 1, LZ * B, LZ * B, 1, 0, TS, BD, false, NT / RLT>(A, twt, false);
+      ct_mid<R, NT, LZ * B, LZ * B, 1, 0, TS, BD>(
+          A, twt, [&](int p, int t) { return psq(p % B, p / B, t); });
+      ct_stages<R, NT, RLT, LZ * B, LZ * B, 1, 0, TS, BD, true>(A, twt, true);
+      ct_stages<R, LZ, 1, NPZ, B, 1, TS, B, BD, false, LZ / RLZ>(A, twz, true);
+      ct_stage_io<R, LZ, LZ / RLZ, RLZ, NPZ, BD, false>(
+          twz, true, [&](int p, int z) { return A[sidx(p, z)]; },
+          [&](int p, int z, cx<R> v) { data[gidx(p, z)] = v; });
+    } else {
+      ct_stages<R, LZ, R1, NPZ, B, 1, TS, B, BD, false, LZ / RLZ>(A, twz, false);
+      ct_mid<R, LZ, NPZ, B, 1, TS, B, BD>(
+          A, twz, [&](int p, int z) { return psq(p % B, z, 0); });
+      ct_stages<R, LZ, RLZ, NPZ, B, 1, TS, B, BD, true, LZ / R1>(A, twz, true);
+      ct_stage_io<R, LZ, LZ / R1, R1, NPZ, BD, false>(
+          twz, true, [&](int p, int z) { return A[sidx(p, z)]; },
+          [&](int p, int z, cx<R> v) { data[gidx(p, z)] = v; });
+    }
+    return;
+  }
 #pragma unroll
   for (int k = 0; k < EPT; k++) {
     const int e = threadIdx.x + k * BD;
@@ -102,8 +153,6 @@ __global__ void __launch_bounds__(ct_threads(B *LZ *NT), ct_minb(B *LZ *NT))
   __syncthreads();
   ct_stages<R, LZ, 1, NT * B, B, 1, TS, B, BD>(A, twz, false);
   if constexpr (FOUR) ct_stages<R, NT, 1, LZ * B, LZ * B, 1, 0, TS, BD>(A, twt, false);
-  const double D = FOUR ? 4.0 : 3.0;
-  const double cxy = c.cs[1 * c.cs_ld + y];
 #pragma unroll
   for (int k = 0; k < EPT; k++) {
     const int e = threadIdx.x + k * BD;

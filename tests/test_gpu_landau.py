@@ -39,7 +39,7 @@ def test_observables_match_oracle(oracle, case, request):
 
 
 @pytest.mark.parametrize("dims", [(4, 4, 4, 8), (8, 6, 4, 12), (6, 10, 5, 3),
-                                  (8, 8, 48, 96)])
+                                  (8, 8, 48, 96), (8, 8, 32, 64)])
 def test_fourier_accelerate_matches_oracle(oracle, dims):
     rng = np.random.default_rng(7)
     V = int(np.prod(dims))
@@ -49,7 +49,8 @@ def test_fourier_accelerate_matches_oracle(oracle, dims):
     assert np.abs(got - ref).max() < 1e-13 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize("dims", [(4, 4, 4, 8), (16, 8, 32, 2), (6, 10, 5, 3)])
+@pytest.mark.parametrize("dims", [(4, 4, 4, 8), (16, 8, 32, 2), (6, 10, 5, 3),
+                                  (16, 16, 64, 2), (16, 16, 48, 2)])
 def test_fourier_accelerate3_matches_oracle(oracle, dims):
     """FOURIER_ACCELERATE2 (one time slice, MAX_COULOMB / p^2 in 3D)."""
     rng = np.random.default_rng(8)
