@@ -1,0 +1,64 @@
+"""The JSON line of ``bench.py --impl reference`` (GLU's Landau FACG on the host
+cores), run as a short subprocess on the CPU: every key of the bench line, a
+positive throughput, the reference arm's own ``cpu_baseline`` and a zero-copy
+``e2e``; and a non-zero rank of a multi-rank launch exits 0 without a line.
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+
+from conftest import ROOT, _ensure_oracle
+
+ARGS = ["--impl", "reference", "--steps", "1", "--warmup", "0",
+        "--cpu-sample-s", "0.5"]
+
+
+def _run(env_extra=None):
+    env = dict(os.environ)
+    env.pop("RANK", None)
+    env.pop("WORLD_SIZE", None)
+    env.update(env_extra or {})
+    return subprocess.run([sys.executable, str(ROOT / "bench.py"), *ARGS],
+                          cwd=ROOT, env=env, capture_output=True, text=True,
+                          timeout=240)
+
+
+def _lines(out: str):
+    return [json.loads(s) for s in out.splitlines() if s.startswith("{")]
+
+
+def test_reference_arm_line():
+    _ensure_oracle()
+    r = _run()
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = _lines(r.stdout)
+    assert len(lines) == 1
+    d = lines[0]
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup",
+              "ms_per_step", "higher_is_better", "scaling", "vs_baseline",
+              "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference"
+    assert d["unit"] == "configs/hour" and d["higher_is_better"] is True
+    assert d["n_gpus"] == 1 and d["steps"] == 1 and d["warmup"] == 0
+    assert d["value"] > 0 and d["ms_per_step"] > 0
+    assert "workload" in d["config"]
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["unit"] == d["unit"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1
+    assert cb["sample"]
+    e = d["e2e"]
+    assert e["value"] == d["value"] and e["unit"] == d["unit"]
+    assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+    # configs/hour and ms per step describe the same step of E configurations
+    n = len(d["config"]["full_fix_iters"])
+    assert abs(d["value"] * d["ms_per_step"] / 3.6e6 - n) < 1e-6 * n
+
+
+def test_reference_arm_other_ranks_silent():
+    r = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert _lines(r.stdout) == []
