@@ -965,8 +965,11 @@ def ensemble_main(args, rank, world, local):
               "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
               "ms_per_step": t_fix * 1e3, "higher_is_better": True,
               "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-              "data": "synthetic (8^4 GLU heatbath tiled + random gauge)",
+              "data": "synthetic: GLU's FASD cost per iteration sampled on the 8^4 GLU heatbath "
+                      "tiled + random gauge stand-in; iteration counts are the FP64 FASD counts "
+                      "recorded on the heatbath ensemble (beta 5.9-6.1, seeds 100-163)",
               "config": {"workload": "ensemble 48x16^3x32 + 16x24^3x48 Landau FASD theta<1e-12",
+                         "configs": len(cfgs), "full_fix_iters_by_group": rec,
                          "parallelism": "host OpenMP, one configuration at a time"},
               "impl": "reference",
               "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores,

@@ -1,7 +1,8 @@
-"""The JSON line of ``bench.py --impl reference`` (GLU's Landau FACG on the host
-cores), run as a short subprocess on the CPU: every key of the bench line, a
-positive throughput, the reference arm's own ``cpu_baseline`` and a zero-copy
-``e2e``; and a non-zero rank of a multi-rank launch exits 0 without a line.
+"""The JSON line of ``bench.py --impl reference`` (GLU's own solver on the host
+cores), run as a short subprocess on the CPU for the Landau FACG workload and
+the FASD ensemble: every key of the bench line, a positive throughput, the
+reference arm's own ``cpu_baseline`` and a zero-copy ``e2e``; and a non-zero
+rank of a multi-rank launch exits 0 without a line.
 """
 from __future__ import annotations
 
@@ -10,18 +11,20 @@ import os
 import subprocess
 import sys
 
+import pytest
+
 from conftest import ROOT, _ensure_oracle
 
 ARGS = ["--impl", "reference", "--steps", "1", "--warmup", "0",
         "--cpu-sample-s", "0.5"]
 
 
-def _run(env_extra=None):
+def _run(extra=(), env_extra=None):
     env = dict(os.environ)
     env.pop("RANK", None)
     env.pop("WORLD_SIZE", None)
     env.update(env_extra or {})
-    return subprocess.run([sys.executable, str(ROOT / "bench.py"), *ARGS],
+    return subprocess.run([sys.executable, str(ROOT / "bench.py"), *ARGS, *extra],
                           cwd=ROOT, env=env, capture_output=True, text=True,
                           timeout=240)
 
@@ -30,9 +33,23 @@ def _lines(out: str):
     return [json.loads(s) for s in out.splitlines() if s.startswith("{")]
 
 
-def test_reference_arm_line():
+# configurations fixed per step, from the line's config
+def _landau_n(cfg):
+    return len(cfg["full_fix_iters"])
+
+
+def _ensemble_n(cfg):
+    assert cfg["configs"] == 48 + 16
+    return cfg["configs"]
+
+
+@pytest.mark.parametrize("extra, configs_per_step", [
+    ((), _landau_n),
+    (("--workload", "ensemble"), _ensemble_n),
+], ids=["landau", "ensemble"])
+def test_reference_arm_line(extra, configs_per_step):
     _ensure_oracle()
-    r = _run()
+    r = _run(extra)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = _lines(r.stdout)
     assert len(lines) == 1
@@ -54,11 +71,11 @@ def test_reference_arm_line():
     assert e["value"] == d["value"] and e["unit"] == d["unit"]
     assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
     # configs/hour and ms per step describe the same step of E configurations
-    n = len(d["config"]["full_fix_iters"])
+    n = configs_per_step(d["config"])
     assert abs(d["value"] * d["ms_per_step"] / 3.6e6 - n) < 1e-6 * n
 
 
 def test_reference_arm_other_ranks_silent():
-    r = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
+    r = _run((), {"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert r.returncode == 0, r.stderr[-2000:]
     assert _lines(r.stdout) == []
