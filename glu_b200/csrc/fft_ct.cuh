@@ -140,43 +140,43 @@ __global__ void __launch_bounds__(ct_threads(B *LZ *NT), ct_minb(B *LZ *NT))
           twz, true, [&](int p, int z) { return A[sidx(p, z)]; },
           [&](int p, int z, cx<R> v) { data[gidx(p, z)] = v; });
     }
-    return;
-  }
+  } else {  // generic form: z (and t) stages in shared memory
 #pragma unroll
-  for (int k = 0; k < EPT; k++) {
-    const int e = threadIdx.x + k * BD;
-    if (N % BD == 0 || e < N) {
-      const int q = e / B, b = e % B, t = q / LZ, z = q % LZ;
-      A[b + B * z + TS * t] = data[base + b + sz * q];
+    for (int k = 0; k < EPT; k++) {
+      const int e = threadIdx.x + k * BD;
+      if (N % BD == 0 || e < N) {
+        const int q = e / B, b = e % B, t = q / LZ, z = q % LZ;
+        A[b + B * z + TS * t] = data[base + b + sz * q];
+      }
     }
-  }
-  __syncthreads();
-  ct_stages<R, LZ, 1, NT * B, B, 1, TS, B, BD>(A, twz, false);
-  if constexpr (FOUR) ct_stages<R, NT, 1, LZ * B, LZ * B, 1, 0, TS, BD>(A, twt, false);
+    __syncthreads();
+    ct_stages<R, LZ, 1, NT * B, B, 1, TS, B, BD>(A, twz, false);
+    if constexpr (FOUR) ct_stages<R, NT, 1, LZ * B, LZ * B, 1, 0, TS, BD>(A, twt, false);
 #pragma unroll
-  for (int k = 0; k < EPT; k++) {
-    const int e = threadIdx.x + k * BD;
-    if (N % BD != 0 && e >= N) continue;
-    const int q = e / B, b = e % B, t = q / LZ, z = q % LZ;
-    double kcos = 0.0;
-    kcos += c.cs[x0 + b];
-    kcos += cxy;
-    kcos += c.cs[2 * c.cs_ld + z];
-    if constexpr (FOUR) kcos += c.cs[3 * c.cs_ld + t];
-    const double p2 = (kcos == D) ? 1.0 : 2.0 * (D - kcos);
-    const R ps = (R)(c.maxp * __drcp_rn(p2));
-    const int o = b + B * z + TS * t;
-    A[o] = mk<R>(A[o].x * ps, A[o].y * ps);
-  }
-  __syncthreads();
-  if constexpr (FOUR) ct_stages<R, NT, 1, LZ * B, LZ * B, 1, 0, TS, BD>(A, twt, true);
-  ct_stages<R, LZ, 1, NT * B, B, 1, TS, B, BD>(A, twz, true);
-#pragma unroll
-  for (int k = 0; k < EPT; k++) {
-    const int e = threadIdx.x + k * BD;
-    if (N % BD == 0 || e < N) {
+    for (int k = 0; k < EPT; k++) {
+      const int e = threadIdx.x + k * BD;
+      if (N % BD != 0 && e >= N) continue;
       const int q = e / B, b = e % B, t = q / LZ, z = q % LZ;
-      data[base + b + sz * q] = A[b + B * z + TS * t];
+      double kcos = 0.0;
+      kcos += c.cs[x0 + b];
+      kcos += cxy;
+      kcos += c.cs[2 * c.cs_ld + z];
+      if constexpr (FOUR) kcos += c.cs[3 * c.cs_ld + t];
+      const double p2 = (kcos == D) ? 1.0 : 2.0 * (D - kcos);
+      const R ps = (R)(c.maxp * __drcp_rn(p2));
+      const int o = b + B * z + TS * t;
+      A[o] = mk<R>(A[o].x * ps, A[o].y * ps);
+    }
+    __syncthreads();
+    if constexpr (FOUR) ct_stages<R, NT, 1, LZ * B, LZ * B, 1, 0, TS, BD>(A, twt, true);
+    ct_stages<R, LZ, 1, NT * B, B, 1, TS, B, BD>(A, twz, true);
+#pragma unroll
+    for (int k = 0; k < EPT; k++) {
+      const int e = threadIdx.x + k * BD;
+      if (N % BD == 0 || e < N) {
+        const int q = e / B, b = e % B, t = q / LZ, z = q % LZ;
+        data[base + b + sz * q] = A[b + B * z + TS * t];
+      }
     }
   }
 }
