@@ -1,6 +1,6 @@
 """The JSON line of ``bench.py --impl reference`` (GLU's own solver on the host
-cores), run as a short subprocess on the CPU for the Landau FACG workload and
-the FASD ensemble: every key of the bench line, a positive throughput, the
+cores), run as a short subprocess on the CPU for the Landau FACG workload, the
+FASD ensemble and the Coulomb fix of 64^3x128: every key of the bench line, a positive throughput, the
 reference arm's own ``cpu_baseline`` and a zero-copy ``e2e``; and a non-zero
 rank of a multi-rank launch exits 0 without a line.
 """
@@ -38,6 +38,11 @@ def _landau_n(cfg):
     return len(cfg["full_fix_iters"])
 
 
+def _coulomb_n(cfg):
+    assert cfg["slice_steps"] > 0
+    return 1
+
+
 def _ensemble_n(cfg):
     assert cfg["configs"] == 48 + 16
     return cfg["configs"]
@@ -46,7 +51,8 @@ def _ensemble_n(cfg):
 @pytest.mark.parametrize("extra, configs_per_step", [
     ((), _landau_n),
     (("--workload", "ensemble"), _ensemble_n),
-], ids=["landau", "ensemble"])
+    (("--workload", "coulomb"), _coulomb_n),
+], ids=["landau", "ensemble", "coulomb"])
 def test_reference_arm_line(extra, configs_per_step):
     _ensure_oracle()
     r = _run(extra)
