@@ -1168,7 +1168,7 @@ def gluonprop_main(args, dims, rank, world, local):
         t = statistics.median(secs)
         value = 3600.0 / t
         emit({"metric": g_metric_name(dims), "value": value, "unit": G_UNIT,
-              "n_gpus": world, "steps": len(secs), "warmup": 0, "ms_per_step": t * 1e3,
+              "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
               "dtype": "f64", "data": "synthetic (8^4 GLU heatbath tiled + random gauge)",
               "config": dict(g_workload(dims), parallelism="host OpenMP"),
@@ -1353,10 +1353,10 @@ def heatbath_main(args, dims, rank, world, local):
         if rank != 0:
             return
         cores = os.cpu_count() or 1
-        t, n = h_reference_seconds(dims, cores)
+        t, n = h_reference_seconds(dims, cores, max(1, min(args.steps, 2)))
         value = 3600.0 / t
         emit({"metric": h_metric_name(dims), "value": value, "unit": H_UNIT,
-              "n_gpus": world, "steps": n, "warmup": 0, "ms_per_step": t * 1e3,
+              "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
               "dtype": "f64", "data": "synthetic (8^4 GLU heatbath tiled + random gauge)",
               "config": dict(cfg, parallelism="host OpenMP"), "impl": "reference",
