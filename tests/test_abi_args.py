@@ -1,0 +1,81 @@
+"""Argument errors of the C-ABI solvers are reported before any device work.
+
+gfix_landau, gfix_landau_device, gfix_coulomb and gfix_coulomb_device
+validate their dimensions, parameters and pointers first: a bad call returns
+-1 with a message in gfix_last_error() and touches no CUDA state, so these
+run without a GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from glu_b200 import _lib
+from glu_b200._lib import GfixParams, GfixResult
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from glu_b200 import build
+    try:
+        build.build()
+    except Exception as e:  # nvcc missing
+        pytest.skip(f"cannot build: {e}")
+    return _lib.load()
+
+
+def _params(**kw):
+    p = GfixParams()
+    p.gf_alpha, p.accuracy, p.max_iters = 0.08, 1e-14, 1000
+    p.algo, p.sd_fixed_step, p.precision, p.switch_theta = 0, 0, 0, 1e-9
+    p.traj_cap = 0
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+LINKS = np.zeros(2 * 2 * 2 * 2 * 4 * 18)
+
+
+def _call(lib, fn, dims, p, links=LINKS):
+    cd = (C.c_size_t * 4)(*dims)
+    ptr = None if links is None else links.ctypes.data
+    r = GfixResult()
+    if fn.startswith("gfix_coulomb"):
+        rc = getattr(lib, fn)(ptr, cd, C.byref(p) if p is not None else None,
+                              C.byref(r), None, None)
+    else:
+        rc = getattr(lib, fn)(ptr, cd, C.byref(p) if p is not None else None, C.byref(r))
+    return rc, lib.gfix_last_error().decode()
+
+
+FNS = ["gfix_landau", "gfix_landau_device", "gfix_coulomb", "gfix_coulomb_device"]
+
+
+@pytest.mark.parametrize("fn", FNS)
+@pytest.mark.parametrize("dims, kw, msg", [
+    ((2, 2, 1, 2), {}, "extent 1 of dimension 2 below 2"),
+    ((0, 2, 2, 2), {}, "extent 0 of dimension 0 below 2"),
+    ((2, 2, 2, 2), {"algo": 7}, "unknown algo 7"),
+    ((2, 2, 2, 2), {"precision": 5}, "unknown precision 5"),
+    ((2, 2, 2, 2), {"traj_cap": 10}, "traj_cap without traj_theta"),
+], ids=["extent1", "extent0", "algo", "precision", "traj"])
+def test_bad_arguments_rejected(lib, fn, dims, kw, msg):
+    rc, err = _call(lib, fn, dims, _params(**kw))
+    assert rc == -1
+    assert msg in err
+
+
+@pytest.mark.parametrize("fn", FNS)
+def test_null_links_and_params_rejected(lib, fn):
+    rc, err = _call(lib, fn, (2, 2, 2, 2), _params(), links=None)
+    assert rc == -1 and "null links" in err
+    rc, err = _call(lib, fn, (2, 2, 2, 2), None)
+    assert rc == -1 and "null dims or params" in err
+
+
+def test_null_batch_rejected(lib):
+    assert lib.gfix_batch_run(None) == -1
+    assert "null batch" in lib.gfix_last_error().decode()
