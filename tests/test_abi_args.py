@@ -79,3 +79,20 @@ def test_null_links_and_params_rejected(lib, fn):
 def test_null_batch_rejected(lib):
     assert lib.gfix_batch_run(None) == -1
     assert "null batch" in lib.gfix_last_error().decode()
+
+
+@pytest.mark.parametrize("dims, msg", [
+    ((256, 256, 256, 2), "at most 16777216 sites"),
+    ((2, 1, 2, 2), "every extent must be at least 2"),
+], ids=["too-large", "extent1"])
+def test_noalloc_limits_rejected(lib, dims, msg):
+    # rejected before the pointers are used, so stand-in addresses serve
+    cd = (C.c_size_t * 4)(*dims)
+    assert lib.gfix_theta_functional_noalloc(C.c_void_p(256), cd, C.c_void_p(512)) == -1
+    assert msg in lib.gfix_noalloc_error().decode()
+
+
+def test_noalloc_null_rejected(lib):
+    cd = (C.c_size_t * 4)(4, 4, 4, 4)
+    assert lib.gfix_theta_functional_noalloc(None, cd, C.c_void_p(512)) == -1
+    assert "null argument" in lib.gfix_noalloc_error().decode()
