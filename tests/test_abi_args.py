@@ -1,9 +1,10 @@
-"""Argument errors of the C-ABI solvers are reported before any device work.
+"""Argument errors of the C-ABI entry points are reported before any device work.
 
-gfix_landau, gfix_landau_device, gfix_coulomb and gfix_coulomb_device
+The solvers (gfix_landau, gfix_coulomb and their _device forms), the
+allocation-free theta/functional, the NERSC codec and the heatbath generator
 validate their dimensions, parameters and pointers first: a bad call returns
--1 with a message in gfix_last_error() and touches no CUDA state, so these
-run without a GPU.
+-1 with a message in the matching *_error() string and touches no CUDA state,
+so these run without a GPU.
 """
 from __future__ import annotations
 
@@ -96,3 +97,35 @@ def test_noalloc_null_rejected(lib):
     cd = (C.c_size_t * 4)(4, 4, 4, 4)
     assert lib.gfix_theta_functional_noalloc(None, cd, C.c_void_p(512)) == -1
     assert "null argument" in lib.gfix_noalloc_error().decode()
+
+
+@pytest.mark.parametrize("fn", ["gfix_nersc_decode", "gfix_nersc_encode"])
+@pytest.mark.parametrize("dims, nreal, nbytes, msg", [
+    ((2, 2, 2, 2), 10, 8, "reals per link must be 12 or 18"),
+    ((2, 2, 2, 2), 18, 2, "bytes per real must be 8 or 4"),
+    ((2, 0, 2, 2), 18, 8, "zero extent"),
+], ids=["nreal", "bytes", "extent"])
+def test_nersc_bad_arguments_rejected(lib, fn, dims, nreal, nbytes, msg):
+    cd = (C.c_size_t * 4)(*dims)
+    buf = np.zeros(2 * 2 * 2 * 2 * 4 * 18)
+    assert getattr(lib, fn)(buf.ctypes.data, cd, nreal, nbytes, 1, buf.ctypes.data,
+                            None) == -1
+    assert msg in lib.gfix_nersc_error().decode()
+
+
+@pytest.mark.parametrize("fn", ["gfix_nersc_decode", "gfix_nersc_encode"])
+def test_nersc_null_rejected(lib, fn):
+    cd = (C.c_size_t * 4)(2, 2, 2, 2)
+    assert getattr(lib, fn)(None, cd, 18, 8, 1, None, None) == -1
+    assert "null payload or links" in lib.gfix_nersc_error().decode()
+
+
+@pytest.mark.parametrize("fn", ["gfix_heatbath", "gfix_heatbath_device"])
+def test_heatbath_bad_arguments_rejected(lib, fn):
+    f = getattr(lib, fn)
+    # the draughtboard update needs even extents
+    cd = (C.c_size_t * 4)(4, 4, 3, 4)
+    assert f(LINKS.ctypes.data, cd, 6.0, 1, 4, 1, 0, None) == -1
+    assert "needs even extents" in lib.gfix_update_error().decode()
+    assert f(None, cd, 6.0, 1, 4, 1, 0, None) == -1
+    assert "null links" in lib.gfix_update_error().decode()
