@@ -1,10 +1,10 @@
 """Argument errors of the C-ABI entry points are reported before any device work.
 
 The solvers (gfix_landau, gfix_coulomb and their _device forms), the
-allocation-free theta/functional, the NERSC codec and the heatbath generator
-validate their dimensions, parameters and pointers first: a bad call returns
--1 with a message in the matching *_error() string and touches no CUDA state,
-so these run without a GPU.
+allocation-free theta/functional, the NERSC codec, the gluon-propagator
+measurement and the heatbath generator validate their dimensions, parameters
+and pointers first: a bad call returns -1 with a message in the matching
+*_error() string and touches no CUDA state, so these run without a GPU.
 """
 from __future__ import annotations
 
@@ -129,3 +129,24 @@ def test_heatbath_bad_arguments_rejected(lib, fn):
     assert "needs even extents" in lib.gfix_update_error().decode()
     assert f(None, cd, 6.0, 1, 4, 1, 0, None) == -1
     assert "null links" in lib.gfix_update_error().decode()
+
+
+@pytest.mark.parametrize("fn", ["gfix_cuts_measure", "gfix_cuts_measure_device"])
+@pytest.mark.parametrize("kw, msg", [
+    ({"dir": 1}, "cut mode 1 not supported"),
+    ({"type": 9}, "momentum cut type 9 unknown"),
+    ({"definition": 7}, "field definition 7 unknown"),
+], ids=["nonexceptional", "type", "definition"])
+def test_cuts_bad_arguments_rejected(lib, fn, kw, msg):
+    from glu_b200._lib import GfixCutInfo
+    ci = GfixCutInfo(dir=6, type=2, max_mom=4, definition=0, angle=60, cyl_width=2.0)
+    for k, v in kw.items():
+        setattr(ci, k, v)
+    cd = (C.c_size_t * 4)(2, 2, 2, 2)
+    out = np.zeros(16)
+    f = getattr(lib, fn)
+    ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    assert f(LINKS.ctypes.data, cd, C.byref(ci), 1, ptr(out), ptr(out), ptr(out)) == -1
+    assert msg in lib.gfix_cuts_error().decode()
+    assert f(None, cd, C.byref(ci), 1, ptr(out), ptr(out), ptr(out)) == -1
+    assert "null links" in lib.gfix_cuts_error().decode()
