@@ -150,3 +150,18 @@ def test_cuts_bad_arguments_rejected(lib, fn, kw, msg):
     assert msg in lib.gfix_cuts_error().decode()
     assert f(None, cd, C.byref(ci), 1, ptr(out), ptr(out), ptr(out)) == -1
     assert "null links" in lib.gfix_cuts_error().decode()
+
+
+def test_python_mirror_raises_the_library_message(lib):
+    # the host mirror checks shapes itself and raises the C library's
+    # message for what the library rejects
+    from glu_b200 import gfix
+    U = np.zeros((2 * 2 * 1 * 2, 4, 3, 3), complex)
+    with pytest.raises(_lib.GfixError, match="extent 1 of dimension 2 below 2"):
+        gfix.landau_fix(U, (2, 2, 1, 2))
+    with pytest.raises(_lib.GfixError, match="extent 1 of dimension 2 below 2"):
+        gfix.coulomb_fix(U, (2, 2, 1, 2))
+    with pytest.raises(ValueError, match="dims must be"):
+        gfix.landau_fix(U, (2, 2, 2))
+    with pytest.raises(ValueError, match="sites"):
+        gfix.landau_fix(U, (2, 2, 2, 2))
