@@ -2,7 +2,8 @@
 cores), run as a short subprocess on the CPU for every workload (Landau FACG,
 the FASD ensemble, Coulomb 64^3x128, gluon propagators, heatbath): every key of the bench line, a positive throughput, the
 reference arm's own ``cpu_baseline`` and a zero-copy ``e2e``; and a non-zero
-rank of a multi-rank launch exits 0 without a line.
+rank of a multi-rank launch exits 0 without a line; without a CUDA device the
+GPU arm of every workload fails with no line printed (no CPU fallback).
 """
 from __future__ import annotations
 
@@ -90,4 +91,22 @@ def test_reference_arm_line(extra, configs_per_step):
 def test_reference_arm_other_ranks_silent():
     r = _run((), {"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert r.returncode == 0, r.stderr[-2000:]
+    assert _lines(r.stdout) == []
+
+
+@pytest.mark.parametrize("workload", ["landau", "coulomb", "ensemble", "gluonprop",
+                                      "heatbath"])
+def test_gpu_arm_fails_loudly_without_cuda(workload):
+    # no CPU fallback: without a CUDA device the GPU arm exits with an error
+    # and prints no bench line
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    env = dict(os.environ)
+    env.pop("RANK", None)
+    env.pop("WORLD_SIZE", None)
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--workload", workload,
+                        "--steps", "1", "--warmup", "3", "--no-cpu-baseline"],
+                       cwd=ROOT, env=env, capture_output=True, text=True, timeout=240)
+    assert r.returncode != 0
     assert _lines(r.stdout) == []
