@@ -1,9 +1,10 @@
 """The JSON line of ``bench.py --impl reference`` (GLU's own solver on the host
 cores), run as a short subprocess on the CPU for every workload (Landau FACG,
-the FASD ensemble, Coulomb 64^3x128, gluon propagators, heatbath): every key of the bench line, a positive throughput, the
-reference arm's own ``cpu_baseline`` and a zero-copy ``e2e``; and a non-zero
-rank of a multi-rank launch exits 0 without a line; without a CUDA device the
-GPU arm of every workload fails with no line printed (no CPU fallback).
+the FASD ensemble, Coulomb 64^3x128, gluon propagators, heatbath): every key
+of the bench line, a positive throughput, the reference arm's own
+``cpu_baseline`` and a zero-copy ``e2e``.  A non-zero rank of a multi-rank
+launch exits 0 without a line.  Without a CUDA device the GPU arm of every
+workload fails with no line printed (no CPU fallback).
 """
 from __future__ import annotations
 
