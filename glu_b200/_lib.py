@@ -155,7 +155,8 @@ def load(path: Path | str | None = None):
     lib.gfix_profile_landau.argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
                                         C.c_int, _dp, _dp]
     lib.gfix_theta_functional_noalloc.restype = C.c_int
-    lib.gfix_theta_functional_noalloc.argtypes = [C.c_void_p, _szp, C.c_void_p]
+    lib.gfix_theta_functional_noalloc.argtypes = [C.c_void_p, _szp, C.c_void_p,
+                                                   C.c_void_p]
     lib.gfix_noalloc_error.restype = C.c_char_p
     lib.gfix_noalloc_error.argtypes = []
     lib.gfix_last_error.restype = C.c_char_p

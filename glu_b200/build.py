@@ -10,6 +10,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -46,14 +47,31 @@ def stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile every translation unit to an object (in parallel: the units
+    share no device code), then link the shared library."""
     if not force and not stale():
         return LIB
     LIB_DIR.mkdir(exist_ok=True)
-    cmd = [_nvcc(), *NVCC_FLAGS, "-o", str(LIB),
-           *[str(CSRC / s) for s in SOURCES if (CSRC / s).exists()], "-lgomp"]
+    obj_dir = LIB_DIR / "obj"
+    obj_dir.mkdir(exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    srcs = [CSRC / s for s in SOURCES if (CSRC / s).exists()]
+    objs = [obj_dir / (s.stem + ".o") for s in srcs]
+    cmds = [[_nvcc(), *compile_flags, "-c", "-o", str(o), str(s)]
+            for s, o in zip(srcs, objs)]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True, cwd=str(CSRC))
+        for c in cmds:
+            print(" ".join(c))
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c, cwd=str(CSRC)), cmds)):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
+    link = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+            "-Xcompiler", "-fopenmp", "-o", str(LIB), *[str(o) for o in objs],
+            "-lgomp"]
+    if verbose:
+        print(" ".join(link))
+    subprocess.run(link, check=True, cwd=str(CSRC))
     return LIB
 
 

@@ -40,6 +40,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -981,10 +982,19 @@ struct Work {
   }
 };
 
-static std::map<std::array<size_t, 4>, std::unique_ptr<Work>> g_work;
+// one workspace per (device, lattice shape): a workspace's buffers and
+// stream belong to the device that was current when it was made
+static std::map<std::array<size_t, 5>, std::unique_ptr<Work>> g_work;
+static std::mutex g_work_mu;
 
 static Work *work_for(const size_t *dims) {
-  const std::array<size_t, 4> k{dims[0], dims[1], dims[2], dims[3]};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cfail("no CUDA device");
+    return nullptr;
+  }
+  const std::array<size_t, 5> k{(size_t)dev, dims[0], dims[1], dims[2], dims[3]};
+  std::lock_guard<std::mutex> lk(g_work_mu);
   auto it = g_work.find(k);
   if (it != g_work.end()) return it->second.get();
   auto w = std::make_unique<Work>();
@@ -1116,6 +1126,9 @@ int gfix_cuts_measure_device(const double *d_links, const size_t dims[4],
   if (check_info(dims, ci)) return -1;
   Work *w = work_for(dims);
   if (!w) return -1;
+  // the library's stream does not synchronise with the caller's: wait for
+  // all work on the device before the links are read
+  CCK(cudaDeviceSynchronize());
   w->c.links = reinterpret_cast<const C2 *>(d_links);
   return run(w, ci, nmom, out0, out1, pspace_err);
 }
@@ -1157,6 +1170,7 @@ int gfix_profile_cuts(const double *d_links, const size_t dims[4], const gfix_cu
   if (check_info(dims, ci)) return -1;
   Work *w = work_for(dims);
   if (!w) return -1;
+  CCK(cudaDeviceSynchronize());
   w->c.links = reinterpret_cast<const C2 *>(d_links);
   const MomList *ml = w->list(*ci);
   if (!ml || w->upload(ml)) return -1;
@@ -1183,6 +1197,9 @@ int gfix_profile_cuts(const double *d_links, const size_t dims[4], const gfix_cu
   return 0;
 }
 
-void gfix_cuts_release(void) { g_work.clear(); }
+void gfix_cuts_release(void) {
+  std::lock_guard<std::mutex> lk(g_work_mu);
+  g_work.clear();
+}
 
 }  // extern "C"

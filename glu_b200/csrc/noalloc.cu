@@ -15,6 +15,8 @@
 // The array is shared by every call: calls that overlap on the GPU race on
 // it.  The first call on a device looks up the array's device address with
 // cudaGetSymbolAddress; make that first call before any stream capture.
+// Both kernels run on the stream the caller passes, in its order, and the
+// call returns without waiting for them.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -36,7 +38,7 @@ static __device__ __align__(256) double g_scratch[kScratchBlocks * 2];
 // symbol's own name as a device pointer)
 double *g_scratch_ptr[kMaxDevices] = {nullptr};
 std::mutex g_mu;
-char g_msg[256] = "";
+thread_local char g_msg[256] = "";
 
 __device__ __forceinline__ double na_warp_sum(double v) {
 #pragma unroll
@@ -139,17 +141,20 @@ extern "C" {
 const char *gfix_noalloc_error(void) { return g_msg; }
 
 int gfix_theta_functional_noalloc(const double *d_links, const size_t dims[4],
-                                  double *d_out) {
+                                  double *d_out, void *stream) {
   if (!d_links || !dims || !d_out) return na_fail("null argument");
+  // the volume is checked after every factor, before any extent is
+  // narrowed to int, so no product can wrap below the limit
+  constexpr size_t kMaxSites = (size_t)kScratchBlocks * kNaThreads;
   size_t V = 1;
   for (int i = 0; i < 4; i++) {
     if (dims[i] < 2) return na_fail("every extent must be at least 2");
+    if (dims[i] > kMaxSites || V * dims[i] > kMaxSites)
+      return na_fail("lattice too large for the fixed scratch: at most "
+                     "16777216 sites");
     V *= dims[i];
   }
   const size_t nblocks = (V + kNaThreads - 1) / kNaThreads;
-  if (nblocks > (size_t)kScratchBlocks)
-    return na_fail("lattice too large for the fixed scratch: at most "
-                   "16777216 sites");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return na_fail("no usable CUDA device");
@@ -171,10 +176,11 @@ int gfix_theta_functional_noalloc(const double *d_links, const size_t dims[4],
   }
   // every slot k_na_finish reads is written first by this call's
   // k_na_partials, so no clearing is needed
-  k_na_partials<<<(unsigned)nblocks, kNaThreads>>>(
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  k_na_partials<<<(unsigned)nblocks, kNaThreads, 0, s>>>(
       reinterpret_cast<const double2 *>(d_links), (int)dims[0], (int)dims[1],
       (int)dims[2], (int)dims[3], scratch);
-  k_na_finish<<<1, 1024>>>(scratch, (int)nblocks, (double)V, d_out);
+  k_na_finish<<<1, 1024, 0, s>>>(scratch, (int)nblocks, (double)V, d_out);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     snprintf(g_msg, sizeof g_msg, "launch: %s", cudaGetErrorString(e));

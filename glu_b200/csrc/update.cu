@@ -41,6 +41,7 @@
 #include <cstdio>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -567,14 +568,29 @@ struct Work {
   }
 };
 
-static std::map<std::array<size_t, 4>, std::unique_ptr<Work>> g_work;
+// one workspace per (device, lattice shape): a workspace's buffers and
+// stream belong to the device that was current when it was made
+static std::map<std::array<size_t, 5>, std::unique_ptr<Work>> g_work;
+static std::mutex g_work_mu;
 
 static Work *work_for(const size_t *dims) {
   if (!dims) {
     ufail("null dims");
     return nullptr;
   }
-  const std::array<size_t, 4> k{dims[0], dims[1], dims[2], dims[3]};
+  for (int i = 0; i < 4; i++)
+    if (dims[i] < 2 || dims[i] % 2) {
+      ufail("extent %zu of dimension %d: the update needs even extents "
+            "(two draughtboard colours)", dims[i], i);
+      return nullptr;
+    }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    ufail("no CUDA device");
+    return nullptr;
+  }
+  const std::array<size_t, 5> k{(size_t)dev, dims[0], dims[1], dims[2], dims[3]};
+  std::lock_guard<std::mutex> lk(g_work_mu);
   auto it = g_work.find(k);
   if (it != g_work.end()) return it->second.get();
   auto w = std::make_unique<Work>();
@@ -597,6 +613,10 @@ int gfix_heatbath_device(double *d_links, const size_t dims[4], double beta,
   if (!d_links) return ufail("null links");
   Work *w = work_for(dims);
   if (!w) return -1;
+  // the library's stream does not synchronise with the caller's: wait for
+  // all work on the device, so a kernel that has just written the links
+  // (on any stream) has finished before they are read
+  UCK(cudaDeviceSynchronize());
   C2 *aos = reinterpret_cast<C2 *>(d_links);
   w->to_cb(aos);
   if (w->run(beta, iterations, n_or, seed, first_iteration, plaquettes)) return -1;
@@ -646,6 +666,9 @@ void gfix_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t o
   out[3] = r.w;
 }
 
-void gfix_update_release(void) { g_work.clear(); }
+void gfix_update_release(void) {
+  std::lock_guard<std::mutex> lk(g_work_mu);
+  g_work.clear();
+}
 
 }  // extern "C"

@@ -21,7 +21,15 @@
  *
  * All calls are synchronous: on return the links have been copied back.
  * A call uses the current CUDA device.  Calls are not re-entrant (GLU's are
- * not either): the library keeps one cached workspace per lattice shape.
+ * not either): the library keeps one cached workspace per device and
+ * lattice shape.
+ *
+ * Ordering of the entry points that take device pointers (the _device
+ * variants, gfix_coulomb_slices*, gfix_profile_*): the library works on its
+ * own non-blocking streams, so each of them first waits for all work on
+ * the device (cudaDeviceSynchronize) before it reads the caller's buffers,
+ * and has finished writing them when it returns.  The one exception is
+ * gfix_theta_functional_noalloc, which is ordered on the stream it is given.
  */
 #ifndef GLU_B200_GFIX_H
 #define GLU_B200_GFIX_H
@@ -240,11 +248,13 @@ int gfix_profile_coulomb(const double *d_links, const size_t dims[4],
  * the device.  It allocates nothing: its scratch is a fixed 1 MiB device
  * array inside the library, so lattices above 16,777,216 sites are rejected.
  * Calls that overlap on the GPU race on that array.  The first call on a
- * device looks the array up; make it before any stream capture.  Launches on
- * the legacy default stream; returns 0, or -1 with the reason in
- * gfix_noalloc_error(). */
+ * device looks the array up; make it before any stream capture.  stream is
+ * a cudaStream_t (NULL: the legacy default stream); both kernels are
+ * launched on it and the call returns without waiting for them, so d_out
+ * is ready once the stream's work up to this call has completed.  Returns
+ * 0, or -1 with the reason in gfix_noalloc_error() (thread-local). */
 int gfix_theta_functional_noalloc(const double *d_links, const size_t dims[4],
-                                  double *d_out);
+                                  double *d_out, void *stream);
 const char *gfix_noalloc_error(void);
 
 /* FFT plans.  0 (default): a fixed plan per lattice shape -- compile-time

@@ -84,18 +84,41 @@ def test_null_batch_rejected(lib):
 
 @pytest.mark.parametrize("dims, msg", [
     ((256, 256, 256, 2), "at most 16777216 sites"),
+    # a volume that wraps around 2^64 to exactly 2^24 sites
+    (((1 << 40) + 1, 1 << 22, 2, 2), "at most 16777216 sites"),
     ((2, 1, 2, 2), "every extent must be at least 2"),
-], ids=["too-large", "extent1"])
+], ids=["too-large", "wraps", "extent1"])
 def test_noalloc_limits_rejected(lib, dims, msg):
     # rejected before the pointers are used, so stand-in addresses serve
     cd = (C.c_size_t * 4)(*dims)
-    assert lib.gfix_theta_functional_noalloc(C.c_void_p(256), cd, C.c_void_p(512)) == -1
+    assert lib.gfix_theta_functional_noalloc(C.c_void_p(256), cd, C.c_void_p(512),
+                                             None) == -1
     assert msg in lib.gfix_noalloc_error().decode()
 
 
 def test_noalloc_null_rejected(lib):
     cd = (C.c_size_t * 4)(4, 4, 4, 4)
-    assert lib.gfix_theta_functional_noalloc(None, cd, C.c_void_p(512)) == -1
+    assert lib.gfix_theta_functional_noalloc(None, cd, C.c_void_p(512), None) == -1
+    assert "null argument" in lib.gfix_noalloc_error().decode()
+
+
+def test_noalloc_error_is_per_thread(lib):
+    """The message buffer is thread-local: a failure on another thread does
+    not overwrite this thread's message."""
+    import threading
+    cd = (C.c_size_t * 4)(4, 4, 4, 4)
+    assert lib.gfix_theta_functional_noalloc(None, cd, C.c_void_p(512), None) == -1
+    other = []
+
+    def run():
+        big = (C.c_size_t * 4)(256, 256, 256, 2)
+        lib.gfix_theta_functional_noalloc(C.c_void_p(256), big, C.c_void_p(512), None)
+        other.append(lib.gfix_noalloc_error().decode())
+
+    t = threading.Thread(target=run)
+    t.start()
+    t.join()
+    assert "16777216" in other[0]
     assert "null argument" in lib.gfix_noalloc_error().decode()
 
 
