@@ -50,6 +50,9 @@ UNIT = "configs/hour"
 ACC = 1e-14
 ALPHA = 0.08
 MAX_ITERS = 20000
+# gauge invariance: the average plaquette of a fixed configuration equals
+# the input's to this absolute tolerance
+PLAQ_TOL = 1e-13
 
 
 def parse():
@@ -270,6 +273,16 @@ def gpu_arm(args, dims, rank, world, local):
         check(lib.gfix_landau(hwork.data_ptr(), cd, C.byref(p), C.byref(r)))
         return r
 
+    def plaquette(ptr):
+        o = np.zeros(3)
+        check(lib.gfix_observables(ptr, cd, o.ctypes.data_as(C.POINTER(C.c_double))))
+        return float(o[2])
+
+    # every fixed configuration must stay on its input's gauge orbit: the
+    # average plaquette of the last step's fixed links (host side, after
+    # the timed region) against the input's
+    plaq_in = [plaquette(h.data_ptr()) for h in hosts]
+
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     out = {}
     with Clocks(local) as clk:
@@ -296,7 +309,8 @@ def gpu_arm(args, dims, rank, world, local):
             ms = max_over_ranks(a.elapsed_time(b))
             # end to end: pinned host buffers, H2D + D2H inside each fix
             e_ms = 0.0
-            for _ in range(args.steps):
+            drift = 0.0
+            for k in range(args.steps):
                 for i in range(E_CONFIGS):
                     hwork.copy_(hosts[i])
                     barrier()
@@ -306,8 +320,14 @@ def gpu_arm(args, dims, rank, world, local):
                     b2.record()
                     torch.cuda.synchronize()
                     e_ms += a2.elapsed_time(b2)
+                    if k == args.steps - 1:
+                        drift = max(drift, abs(plaquette(hwork.data_ptr()) - plaq_in[i]))
             e_ms = max_over_ranks(e_ms)
-            out[prec] = dict(ms=ms, e2e_ms=e_ms, per=per, launches=launches)
+            if not drift < PLAQ_TOL:
+                raise RuntimeError(f"{prec}: a fixed configuration left its gauge orbit "
+                                   f"(plaquette changed by {drift:.3e})")
+            out[prec] = dict(ms=ms, e2e_ms=e_ms, per=per, launches=launches,
+                             plaq_drift=drift)
     clocks = clk.summary()
     res = dict(out=out, clocks=clocks, V=V)
     # per-kernel device times for the roofline (events on the launch stream)
@@ -465,6 +485,7 @@ def gpu_line(args, dims, world, res, cpu):
                    "iters_per_config": [x[0] for x in o["per"]],
                    "iters_fp32_per_config": [x[1] for x in o["per"]],
                    "final_theta_max": max(x[2] for x in o["per"]),
+                   "plaquette_change_max": max(o["plaq_drift"], o64["plaq_drift"]),
                    "ms_per_config": ms_step / E_CONFIGS,
                    "fp64_only": {"value": nfix * 3600e3 / o64["ms"],
                                  "ms_per_step": o64["ms"] / steps,
@@ -610,6 +631,16 @@ def coulomb_gpu(args, dims, rank, world, local):
                  sth.ctypes.data_as(C.POINTER(C.c_double)),
                  sit.ctypes.data_as(C.POINTER(C.c_size_t))))
         return r
+
+    def plaquette(ptr):
+        o = np.zeros(3)
+        check(lib.gfix_observables(ptr, cd, o.ctypes.data_as(C.POINTER(C.c_double))))
+        return float(o[2])
+
+    # every fixed configuration must stay on its input's gauge orbit: the
+    # average plaquette of the last step's fixed links (host side, after
+    # the timed region) against the input's
+    plaq_in = [plaquette(h.data_ptr()) for h in hosts]
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     out = {}
@@ -1010,6 +1041,16 @@ def ensemble_main(args, rank, world, local):
     cds = [(C.c_size_t * 4)(*d) for d, _ in cfgs]
     nbytes = sum(t.numel() * 8 for t in pristine)
     sites = sum(int(np.prod(d)) for d, _ in cfgs)
+    def plaquette(ptr):
+        o = np.zeros(3)
+        check(lib.gfix_observables(ptr, cd, o.ctypes.data_as(C.POINTER(C.c_double))))
+        return float(o[2])
+
+    # every fixed configuration must stay on its input's gauge orbit: the
+    # average plaquette of the last step's fixed links (host side, after
+    # the timed region) against the input's
+    plaq_in = [plaquette(h.data_ptr()) for h in hosts]
+
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     out = {}
     with Clocks(local) as clk:

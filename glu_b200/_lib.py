@@ -20,7 +20,8 @@ class GfixParams(C.Structure):
                 ("max_iters", C.c_size_t), ("algo", C.c_int),
                 ("sd_fixed_step", C.c_int), ("precision", C.c_int),
                 ("switch_theta", C.c_double), ("traj_theta", _dp),
-                ("traj_func", _dp), ("traj_cap", C.c_size_t)]
+                ("traj_func", _dp), ("traj_cap", C.c_size_t),
+                ("max_restarts", C.c_int), ("restart_seed", C.c_uint64)]
 
 
 class GfixCutInfo(C.Structure):
@@ -38,7 +39,8 @@ class GfixResult(C.Structure):
 # every symbol include/glu_gfix.h declares
 EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
            "Coulomb_FA", "FOURIER_ACCELERATE2", "cuts_struct", "gfix_landau",
-           "gfix_landau_device", "gfix_coulomb", "gfix_coulomb_device",
+           "gfix_landau_device", "gfix_landau_driver", "gfix_coulomb",
+           "gfix_coulomb_device", "gfix_coulomb_driver",
            "gfix_observables", "gfix_reunit", "gfix_fourier_accelerate",
            "gfix_profile_landau", "gfix_profile_coulomb",
            "gfix_theta_functional_noalloc", "gfix_batch_create",
@@ -81,6 +83,12 @@ def load(path: Path | str | None = None):
         getattr(lib, fn).restype = C.c_int
         getattr(lib, fn).argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
                                      C.POINTER(GfixResult), _dp, _szp]
+    lib.gfix_landau_driver.restype = C.c_int
+    lib.gfix_landau_driver.argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
+                                       C.POINTER(GfixResult), _dp, _dp]
+    lib.gfix_coulomb_driver.restype = C.c_int
+    lib.gfix_coulomb_driver.argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
+                                        C.POINTER(GfixResult), _dp, _dp, _dp, _dp]
     lib.gfix_observables.restype = C.c_int
     lib.gfix_observables.argtypes = [C.c_void_p, _szp, _dp]
     for fn in ("gfix_nersc_decode", "gfix_nersc_encode"):

@@ -1,6 +1,7 @@
 // Auxiliary kernels: observables, reunitarisation, precision switch.
 #pragma once
 
+#include "coulomb.cuh"
 #include "kernels.cuh"
 #include "su3_log.cuh"
 
@@ -173,6 +174,34 @@ __global__ void __launch_bounds__(kSiteThreads)
     gtransform(A, U, B);
     store_link(c.U, c.V, mu, s, U);
   }
+}
+
+// Random SU(3) gauge matrices G[9][V] for a random restart of a Landau fix
+// (GLU's random_transform, src/Geometry/random_config.c:107-120, which
+// draws them from its own per-thread generator): per site nine complex
+// Gaussian entries (Box-Muller on a SplitMix64 stream keyed by the seed,
+// the attempt and the site), then the column Gram-Schmidt of gram_reunit
+// (columns 0 and 1 orthonormal, column 2 their conjugate cross product).
+// Reproducible for a given (seed, attempt); not GLU's stream.
+__global__ void k_random_gauge(cx<double> *G, int V, unsigned long long seed,
+                               int attempt) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= V) return;
+  unsigned long long h =
+      mix64(seed ^ mix64(((unsigned long long)attempt << 40) ^ (unsigned long long)s));
+  cx<double> g[9];
+#pragma unroll
+  for (int e = 0; e < 9; e++) {
+    h = mix64(h);
+    const double u1 = ((h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    h = mix64(h);
+    const double u2 = ((h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+    const double rad = sqrt(-2.0 * log(u1));
+    g[e] = mk<double>(rad * cospi(2.0 * u2), rad * sinpi(2.0 * u2));
+  }
+  gram_reunit(g);
+#pragma unroll
+  for (int e = 0; e < 9; e++) G[(size_t)e * V + s] = g[e];
 }
 
 }  // namespace gfix

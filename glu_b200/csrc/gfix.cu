@@ -56,6 +56,7 @@ static int fail(const char *fmt, ...) {
 void count_launches(unsigned long long n) { LAUNCHED(n); }
 
 constexpr size_t kSentinel = 123456789;
+constexpr size_t kGluFailure = (size_t)-1;  // GLU_FAILURE returned as size_t
 
 // FFT plans: 0 = the default plan per shape (bit-reproducible runs), 1 =
 // autotuned per shape at first use (gfix_fft_tuning, GLU_GFIX_FFT_TUNE=1)
@@ -1301,8 +1302,25 @@ static Params to_params(const gfix_params *p) {
 // conjugate directions continue across the switch.  A phase that ended
 // non-finite hands over nothing (FP64 from the staged input links; it32 = 0,
 // *restart = 1).
+// The links a Landau attempt starts from: the staged input (AoS FP64 in
+// d_aos); for a restart (attempt > 0) randomly gauge transformed, as GLU's
+// Landau driver re-reads its input and applies random_transform
+// (src/Gfix/Landau.c:241-257, src/Geometry/random_config.c:107-120).
+static int stage_input(Engine<double> *e, unsigned long long seed, int attempt) {
+  if (e->from_aos(e->d_aos)) return -1;
+  if (attempt > 0) {
+    cx<double> *G = e->c.fb[0];  // 9 V complex fit in the field pool
+    k_random_gauge<<<(e->V + 255) / 256, 256, 0, e->s>>>(G, e->V, seed, attempt);
+    k_apply_gauge<<<e->nb_site, kSiteThreads, 0, e->s>>>(e->c, G);
+    LAUNCHED(2);
+    CK(cudaGetLastError());
+  }
+  return 0;
+}
+
 static int mixed_handover(Engine<double> *e, Engine<float> *f, const Params &p64,
-                          size_t *it32, double th32, int *restart) {
+                          size_t *it32, double th32, int *restart,
+                          unsigned long long seed, int attempt) {
   *restart = 0;
   if (!(*it32 == kSentinel || *it32 > 0)) return 0;
   cx<double> *G64 = e->c.fb[0];  // 9 V complex fit in the field pool
@@ -1315,7 +1333,7 @@ static int mixed_handover(Engine<double> *e, Engine<float> *f, const Params &p64
   double tt = 0.0;
   if (e->reset(p64) || e->theta_test(&tt)) return -1;
   if (!std::isfinite(th32) || !std::isfinite(tt)) {
-    if (e->from_aos(e->d_aos)) return -1;
+    if (stage_input(e, seed, attempt)) return -1;
     *it32 = 0;
     *restart = 1;
     return 0;
@@ -1338,13 +1356,15 @@ static int mixed_handover(Engine<double> *e, Engine<float> *f, const Params &p64
   return 0;
 }
 
-static int landau_staged(Engine<double> *e64, const gfix_params *gp,
-                         gfix_result *r) {
+// One Landau solve (GLU's FACG / FASD, or the mixed-precision pair of
+// them) from the staged input; the fixed links are left in e64's SoA
+// links.  attempt > 0: a random restart (stage_input).
+static int landau_attempt(Engine<double> *e64, const gfix_params *gp,
+                          int attempt, gfix_result *r) {
   Params p = to_params(gp);
   gfix_result res;
   memset(&res, 0, sizeof res);
-  if (e64->from_aos(e64->d_aos)) return -1;
-  CK(cudaEventRecord(e64->ev0, e64->s));
+  if (stage_input(e64, gp->restart_seed, attempt)) return -1;
   size_t iters = 0;
   double th = 0.0;
   size_t tl = 0;
@@ -1369,7 +1389,9 @@ static int landau_staged(Engine<double> *e64, const gfix_params *gp,
     if (e32->fetch_traj(p32, &tl32)) return -1;
     {
       int restart = 0;
-      if (mixed_handover(e64, e32, p, &it32, th32, &restart)) return -1;
+      if (mixed_handover(e64, e32, p, &it32, th32, &restart, gp->restart_seed,
+                         attempt))
+        return -1;
       if (restart) {
         tl32 = 0;
         res.restarts++;
@@ -1391,14 +1413,59 @@ static int landau_staged(Engine<double> *e64, const gfix_params *gp,
     if (e64->solve(p, &iters, &th)) return -1;
     if (e64->fetch_traj(p, &tl)) return -1;
   }
+  res.iters = iters;
+  res.theta = th;
+  res.traj_len = tl;
+  *r = res;
+  return 0;
+}
+
+// GLU's Landau driver prints every failed attempt (print_failure_info,
+// src/Gfix/Landau.c:70-86); the flat entry points stay silent
+static thread_local bool t_restart_log = false;
+void set_restart_log(bool on) { t_restart_log = on; }
+
+// A Landau fix of the links staged in e64->d_aos, with GLU's random
+// restarts (src/Gfix/Landau.c:303-340) when p->max_restarts > 0: after a
+// failed solve (the sentinel) the input is randomly gauge transformed and
+// solved again, up to max_restarts times.  The count follows GLU's sums:
+// the first attempt's sentinel, + max_iters per failed restart, + the
+// successful attempt's count; GLU_FAILURE when every attempt failed.  The
+// fixed links are left in e64's SoA links (resident) and in d_aos.
+static int landau_staged(Engine<double> *e64, const gfix_params *gp,
+                         gfix_result *r) {
+  CK(cudaEventRecord(e64->ev0, e64->s));
+  gfix_result res;
+  if (landau_attempt(e64, gp, 0, &res)) return -1;
+  if (res.iters == kSentinel && gp->max_restarts > 0) {
+    if (t_restart_log)
+      fprintf(stderr, "\n[GF] Non-convergence ... Randomly-restarting \n"
+              "\n[GF] Failure :: %d || Iters :: %zu || ACC :: %e \n", 0,
+              gp->max_iters, res.theta);
+    size_t total = kSentinel;
+    int failure = 1;
+    for (; failure <= gp->max_restarts; failure++) {
+      gfix_result a;
+      if (landau_attempt(e64, gp, failure, &a)) return -1;
+      a.restarts += res.restarts + 1;
+      res = a;
+      if (a.iters != kSentinel) {
+        total += a.iters;
+        break;
+      }
+      total += gp->max_iters;
+      if (t_restart_log)
+        fprintf(stderr, "\n[GF] Non-convergence ... Randomly-restarting \n"
+                "\n[GF] Failure :: %d || Iters :: %zu || ACC :: %e \n",
+                failure, a.iters, a.theta);
+    }
+    res.iters = failure > gp->max_restarts ? kGluFailure : total;
+  }
   CK(cudaEventRecord(e64->ev1, e64->s));
   if (e64->to_aos(e64->d_aos)) return -1;
   CK(cudaStreamSynchronize(e64->s));
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, e64->ev0, e64->ev1));
-  res.iters = iters;
-  res.theta = th;
-  res.traj_len = tl;
   res.gpu_ms = ms;
   if (r) *r = res;
   return 0;
@@ -1578,7 +1645,8 @@ static int batch_run(Batch *b) {
     if (batch_solve(e32, p32, it32, th32, b->bs)) return -1;
     for (size_t i = 0; i < n; i++) {
       int restart = 0;
-      if (mixed_handover(e64[i], e32[i], p64, &it32[i], th32[i], &restart))
+      // (batches make no random restarts: attempt 0 only)
+      if (mixed_handover(e64[i], e32[i], p64, &it32[i], th32[i], &restart, 0, 0))
         return -1;
       b->inst[i]->res.restarts += restart;
     }
@@ -1683,6 +1751,7 @@ static int check_params(const size_t *dims, const gfix_params *p) {
   if (p->precision != GFIX_FP64 && p->precision != GFIX_MIXED)
     return fail("unknown precision %d", p->precision);
   if (p->traj_cap && !p->traj_theta) return fail("traj_cap without traj_theta");
+  if (p->max_restarts < 0) return fail("max_restarts %d below 0", p->max_restarts);
   return 0;
 }
 
@@ -1716,13 +1785,9 @@ int gfix_landau_device(double *d_links, const size_t dims[4],
   return 0;
 }
 
-int gfix_observables(const double *links, const size_t dims[4], double *out) {
-  if (!links || !dims || !out) return fail("null argument");
-  Engine<double> *e = engine64(dims);
-  if (!e) return -1;
-  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
-  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
-  if (e->from_aos(e->d_aos)) return -1;
+// theta_test_lin, functional and plaquette of the links resident in e's
+// SoA buffer (out[0..2])
+static int observables_resident(Engine<double> *e, double *out) {
   Params p;
   if (e->reset(p)) return -1;
   double tt = 0;
@@ -1742,14 +1807,16 @@ int gfix_observables(const double *links, const size_t dims[4], double *out) {
   return 0;
 }
 
-int gfix_link_diagnostics(const double *links, const size_t dims[4],
-                          double *out) {
-  if (!links || !dims || !out) return fail("null argument");
-  Engine<double> *e = engine64(dims);
-  if (!e) return -1;
+// host links -> e's AoS staging -> e's SoA links
+static int stage_host(Engine<double> *e, const double *links) {
   const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
   CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
-  if (e->from_aos(e->d_aos)) return -1;
+  return e->from_aos(e->d_aos);
+}
+
+// GLU's post-fix link diagnostics of the links resident in e (out[0..5],
+// as gfix_link_diagnostics)
+static int diagnostics_resident(Engine<double> *e, double *out) {
   const int T = e->c.L[3], lcu = e->V / T;
   const int nbs = (lcu + kDiagThreads - 1) / kDiagThreads;
   std::vector<double> part((size_t)kDiagVals * nbs * T);
@@ -1799,17 +1866,37 @@ int gfix_link_diagnostics(const double *links, const size_t dims[4],
   return 0;
 }
 
-int gfix_reunit(double *links, const size_t dims[4]) {
-  if (!links || !dims) return fail("null argument");
-  Engine<double> *e = engine64(dims);
-  if (!e) return -1;
-  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
-  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
-  if (e->from_aos(e->d_aos)) return -1;
+// latt_reunitU of the links resident in e
+static int reunit_resident(Engine<double> *e) {
   const size_t nl = (size_t)e->V * 4;
   k_reunit_links<double><<<(unsigned)((nl + 255) / 256), 256, 0, e->s>>>(
       e->d_U, nl, (size_t)e->V);
   LAUNCHED(1);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int gfix_observables(const double *links, const size_t dims[4], double *out) {
+  if (!links || !dims || !out) return fail("null argument");
+  Engine<double> *e = engine64(dims);
+  if (!e || stage_host(e, links)) return -1;
+  return observables_resident(e, out);
+}
+
+int gfix_link_diagnostics(const double *links, const size_t dims[4],
+                          double *out) {
+  if (!links || !dims || !out) return fail("null argument");
+  Engine<double> *e = engine64(dims);
+  if (!e || stage_host(e, links)) return -1;
+  return diagnostics_resident(e, out);
+}
+
+int gfix_reunit(double *links, const size_t dims[4]) {
+  if (!links || !dims) return fail("null argument");
+  Engine<double> *e = engine64(dims);
+  if (!e || stage_host(e, links)) return -1;
+  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+  if (reunit_resident(e)) return -1;
   if (e->to_aos(e->d_aos)) return -1;
   CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
   CK(cudaStreamSynchronize(e->s));
@@ -1964,6 +2051,64 @@ int gfix_coulomb(double *links, const size_t dims[4], const gfix_params *p,
   if (coulomb_staged(e, p, r, slice_theta, slice_iters)) return -1;
   CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
   CK(cudaStreamSynchronize(e->s));
+  return 0;
+}
+
+// GLU's Landau driver in one device-resident sequence: the solve with its
+// random restarts, then -- when it converged -- output_fixing_info's
+// reunitarisation and diagnostics, all on the links in HBM, so the links
+// cross PCIe once each way.
+int gfix_landau_driver(double *links, const size_t dims[4], const gfix_params *p,
+                       gfix_result *r, double *obs, double *diag) {
+  if (check_params(dims, p)) return -1;
+  if (!links) return fail("null links");
+  Engine<double> *e = engine64(dims);
+  if (!e) return -1;
+  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
+  gfix_result res;
+  if (landau_staged(e, p, &res)) return -1;
+  if (res.iters != kSentinel && res.iters != kGluFailure) {
+    if (reunit_resident(e)) return -1;
+    if (obs && observables_resident(e, obs)) return -1;
+    if (diag && diagnostics_resident(e, diag)) return -1;
+    if (e->to_aos(e->d_aos)) return -1;
+  } else {
+    if (obs) memset(obs, 0, 3 * sizeof(double));
+    if (diag) memset(diag, 0, 6 * sizeof(double));
+  }
+  CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
+  CK(cudaStreamSynchronize(e->s));
+  if (r) *r = res;
+  return 0;
+}
+
+// GLU's Coulomb driver in one device-resident sequence: the diagnostics of
+// the input, the solve of every slice with the slice transforms, the final
+// reunitarisation and the diagnostics of the result.
+int gfix_coulomb_driver(double *links, const size_t dims[4], const gfix_params *p,
+                        gfix_result *r, double *obs_in, double *diag_in,
+                        double *obs, double *diag) {
+  if (check_params(dims, p)) return -1;
+  if (!links) return fail("null links");
+  Engine<double> *e = engine_coul(dims);
+  if (!e) return -1;
+  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
+  if (obs_in || diag_in) {
+    if (e->from_aos(e->d_aos)) return -1;
+    if (obs_in && observables_resident(e, obs_in)) return -1;
+    if (diag_in && diagnostics_resident(e, diag_in)) return -1;
+  }
+  gfix_result res;
+  if (coulomb_staged(e, p, &res, nullptr, nullptr)) return -1;
+  if (reunit_resident(e)) return -1;
+  if (obs && observables_resident(e, obs)) return -1;
+  if (diag && diagnostics_resident(e, diag)) return -1;
+  if (e->to_aos(e->d_aos)) return -1;
+  CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
+  CK(cudaStreamSynchronize(e->s));
+  if (r) *r = res;
   return 0;
 }
 

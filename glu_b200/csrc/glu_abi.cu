@@ -15,6 +15,10 @@
 #include "../../include/glu_gfix.h"
 #include "glu_compat.h"
 
+namespace gfix {
+void set_restart_log(bool on);  // gfix.cu: print GLU's restart messages
+}
+
 using gfix::glu_fftw_stuff;
 using gfix::glu_latt_info;
 using gfix::glu_site;
@@ -27,8 +31,8 @@ __attribute__((weak)) glu_latt_info Latt;
 
 namespace {
 
-constexpr size_t kSentinel = 123456789;
 constexpr size_t kGluFailure = (size_t)-1;  // GLU_FAILURE returned as size_t
+constexpr int kGfGluFailures = 7;           // GF_GLU_FAILURES (GLU_definitions.h:400-402)
 
 // optional precision selection for the drop-in entry points:
 //   GLU_GFIX_PRECISION = FP64 (default) | MIXED
@@ -65,14 +69,34 @@ void scatter(glu_site *lat, const double *buf, size_t V) {
       memcpy(lat[i].O[mu], buf + ((size_t)i * 4 + mu) * 18, 18 * sizeof(double));
 }
 
-struct Pinned {
+// One pinned staging buffer for the whole process, grown on demand: GLU
+// calls these entry points once per configuration with the same lattice,
+// and a fresh cudaMallocHost of the link payload per call costs more than
+// the copies themselves.  Freed at exit.
+struct Staging {
   double *p = nullptr;
-  explicit Pinned(size_t n) {
-    if (cudaMallocHost(&p, n * sizeof(double)) != cudaSuccess) p = nullptr;
-  }
-  ~Pinned() {
+  size_t n = 0;
+  ~Staging() {
     if (p) cudaFreeHost(p);
   }
+  double *get(size_t need) {
+    if (need <= n) return p;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+    if (cudaMallocHost(&p, need * sizeof(double)) != cudaSuccess) {
+      p = nullptr;
+      return nullptr;
+    }
+    n = need;
+    return p;
+  }
+};
+Staging g_stage;
+
+struct Buf {
+  double *p;
+  explicit Buf(size_t n) : p(g_stage.get(n)) {}
 };
 
 size_t landau_fa(glu_site *lat, double *th, double acc, size_t max_iters,
@@ -80,7 +104,7 @@ size_t landau_fa(glu_site *lat, double *th, double acc, size_t max_iters,
   size_t d[4];
   dims_of(d);
   const size_t V = volume();
-  Pinned buf(V * 72);
+  Buf buf(V * 72);
   if (!buf.p) {
     fprintf(stderr, "[FACG] allocation of temporaries failed\n");
     return 0;
@@ -148,8 +172,11 @@ size_t Landau(struct site *lat, const double accuracy, const size_t iter,
   size_t d[4];
   dims_of(d);
   const size_t V = volume();
-  Pinned buf(V * 72);
-  if (!buf.p) return kGluFailure;
+  Buf buf(V * 72);
+  if (!buf.p) {
+    fprintf(stderr, "[GF] allocation of the GPU staging buffer failed\n");
+    return kGluFailure;
+  }
   gather(L, buf.p, V);
   gfix_params p;
   memset(&p, 0, sizeof p);
@@ -161,29 +188,31 @@ size_t Landau(struct site *lat, const double accuracy, const size_t iter,
   p.algo = GFIX_SD;
   p.sd_fixed_step = 1;
 #endif
+  // GLU's restart loop: up to GF_GLU_FAILURES - 1 random restarts
+  // (src/Gfix/Landau.c:322), the transforms seeded by GLU's seed
+  p.max_restarts = kGfGluFailures - 1;
+  p.restart_seed = Latt.Seed[0];
   env_precision(&p);
   gfix_result r;
-  if (gfix_landau(buf.p, d, &p, &r) != 0) {
+  double obs[3] = {0, 0, 0}, dg[6] = {0, 0, 0, 0, 0, 0};
+  gfix::set_restart_log(true);
+  const int rc = gfix_landau_driver(buf.p, d, &p, &r, obs, dg);
+  gfix::set_restart_log(false);
+  if (rc != 0) {
     fprintf(stderr, "[GF] GPU gauge fixing failed: %s\n", gfix_last_error());
     return kGluFailure;
   }
-  if (r.iters == kSentinel) {
-    fprintf(stderr,
-            "\n[GF] Insufficient Convergence ......\n\n"
-            "[GF] -> Try reducing the tuning parameter OR/AND\n"
-            "increasing the maximum number of iterations -< \n\n");
+  // the links of the last attempt go back to the caller either way
+  scatter(L, buf.p, V);
+  if (r.iters == kGluFailure) {
     printf("\n[GF] Failure to converge to a sufficient solution \n"
            "[GF] Please lower the GF_TUNE parameter from %g \n",
            Latt.gf_alpha);
     return kGluFailure;
   }
-  // output_fixing_info (src/Gfix/Landau.c:42-66): reunitarise, report
-  gfix_reunit(buf.p, d);
-  double obs[3] = {0, 0, 0};
-  gfix_observables(buf.p, d, obs);
-  scatter(L, buf.p, V);
-  double dg[6] = {0, 0, 0, 0, 0, 0};
-  gfix_link_diagnostics(buf.p, d, dg);
+  // output_fixing_info (src/Gfix/Landau.c:42-66), computed on the GPU by
+  // the driver: reunitarised links, plaquette, link traces, const_time,
+  // functional
   printf("[GF] Plaquette :: %1.15f \n[GF] Accuracy :: %1.4e\n", obs[2],
          r.theta);
   printf("[GF] Iters :: %zu\n[GF] Link trace :: %1.15f || Maximum :: %1.15f\n",
@@ -201,8 +230,11 @@ size_t Coulomb_FA(struct site *lat, struct fftw_stuff *FFTW,
   size_t d[4];
   dims_of(d);
   const size_t V = volume();
-  Pinned buf(V * 72);
-  if (!buf.p) return 0;
+  Buf buf(V * 72);
+  if (!buf.p) {
+    fprintf(stderr, "[CG] allocation of the GPU staging buffer failed\n");
+    return 0;
+  }
   gather(L, buf.p, V);
   gfix_params p;
   memset(&p, 0, sizeof p);
@@ -225,30 +257,46 @@ size_t Coulomb_FA(struct site *lat, struct fftw_stuff *FFTW,
 }
 
 size_t Coulomb(struct site *lat, const double accuracy, const size_t iter) {
-  size_t it = Coulomb_FA(lat, nullptr, accuracy, iter,
-#ifdef GLU_GFIX_SD
-                         0
-#else
-                         1
-#endif
-  );
-  // latt_reunitU after the fix (src/Gfix/Coulomb.c:97)
   glu_site *L = reinterpret_cast<glu_site *>(lat);
   size_t d[4];
   dims_of(d);
   const size_t V = volume();
-  Pinned buf(V * 72);
-  if (!buf.p) return it;
+  Buf buf(V * 72);
+  if (!buf.p) {
+    fprintf(stderr, "[CG] allocation of the GPU staging buffer failed\n");
+    return 0;
+  }
   gather(L, buf.p, V);
-  gfix_reunit(buf.p, d);
+  gfix_params p;
+  memset(&p, 0, sizeof p);
+  p.gf_alpha = Latt.gf_alpha;
+  p.accuracy = accuracy;
+  p.max_iters = iter;
+#ifdef GLU_GFIX_SD
+  p.algo = GFIX_SD;
+  p.sd_fixed_step = 1;
+#else
+  p.algo = GFIX_CG;
+#endif
+  env_precision(&p);
+  // the initial link traces and plaquette, the solve of every slice, the
+  // final latt_reunitU (src/Gfix/Coulomb.c:97) and the final diagnostics,
+  // in one sequence on the GPU
+  gfix_result r;
+  double obs0[3] = {0, 0, 0}, dg0[6] = {0, 0, 0, 0, 0, 0};
   double obs[3] = {0, 0, 0}, dg[6] = {0, 0, 0, 0, 0, 0};
-  gfix_observables(buf.p, d, obs);
-  gfix_link_diagnostics(buf.p, d, dg);
+  if (gfix_coulomb_driver(buf.p, d, &p, &r, obs0, dg0, obs, dg) != 0) {
+    fprintf(stderr, "[CG] GPU Coulomb gauge fixing failed: %s\n",
+            gfix_last_error());
+    return 0;
+  }
+  printf("[GF] Initial Tlink :: %1.15f || Slink :: %1.15f \n"
+         "[GF] Plaquette :: %1.15f \n", dg0[1], dg0[0], obs0[2]);
   scatter(L, buf.p, V);
   printf("[GF] Tuning :: %f || Iterations :: %zu ||\n[GF] Final Tlink :: %1.15f "
          "|| Slink :: %1.15f \n[GF] Plaquette :: %1.15f \n",
-         Latt.gf_alpha, it, dg[1], dg[0], obs[2]);
-  return it;
+         Latt.gf_alpha, r.iters, dg[1], dg[0], obs[2]);
+  return r.iters;
 }
 
 void FOURIER_ACCELERATE2(struct fftw_stuff *FFTW) {
@@ -290,7 +338,7 @@ int cuts_struct(struct site *lat, const struct cut_info CUTINFO) {
   ci.definition = CUTINFO.definition;
   ci.angle = CUTINFO.angle;
   ci.cyl_width = CUTINFO.cyl_width;
-  Pinned buf(V * 72);
+  Buf buf(V * 72);
   if (!buf.p) {
     fprintf(stderr, "[CUTS] allocation of temporaries failed\n");
     return -1;

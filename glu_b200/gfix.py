@@ -59,7 +59,8 @@ def _links(links, d):
     return a.copy()
 
 
-def _params(alpha, acc, max_iters, algo, sd_fixed, precision, switch, cap):
+def _params(alpha, acc, max_iters, algo, sd_fixed, precision, switch, cap,
+            max_restarts=0, restart_seed=0):
     tt = np.zeros(max(cap, 1))
     tf = np.zeros(max(cap, 1))
     p = GfixParams()
@@ -73,23 +74,33 @@ def _params(alpha, acc, max_iters, algo, sd_fixed, precision, switch, cap):
     p.traj_theta = tt.ctypes.data_as(C.POINTER(C.c_double)) if cap else None
     p.traj_func = tf.ctypes.data_as(C.POINTER(C.c_double)) if cap else None
     p.traj_cap = int(cap)
+    if int(max_restarts) < 0:
+        raise ValueError("max_restarts must be >= 0")
+    p.max_restarts = int(max_restarts)
+    p.restart_seed = int(restart_seed) & 0xFFFFFFFFFFFFFFFF
     return p, tt, tf
 
 
 def landau_fix(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
                algo="FACG", sd_fixed_step=False, precision="FP64",
-               switch_theta=1e-9, traj_cap=0) -> FixResult:
-    """Landau FA gauge fixing (GLU's FACG/FASD) of a copy of `links`."""
+               switch_theta=1e-9, traj_cap=0, max_restarts=0,
+               restart_seed=0) -> FixResult:
+    """Landau FA gauge fixing (GLU's FACG/FASD) of a copy of `links`.
+    max_restarts > 0 adds GLU's random restarts after a failed solve (its
+    Landau driver, src/Gfix/Landau.c:303-340); iters then follows GLU's
+    sums and is GLU_FAILURE when every attempt failed."""
     lib = _lib.load()
     cd, d = _dims(dims)
     U = _links(links, d)
     p, tt, tf = _params(gf_alpha, accuracy, max_iters, algo, sd_fixed_step,
-                        precision, switch_theta, traj_cap)
+                        precision, switch_theta, traj_cap, max_restarts,
+                        restart_seed)
     r = GfixResult()
     check(lib.gfix_landau(U.ctypes.data, cd, C.byref(p), C.byref(r)))
     n = r.traj_len
     return FixResult(U, int(r.iters), float(r.theta), int(r.iters_fp32),
-                     float(r.gpu_ms), tt[:n].copy(), tf[:n].copy())
+                     float(r.gpu_ms), tt[:n].copy(), tf[:n].copy(),
+                     restarts=int(r.restarts))
 
 
 def coulomb_fix(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
@@ -182,13 +193,76 @@ def FASD(links, dims, gf_alpha, acc, max_iters, **kw):
     return r.links, r.iters, r.theta
 
 
+GF_GLU_FAILURES = 7  # src/Headers/GLU_definitions.h:400-402
+
+
+@dataclass
+class DriverResult:
+    links: np.ndarray
+    iters: int
+    theta: float
+    restarts: int
+    plaquette: float = 0.0
+    functional: float = 0.0
+    theta_test: float = 0.0
+    diagnostics: dict = field(default_factory=dict)
+
+
+def landau_driver(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
+                  algo="FACG", sd_fixed_step=False, precision="FP64",
+                  switch_theta=1e-9, max_restarts=GF_GLU_FAILURES - 1,
+                  restart_seed=1) -> DriverResult:
+    """GLU's Landau driver (src/Gfix/Landau.c:261-374) in one pass on the GPU
+    (gfix_landau_driver): the solve with random restarts, then the
+    reunitarised links and output_fixing_info's numbers."""
+    lib = _lib.load()
+    cd, d = _dims(dims)
+    U = _links(links, d)
+    p, _, _ = _params(gf_alpha, accuracy, max_iters, algo, sd_fixed_step,
+                      precision, switch_theta, 0, max_restarts, restart_seed)
+    r = GfixResult()
+    obs = np.zeros(3)
+    dg = np.zeros(6)
+    check(lib.gfix_landau_driver(U.ctypes.data, cd, C.byref(p), C.byref(r),
+                                 obs.ctypes.data_as(C.POINTER(C.c_double)),
+                                 dg.ctypes.data_as(C.POINTER(C.c_double))))
+    return DriverResult(U, int(r.iters), float(r.theta), int(r.restarts),
+                        float(obs[2]), float(obs[1]), float(obs[0]),
+                        dict(splink=dg[0], tlink=dg[1], link=dg[2], link_max=dg[3],
+                             const_lin=dg[4], const_log=dg[5]))
+
+
+def coulomb_driver(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
+                   algo="FACG", sd_fixed_step=False, precision="FP64",
+                   switch_theta=1e-9):
+    """GLU's Coulomb driver (src/Gfix/Coulomb.c:32-106) in one pass on the
+    GPU (gfix_coulomb_driver): (initial, final) DriverResult pair, the final
+    one holding the fixed, reunitarised links."""
+    lib = _lib.load()
+    cd, d = _dims(dims)
+    U = _links(links, d)
+    p, _, _ = _params(gf_alpha, accuracy, max_iters, algo, sd_fixed_step,
+                      precision, switch_theta, 0)
+    r = GfixResult()
+    o0, d0, o1, d1 = np.zeros(3), np.zeros(6), np.zeros(3), np.zeros(6)
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    check(lib.gfix_coulomb_driver(U.ctypes.data, cd, C.byref(p), C.byref(r),
+                                  dp(o0), dp(d0), dp(o1), dp(d1)))
+    diag = lambda g: dict(splink=g[0], tlink=g[1], link=g[2], link_max=g[3],  # noqa: E731
+                          const_lin=g[4], const_log=g[5])
+    first = DriverResult(None, 0, 0.0, 0, float(o0[2]), float(o0[1]), float(o0[0]),
+                         diag(d0))
+    last = DriverResult(U, int(r.iters), float(r.theta), int(r.restarts),
+                        float(o1[2]), float(o1[1]), float(o1[0]), diag(d1))
+    return first, last
+
+
 def Landau(links, dims, gf_alpha, accuracy, max_iters, **kw):
-    """src/Gfix/Landau.c:261 -> (links, iters); iters = GLU_FAILURE when the
-    solve does not converge."""
-    r = landau_fix(links, dims, gf_alpha, accuracy, max_iters, "FACG", **kw)
-    if r.iters == SENTINEL:
-        return r.links, GLU_FAILURE
-    return latt_reunitU(r.links, dims), r.iters
+    """src/Gfix/Landau.c:261 -> (links, iters): the solve with GLU's random
+    restarts and the final reunitarisation; iters = GLU_FAILURE when every
+    attempt failed."""
+    r = landau_driver(links, dims, gf_alpha, accuracy, max_iters, **kw)
+    return r.links, r.iters
 
 
 def Coulomb_FA(links, dims, gf_alpha, accuracy, max_iters, facg=True, **kw):
@@ -200,8 +274,8 @@ def Coulomb_FA(links, dims, gf_alpha, accuracy, max_iters, facg=True, **kw):
 
 def Coulomb(links, dims, gf_alpha, accuracy, max_iters, **kw):
     """src/Gfix/Coulomb.c:32 -> (links, iters), links reunitarised."""
-    U, it = Coulomb_FA(links, dims, gf_alpha, accuracy, max_iters, **kw)
-    return latt_reunitU(U, dims), it
+    _, r = coulomb_driver(links, dims, gf_alpha, accuracy, max_iters, **kw)
+    return r.links, r.iters
 
 
 def observables(links, dims):

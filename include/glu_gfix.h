@@ -69,7 +69,10 @@ void FOURIER_ACCELERATE3(struct fftw_stuff *FFTW);
 /* Landau driver: FA solve, up to GF_GLU_FAILURES-1 random restarts,
  * reunitarisation and the "[GF]" summary.  Replaces
  * src/Gfix/Landau.c:261-374 (src/Headers/Landau.h:51-54).  Restarts use the
- * links as they were on entry instead of re-reading `infile`. */
+ * links as they were on entry (kept on the GPU) instead of re-reading
+ * `infile`, and random gauge transforms from this library's generator
+ * seeded by Latt.Seed[0]; the returned count follows GLU's sums (see
+ * gfix_landau), GLU_FAILURE after the last failed attempt. */
 size_t Landau(struct site *lat, const double accuracy, const size_t iter,
               const char *infile);
 
@@ -114,6 +117,10 @@ typedef struct gfix_params {
   double *traj_theta;    /* optional host arrays, one entry per derivative */
   double *traj_func;     /*   evaluation (theta, gauge functional)         */
   size_t traj_cap;
+  int max_restarts;      /* Landau: random restarts after a failed solve   */
+                         /*   (0: none, as GLU's FACG/FASD; GLU's Landau   */
+                         /*   driver makes GF_GLU_FAILURES - 1 = 6)        */
+  uint64_t restart_seed; /* seed of the restarts' random gauge transforms  */
 } gfix_params;
 
 typedef struct gfix_result {
@@ -122,14 +129,49 @@ typedef struct gfix_result {
   double theta;          /* final in-loop theta                            */
   size_t traj_len;
   double gpu_ms;         /* device time of the solve (CUDA events)         */
-  int restarts;
+  int restarts;          /* random restarts made (Landau: max_restarts;    */
+                         /*   Coulomb: over all slices; also a mixed       */
+                         /*   phase restarted in FP64)                     */
 } gfix_result;
 
 /* Landau FA gauge fixing of host links (double[V][4][9][2]) in place.
  * dims = {Lx, Ly, Lz, Lt}.  Returns 0, or a negative error code (see
- * gfix_last_error). */
+ * gfix_last_error).
+ *
+ * With p->max_restarts = 0 the result is GLU's FACG / FASD
+ * (src/Gfix/FACG.c:341-446): r->iters is the iteration count, or the
+ * sentinel 123456789 when the solve did not converge.  With max_restarts >
+ * 0 a failed solve is retried as GLU's Landau driver does
+ * (src/Gfix/Landau.c:303-340): the links as they were on entry (kept on the
+ * GPU; GLU re-reads its input file), a random SU(3) gauge transform
+ * (seeded by restart_seed and the attempt; GLU's random_transform draws
+ * from its own generator), a new solve -- up to max_restarts times.
+ * r->iters then follows GLU's accounting: the first attempt's sentinel,
+ * plus max_iters per failed restart, plus the successful attempt's count;
+ * (size_t)-1 (GLU_FAILURE) when every attempt failed, the links then being
+ * the last attempt's.  r->restarts counts the restarts made. */
 int gfix_landau(double *links, const size_t dims[4], const gfix_params *p,
                 gfix_result *r);
+
+/* GLU's Landau driver (src/Gfix/Landau.c:261-374) as one device-resident
+ * sequence: gfix_landau (with p->max_restarts random restarts; Landau()
+ * passes GF_GLU_FAILURES - 1 = 6) and, when it converged, output_fixing_info
+ * (Landau.c:42-66): the links reunitarised (latt_reunitU), then obs[0..2] as
+ * gfix_observables and diag[0..5] as gfix_link_diagnostics of the result.
+ * The links cross PCIe once each way.  On failure (r->iters = (size_t)-1,
+ * or the sentinel with max_restarts = 0) the links are the last attempt's,
+ * not reunitarised, and obs / diag are zero.  obs, diag may be NULL. */
+int gfix_landau_driver(double *links, const size_t dims[4], const gfix_params *p,
+                       gfix_result *r, double *obs, double *diag);
+
+/* GLU's Coulomb driver (src/Gfix/Coulomb.c:32-106) as one device-resident
+ * sequence: obs_in / diag_in of the input (GLU prints the initial link
+ * traces and plaquette), gfix_coulomb, latt_reunitU, obs / diag of the
+ * result (layouts as gfix_observables / gfix_link_diagnostics; each may be
+ * NULL).  The links cross PCIe once each way. */
+int gfix_coulomb_driver(double *links, const size_t dims[4], const gfix_params *p,
+                        gfix_result *r, double *obs_in, double *diag_in,
+                        double *obs, double *diag);
 
 /* As gfix_landau, but `d_links` is a device pointer to the same layout
  * (links already resident in HBM); nothing crosses PCIe but scalars. */
