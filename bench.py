@@ -273,14 +273,19 @@ def gpu_arm(args, dims, rank, world, local):
         check(lib.gfix_landau(hwork.data_ptr(), cd, C.byref(p), C.byref(r)))
         return r
 
-    def plaquette(ptr):
+    def plaquette(ptr, reunit=False):
+        if reunit:
+            check(lib.gfix_reunit(ptr, cd))
         o = np.zeros(3)
         check(lib.gfix_observables(ptr, cd, o.ctypes.data_as(C.POINTER(C.c_double))))
         return float(o[2])
 
     # every fixed configuration must stay on its input's gauge orbit: the
     # average plaquette of the last step's fixed links (host side, after
-    # the timed region) against the input's
+    # the timed region), reunitarised as GLU's Landau driver does before it
+    # reports (output_fixing_info: over a long fix the links drift off
+    # SU(3) through GLU's update, which rebuilds one column from the other
+    # two), against the input's
     plaq_in = [plaquette(h.data_ptr()) for h in hosts]
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
@@ -321,7 +326,8 @@ def gpu_arm(args, dims, rank, world, local):
                     torch.cuda.synchronize()
                     e_ms += a2.elapsed_time(b2)
                     if k == args.steps - 1:
-                        drift = max(drift, abs(plaquette(hwork.data_ptr()) - plaq_in[i]))
+                        drift = max(drift, abs(plaquette(hwork.data_ptr(), True)
+                                               - plaq_in[i]))
             e_ms = max_over_ranks(e_ms)
             if not drift < PLAQ_TOL:
                 raise RuntimeError(f"{prec}: a fixed configuration left its gauge orbit "
@@ -393,6 +399,57 @@ def cpu_sample(U, dims, sample_s: float, nthreads: int, algo: str = "FACG"):
                 sample_s=t1 + t2)
 
 
+def physical_cores() -> int | None:
+    """Physical cores of this host (distinct core, socket pairs of lscpu),
+    or None when lscpu is unavailable."""
+    try:
+        out = subprocess.run(["lscpu", "-p=CORE,SOCKET"], capture_output=True,
+                             text=True, timeout=10).stdout
+        pairs = {ln.strip() for ln in out.splitlines() if ln and not ln.startswith("#")}
+        return len(pairs) or None
+    except Exception:
+        return None
+
+
+def recorded_seconds(dims):
+    """Wall seconds of the reference's own full fixes of the step's
+    configurations (profiles/reference_full_fix.json), or None."""
+    f = ROOT / "profiles" / "reference_full_fix.json"
+    if not f.exists():
+        return None
+    rec = {e.get("input"): e for e in json.loads(f.read_text())
+           if tuple(e["dims"]) == tuple(dims) and "seconds" in e}
+    es = [rec.get(INPUT_NAME % sd) for sd in seeds(0)]
+    if any(e is None for e in es):
+        return None
+    return sum(float(e["seconds"]) for e in es), int(es[0].get("threads", 0))
+
+
+def reference_model(s, n_ref, dims):
+    """The reference's time for one step (the step's full fixes) from a
+    sample `s` of cpu_sample: fixed cost per call + seconds per iteration x
+    the full fixes' iteration counts.  Beside it the same with the FFT phase
+    taken out: the reference's Fourier acceleration runs its four fields'
+    transforms one per thread (an omp for over the fields), so the phase
+    lasts the FFT stand-in's thread-seconds / min(4, threads) of wall time
+    per iteration.  And the recorded wall time of the reference's own full
+    fixes, when present, with the model's deviation from it."""
+    t_set = E_CONFIGS * s["fixed_s"] + s["s_iter"] * sum(n_ref)
+    fft_wall = s["fft_thread_s_iter"] / max(1, min(4, s["cores"]))
+    t_nofft = E_CONFIGS * s["fixed_s"] + max(s["s_iter"] - fft_wall, 0.0) * sum(n_ref)
+    out = {"value": E_CONFIGS * 3600.0 / t_set, "t_set": t_set,
+           "value_excluding_fft": E_CONFIGS * 3600.0 / t_nofft,
+           "fft_wall_s_per_iteration": fft_wall,
+           "s_per_iteration_excluding_fft": max(s["s_iter"] - fft_wall, 0.0),
+           "threads": s["cores"], "physical_cores": physical_cores()}
+    rec = recorded_seconds(dims)
+    if rec is not None:
+        out["recorded_full_fix_seconds"] = rec[0]
+        out["recorded_threads"] = rec[1]
+        out["model_deviation"] = t_set / rec[0] - 1.0
+    return out
+
+
 def emit(d):
     print(json.dumps(d), flush=True)
 
@@ -419,9 +476,13 @@ def reference_arm(args, dims, rank, world):
               "no recorded full-fix iteration counts for dims %s" % (dims,)})
         return
     # one step: the E_CONFIGS fixes, each GLU's recorded iteration count
-    t_set = E_CONFIGS * fixed + s_iter * sum(n_ref)
-    value = E_CONFIGS * 3600.0 / t_set
     s0 = samples[0]
+    model = reference_model(dict(s0, s_iter=s_iter, fixed_s=fixed,
+                                 fft_thread_s_iter=statistics.median(
+                                     x["fft_thread_s_iter"] for x in samples)),
+                            n_ref, dims)
+    t_set = model["t_set"]
+    value = model["value"]
     emit({"metric": metric_name(dims), "value": value, "unit": UNIT, "n_gpus": world,
           "steps": args.steps, "warmup": args.warmup,
           "ms_per_step": t_set * 1e3, "higher_is_better": True,
@@ -435,10 +496,15 @@ def reference_arm(args, dims, rank, world):
                      "full_fix_iters": n_ref, "parallelism": "host OpenMP"},
           "impl": "reference",
           "cpu_baseline": {"value": value, "unit": UNIT, "cores": s0["cores"],
+                           "physical_cores": model["physical_cores"],
                            "kind": s0["kind"],
+                           "value_excluding_fft": model["value_excluding_fft"],
+                           "model": {k: v for k, v in model.items() if k != "t_set"},
                            "sample": "%d x %d FACG iterations per step, "
-                                     "%.3f s/iteration x %s iterations" %
-                                     (len(samples), s0["sample_iters"], s_iter, n_ref)},
+                                     "%.3f s/iteration (%.3f without the FFT phase) "
+                                     "x %s iterations" %
+                                     (len(samples), s0["sample_iters"], s_iter,
+                                      model["s_per_iteration_excluding_fft"], n_ref)},
           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                   "d2h_bytes_per_step": 0}})
 
@@ -632,14 +698,19 @@ def coulomb_gpu(args, dims, rank, world, local):
                  sit.ctypes.data_as(C.POINTER(C.c_size_t))))
         return r
 
-    def plaquette(ptr):
+    def plaquette(ptr, reunit=False):
+        if reunit:
+            check(lib.gfix_reunit(ptr, cd))
         o = np.zeros(3)
         check(lib.gfix_observables(ptr, cd, o.ctypes.data_as(C.POINTER(C.c_double))))
         return float(o[2])
 
     # every fixed configuration must stay on its input's gauge orbit: the
     # average plaquette of the last step's fixed links (host side, after
-    # the timed region) against the input's
+    # the timed region), reunitarised as GLU's Landau driver does before it
+    # reports (output_fixing_info: over a long fix the links drift off
+    # SU(3) through GLU's update, which rebuilds one column from the other
+    # two), against the input's
     plaq_in = [plaquette(h.data_ptr()) for h in hosts]
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
@@ -1041,14 +1112,19 @@ def ensemble_main(args, rank, world, local):
     cds = [(C.c_size_t * 4)(*d) for d, _ in cfgs]
     nbytes = sum(t.numel() * 8 for t in pristine)
     sites = sum(int(np.prod(d)) for d, _ in cfgs)
-    def plaquette(ptr):
+    def plaquette(ptr, reunit=False):
+        if reunit:
+            check(lib.gfix_reunit(ptr, cd))
         o = np.zeros(3)
         check(lib.gfix_observables(ptr, cd, o.ctypes.data_as(C.POINTER(C.c_double))))
         return float(o[2])
 
     # every fixed configuration must stay on its input's gauge orbit: the
     # average plaquette of the last step's fixed links (host side, after
-    # the timed region) against the input's
+    # the timed region), reunitarised as GLU's Landau driver does before it
+    # reports (output_fixing_info: over a long fix the links drift off
+    # SU(3) through GLU's update, which rebuilds one column from the other
+    # two), against the input's
     plaq_in = [plaquette(h.data_ptr()) for h in hosts]
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
@@ -1549,13 +1625,16 @@ def main():
             if n_ref is None:  # our FP64 counts stand in for GLU's
                 n_ref = [x[0] for x in res["out"]["fp64"]["per"]]
                 src = "our FP64 fixes' counts"
-            t_set = E_CONFIGS * s["fixed_s"] + s["s_iter"] * sum(n_ref)
-            cpu = {"value": E_CONFIGS * 3600.0 / t_set, "unit": UNIT, "cores": s["cores"],
-                   "kind": s["kind"],
+            model = reference_model(s, n_ref, dims)
+            cpu = {"value": model["value"], "unit": UNIT, "cores": s["cores"],
+                   "physical_cores": model["physical_cores"], "kind": s["kind"],
+                   "value_excluding_fft": model["value_excluding_fft"],
+                   "model": {k: v for k, v in model.items() if k != "t_set"},
                    "sample": "%d FACG iterations (%.1f s); %.3f s/iteration x %s "
-                             "iterations (%s); FFT stand-in %.3f thread-s/iteration"
+                             "iterations (%s); FFT stand-in %.3f thread-s/iteration "
+                             "(%.3f s of wall time)"
                              % (s["sample_iters"], s["sample_s"], s["s_iter"], n_ref, src,
-                                s["fft_thread_s_iter"])}
+                                s["fft_thread_s_iter"], model["fft_wall_s_per_iteration"])}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "kind": "unavailable", "sample": str(e)}
     if rank == 0:

@@ -47,7 +47,8 @@ EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
            "gfix_batch_add", "gfix_batch_add_device", "gfix_batch_run",
            "gfix_batch_result", "gfix_batch_destroy", "gfix_coulomb_slices",
            "gfix_coulomb_slices_finish", "gfix_fft_tuning", "gfix_fft_plan",
-           "gfix_link_diagnostics", "gfix_nersc_decode", "gfix_nersc_encode",
+           "gfix_link_diagnostics", "gfix_gf_check", "gfix_nersc_decode",
+           "gfix_nersc_encode",
            "gfix_nersc_error", "gfix_scidac_checksum", "gfix_cut_veclist",
            "gfix_cuts_measure", "gfix_cuts_measure_device", "gfix_cuts_write",
            "gfix_profile_cuts", "gfix_cuts_error", "gfix_cuts_release",
@@ -127,6 +128,8 @@ def load(path: Path | str | None = None):
     lib.gfix_cuts_release.restype = None
     lib.gfix_nersc_error.restype = C.c_char_p
     lib.gfix_nersc_error.argtypes = []
+    lib.gfix_gf_check.restype = C.c_int
+    lib.gfix_gf_check.argtypes = [C.c_void_p, _szp, _dp]
     lib.gfix_link_diagnostics.restype = C.c_int
     lib.gfix_link_diagnostics.argtypes = [C.c_void_p, _szp, _dp]
     lib.gfix_reunit.restype = C.c_int

@@ -204,4 +204,101 @@ __global__ void k_random_gauge(cx<double> *G, int V, unsigned long long seed,
   for (int e = 0; e < 9; e++) G[(size_t)e * V + s] = g[e];
 }
 
+// GLU's gauge-fixing accuracy report (gf_check, src/Wrappers/OBS_wrap.c:
+// 93-126): per site the lattice derivative sum_mu [A_mu(x - mu) - A_mu(x)]
+// of the Hermitian fields A of the links, by the linear definition
+// (Hermitian_proj_short, as theta_test_lin, src/Gfix/gftests.c:214-250)
+// and the logarithmic one (exact_log_slow_short, as theta_test_log,
+// gftests.c:253-290, through log_deriv, src/Gfix/log_derivs.c:29-50), over
+// the four directions (Landau) and the three spatial ones (Coulomb); the
+// local value is trace_deriv (src/Gfix/lin_derivs.c:29-52).  Per block:
+// the sums of the four local values and their maxima, kGfcVals doubles.
+constexpr int kGfcVals = 8;
+
+__device__ __forceinline__ double gfc_trace_deriv(const double *r) {
+  // r = {Re s0, Re s3, s1, s2, s4 (re, im)}
+  return 4.0 * (r[0] * r[0] + r[1] * r[1] + r[0] * r[1] + r[2] * r[2] + r[3] * r[3] +
+                r[4] * r[4] + r[5] * r[5] + r[6] * r[6] + r[7] * r[7]);
+}
+
+// the eight reals of a short Hermitian field: linear definition
+__device__ __forceinline__ void gfc_lin(const cx<double> *u, double *a) {
+  double q0, q3;
+  cx<double> q1, q2, q4;
+  herm_short(u, q0, q1, q2, q3, q4);
+  a[0] = q0;
+  a[1] = q3;
+  a[2] = q1.x;
+  a[3] = q1.y;
+  a[4] = q2.x;
+  a[5] = q2.y;
+  a[6] = q4.x;
+  a[7] = q4.y;
+}
+
+// logarithmic definition: (Re Q00, Re Q11, Q01, Q02, Q12)
+__device__ __forceinline__ void gfc_log(const cx<double> *u, double *a) {
+  cx<double> q[4];
+  su3log::log_components(u, q);
+  a[0] = q[0].x;
+  a[1] = q[0].y;
+  a[2] = q[1].x;
+  a[3] = q[1].y;
+  a[4] = q[2].x;
+  a[5] = q[2].y;
+  a[6] = q[3].x;
+  a[7] = q[3].y;
+}
+
+__global__ void __launch_bounds__(kSiteThreads) k_gf_check(Ctx<double> c) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  // {lin 4D, log 4D, lin 3D, log 3D}
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  if (s < c.V) {
+    int x[4], sd[4];
+    coords(s, c.L, x);
+    strides(c, sd);
+    double sl[8] = {0, 0, 0, 0, 0, 0, 0, 0}, sg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+    for (int mu = 0; mu < 4; mu++) {
+      cx<double> u[9], b[9];
+      load_link(c.U, c.V, mu, s, u);
+      load_link(c.U, c.V, mu, bck_site(s, mu, x, c.L, sd), b);
+      double a[8], ab[8];
+      gfc_lin(u, a);
+      gfc_lin(b, ab);
+#pragma unroll
+      for (int k = 0; k < 8; k++) sl[k] += ab[k] - a[k];
+      gfc_log(u, a);
+      gfc_log(b, ab);
+#pragma unroll
+      for (int k = 0; k < 8; k++) sg[k] += ab[k] - a[k];
+      if (mu == 2) {
+        v[2] = gfc_trace_deriv(sl);
+        v[3] = gfc_trace_deriv(sg);
+      }
+    }
+    v[0] = gfc_trace_deriv(sl);
+    v[1] = gfc_trace_deriv(sg);
+  }
+  double m[4] = {v[0], v[1], v[2], v[3]};
+  double *out = c.part + (size_t)kGfcVals * blockIdx.x;
+  block_sum_store<4>(v, out);
+  __shared__ double smax[4][kSiteThreads / 32];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m[k] = fmax(m[k], __shfl_down_sync(0xffffffffu, m[k], o));
+    if ((threadIdx.x & 31) == 0) smax[k][threadIdx.x >> 5] = m[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 4; k++) {
+      double mm = smax[k][0];
+      for (int w = 1; w < (int)(blockDim.x >> 5); w++) mm = fmax(mm, smax[k][w]);
+      out[4 + k] = mm;
+    }
+  }
+}
+
 }  // namespace gfix

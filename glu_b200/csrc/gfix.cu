@@ -1866,6 +1866,45 @@ static int diagnostics_resident(Engine<double> *e, double *out) {
   return 0;
 }
 
+// gf_check of the links resident in e: out[0..9] as gfix_gf_check
+static int gf_check_resident(Engine<double> *e, double *out) {
+  const int nb = e->nb_site;
+  double *d_p = nullptr;
+  CK(cudaMalloc(&d_p, (size_t)nb * kGfcVals * sizeof(double)));
+  Ctx<double> c = e->c;
+  c.part = d_p;
+  k_gf_check<<<nb, kSiteThreads, 0, e->s>>>(c);
+  LAUNCHED(1);
+  std::vector<double> part((size_t)nb * kGfcVals);
+  const cudaError_t err = cudaMemcpyAsync(part.data(), d_p, part.size() * sizeof(double),
+                                          cudaMemcpyDeviceToHost, e->s);
+  const cudaError_t err2 = cudaStreamSynchronize(e->s);
+  cudaFree(d_p);
+  CK(err);
+  CK(err2);
+  // fixed-order sums; theta = 2 sum / (NC V) (gftests.c:249, :289)
+  double sum[4] = {0, 0, 0, 0}, mx[4] = {0, 0, 0, 0};
+  for (int b = 0; b < nb; b++)
+    for (int k = 0; k < 4; k++) {
+      sum[k] += part[(size_t)b * kGfcVals + k];
+      mx[k] = std::max(mx[k], part[(size_t)b * kGfcVals + 4 + k]);
+    }
+  const double V = (double)e->V;
+  double dg[6];
+  if (diagnostics_resident(e, dg)) return -1;
+  out[0] = 2.0 * sum[0] / (3.0 * V);
+  out[1] = mx[0];
+  out[2] = 2.0 * sum[1] / (3.0 * V);
+  out[3] = mx[1];
+  out[4] = dg[4];
+  out[5] = dg[5];
+  out[6] = 2.0 * sum[2] / (3.0 * V);
+  out[7] = mx[2];
+  out[8] = 2.0 * sum[3] / (3.0 * V);
+  out[9] = mx[3];
+  return 0;
+}
+
 // latt_reunitU of the links resident in e
 static int reunit_resident(Engine<double> *e) {
   const size_t nl = (size_t)e->V * 4;
@@ -1889,6 +1928,13 @@ int gfix_link_diagnostics(const double *links, const size_t dims[4],
   Engine<double> *e = engine64(dims);
   if (!e || stage_host(e, links)) return -1;
   return diagnostics_resident(e, out);
+}
+
+int gfix_gf_check(const double *links, const size_t dims[4], double *out) {
+  if (!links || !dims || !out) return fail("null argument");
+  Engine<double> *e = engine64(dims);
+  if (!e || stage_host(e, links)) return -1;
+  return gf_check_resident(e, out);
 }
 
 int gfix_reunit(double *links, const size_t dims[4]) {

@@ -333,6 +333,37 @@ def link_diagnostics(links, dims) -> dict:
                 const_lin=out[4], const_log=out[5])
 
 
+def gf_check(links, dims) -> dict:
+    """GLU's gauge-fixing accuracy report (gf_check, OBS_wrap.c:93-126):
+    theta_test_lin / theta_test_log and their largest local values over the
+    four (landau_*) and the three spatial (coulomb_*) directions, and the
+    temporal constancy of both definitions."""
+    lib = _lib.load()
+    cd, d = _dims(dims)
+    U = _links(links, d)
+    o = np.zeros(10)
+    check(lib.gfix_gf_check(U.ctypes.data, cd, o.ctypes.data_as(C.POINTER(C.c_double))))
+    return dict(landau_lin=o[0], landau_lin_max=o[1], landau_log=o[2],
+                landau_log_max=o[3], const_lin=o[4], const_log=o[5],
+                coulomb_lin=o[6], coulomb_lin_max=o[7], coulomb_log=o[8],
+                coulomb_log_max=o[9])
+
+
+def gf_check_report(r: dict) -> str:
+    """The [GFACC] lines GLU prints for gf_check's numbers."""
+    return ("[GFACC] Looking at Landau Gauge-Fixing Information \n"
+            f"[GFACC LANDAU]      LIN :: {r['landau_lin']:1.6e} \n"
+            f"[GFACC MAX LANDAU]  LIN :: {r['landau_lin_max']:1.6e} \n"
+            f"[GFACC LANDAU]      LOG :: {r['landau_log']:1.6e} \n"
+            f"[GFACC MAX LANDAU]  LOG :: {r['landau_log_max']:1.6e} \n"
+            f"[GFACC] Temporal constance || LIN {r['const_lin']:e} || Log {r['const_log']:e} "
+            "\n[GFACC] Looking at Coulomb Gauge-Fixing Information \n"
+            f"[GFACC COULOMB]     LIN :: {r['coulomb_lin']:1.6e} \n"
+            f"[GFACC MAX COULOMB] LIN :: {r['coulomb_lin_max']:1.6e} \n"
+            f"[GFACC COULOMB]     LOG :: {r['coulomb_log']:1.6e} \n"
+            f"[GFACC MAX COULOMB] LOG :: {r['coulomb_log_max']:1.6e} \n\n")
+
+
 def fft_tuning(on: bool):
     """Autotuned FFT plans per lattice shape (True) or the fixed default
     plans (False, bit-reproducible); see gfix_fft_tuning."""

@@ -249,6 +249,16 @@ int gfix_observables(const double *links, const size_t dims[4], double *out);
 int gfix_link_diagnostics(const double *links, const size_t dims[4],
                           double *out);
 
+/* GLU's gauge-fixing accuracy report (gf_check, src/Wrappers/OBS_wrap.c:
+ * 93-126) of host links: out[0] theta_test_lin and out[1] its largest local
+ * value over the four directions (Landau; src/Gfix/gftests.c:214-250),
+ * out[2], out[3] the same by the logarithmic definition (theta_test_log,
+ * gftests.c:253-290), out[4], out[5] the temporal constancy (const_time,
+ * linear and logarithmic), out[6..9] as out[0..3] over the three spatial
+ * directions (Coulomb).  out holds 10.  A link whose three eigenvalue
+ * phases are equal (the identity) contributes a zero logarithm. */
+int gfix_gf_check(const double *links, const size_t dims[4], double *out);
+
 /* Reunitarise every link (GLU's latt_reunitU, src/Geometry/random_config.c:
  * 42-57) on the GPU, host links in place. */
 int gfix_reunit(double *links, const size_t dims[4]);

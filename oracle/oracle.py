@@ -218,6 +218,8 @@ class Reference:
         L.ref_indivlinks.argtypes = [_dp]
         L.ref_const_time.restype = None
         L.ref_const_time.argtypes = [_dp, _dp]
+        L.ref_gf_check.restype = None
+        L.ref_gf_check.argtypes = [_dp]
         L.ref_landau_fa.restype = _sz
         L.ref_landau_fa.argtypes = [C.c_int, C.c_double, _sz, _dp, _dp, _dp,
                                     _sz, _szp]
@@ -297,6 +299,14 @@ class Reference:
         self.lib.ref_const_time(_ptr(lin), _ptr(lg))
         return (float(sp[0]), float(t[0]), float(al), float(avg), float(mx[0]),
                 float(lin[0]), float(lg[0]))
+
+    def gf_check(self):
+        """GLU's gf_check numbers of the lattice in place: (Landau lin, its
+        max, Landau log, its max, const_time lin, log, Coulomb lin, max,
+        Coulomb log, max)."""
+        out = np.zeros(10)
+        self.lib.ref_gf_check(_ptr(out))
+        return out
 
     def landau_fa(self, acc, max_iters, algo="FACG", traj_cap=0):
         th = np.zeros(1)

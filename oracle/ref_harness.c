@@ -153,6 +153,22 @@ double ref_indivlinks(double *max) {
 }
 void ref_const_time(double *lin, double *lg) { const_time(g_lat, lin, lg); }
 
+/* the numbers of GLU's gf_check report (src/Wrappers/OBS_wrap.c:93-126):
+ * theta_test_lin / _log with their maxima over ND and ND - 1 directions,
+ * and const_time; out[10] in the order the report prints them */
+void ref_gf_check(double *out) {
+  GLU_real mx = 0.;
+  out[0] = theta_test_lin(g_lat, &mx, ND);
+  out[1] = mx;
+  out[2] = theta_test_log(g_lat, &mx, ND);
+  out[3] = mx;
+  const_time(g_lat, &out[4], &out[5]);
+  out[6] = theta_test_lin(g_lat, &mx, ND - 1);
+  out[7] = mx;
+  out[8] = theta_test_log(g_lat, &mx, ND - 1);
+  out[9] = mx;
+}
+
 /* GLU's writer (src/IO/writers.c:329-420, write_configuration): storage
  * is a GLU_output value (OUTPUT_ILDG, OUTPUT_GAUGE, ...) */
 int ref_write_config(const char *path, int storage, const char *details) {

@@ -219,3 +219,33 @@ def test_random_odd_lattice_against_oracle(oracle):
     # scale of the run, not of the tiny last value
     assert np.all(np.abs(r.traj_theta - ot) <= 1e-11 * ot + 1e-14 * ot[0])
     assert np.abs(r.links - o["links"]).max() < 1e-12
+
+
+@pytest.mark.parametrize("case, which", [("lat400", "links"),
+                                         ("lat400", "landau_facg_links"),
+                                         ("lat400", "coulomb_facg_links"),
+                                         ("hb8", "links")])
+def test_gf_check_matches_reference(reference, case, which, request):
+    """GLU's gf_check numbers (theta_test_lin and theta_test_log with their
+    largest local values, over four and three directions, and const_time)
+    against GLU itself on the same links.  On fixed links theta is a sum of
+    squares of rounding-sized derivatives, so the comparison there is
+    relative to GLU's own rounding (1e-6), elsewhere 1e-12."""
+    g = request.getfixturevalue(case)
+    d = _dims(g)
+    U = g[which]
+    got = gfix.gf_check(U, d)
+    reference.setup(d, 1, 0.08)
+    reference.put_links(U)
+    ref = reference.gf_check()
+    keys = ["landau_lin", "landau_lin_max", "landau_log", "landau_log_max",
+            "const_lin", "const_log", "coulomb_lin", "coulomb_lin_max",
+            "coulomb_log", "coulomb_log_max"]
+    for k, r in zip(keys, ref):
+        tol = 1e-6 if r < 1e-8 else 1e-11
+        # const_time is a difference of slice sums of O(1) entries: its
+        # rounding floor is ~1e-15 absolute
+        floor = 1e-15 if k.startswith("const") else 1e-300
+        assert abs(got[k] - r) <= tol * abs(r) + floor, (k, got[k], r)
+    text = gfix.gf_check_report(got)
+    assert "[GFACC LANDAU]      LOG ::" in text and "[GFACC MAX COULOMB] LOG ::" in text
