@@ -46,18 +46,31 @@ __global__ void __launch_bounds__(kSiteThreads) k_plaquette(Ctx<R> c) {
   block_sum_store<1>(v, c.part + blockIdx.x);
 }
 
+// latt_reunitU (src/Geometry/random_config.c:42-57) of the links (stored
+// as their first two columns: the Gram-Schmidt needs no third)
 template <typename R>
-__global__ void k_reunit_links(cx<R> *U, size_t nlinks, size_t V) {
+__global__ void k_reunit_links(cx<R> *U, int V) {
   const size_t l = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (l >= nlinks) return;
-  const size_t mu = l / V, s = l % V;
+  if (l >= 4 * (size_t)V) return;
+  const int mu = (int)(l / V), s = (int)(l % V);
   cx<R> u[9];
-  cx<R> *p = U + mu * 9 * V + s;
+  load_link(U, V, mu, s, u);
+  gram_reunit(u);
+  store_link(U, V, mu, s, u);
+}
+
+// the same for n full matrices G[9][n] (gauge transforms)
+template <typename R>
+__global__ void k_reunit_mats(cx<R> *G, size_t n) {
+  const size_t s = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  cx<R> u[9];
+  cx<R> *p = G + s;
 #pragma unroll
-  for (int e = 0; e < 9; e++) u[e] = p[(size_t)e * V];
+  for (int e = 0; e < 9; e++) u[e] = p[(size_t)e * n];
   gram_reunit(u);
 #pragma unroll
-  for (int e = 0; e < 9; e++) p[(size_t)e * V] = u[e];
+  for (int e = 0; e < 9; e++) p[(size_t)e * n] = u[e];
 }
 
 // Link diagnostics of GLU's output (src/Field/plaqs_links.c:399-446,

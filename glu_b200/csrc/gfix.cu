@@ -309,7 +309,7 @@ class Engine {
     CK(cudaMallocHost(&h_st, sizeof(DevState)));
     memset(h_st, 0, sizeof(DevState));
     c.st = d_st;
-    CK(cudaMalloc(&d_U, (size_t)V * 36 * sizeof(cx<R>)));
+    CK(cudaMalloc(&d_U, (size_t)V * 4 * kLinkCx * sizeof(cx<R>)));
     CK(cudaMalloc(&d_F, (size_t)V * 16 * sizeof(cx<R>)));
     c.U = d_U;
     c.fb[0] = d_F;
@@ -871,9 +871,11 @@ class Engine {
     const double B = sizeof(cx<R>) * (double)V;  // one complex per site
     // update: links in and out, the direction; with G (the FP32 phase of
     // mixed precision) also the accumulated transform in and out
-    const double b[7] = {(36 + 4) * B, 8 * B, 8 * B, 12 * B,
-                         (36 + 4 + 4 + 4) * B,
-                         (36 + 4 + 36 + (c.G ? 18 : 0)) * B, 0.0};
+    // (links: 4 kLinkCx complex numbers per site, their first two columns)
+    const double L4 = 4.0 * kLinkCx;
+    const double b[7] = {(L4 + 4) * B, 8 * B, 8 * B, 12 * B,
+                         (L4 + 4 + 4 + 4) * B,
+                         (L4 + 4 + L4 + (c.G ? 18 : 0)) * B, 0.0};
     for (int k = 0; k < 7; k++) {
       ms[k] = acc[k] / n;
       if (bytes) bytes[k] = b[k];
@@ -1172,8 +1174,9 @@ class Engine {
     // derivative: 3 links, g, 4 fields out; FFT passes: 4 fields in and out
     // (+ in_old for the sums); probes: in, sn_old, sn out, 3 links, g;
     // update: sn, g in and out
-    const double b[7] = {(27 + 9 + 4) * B, 8 * B, 8 * B, 12 * B,
-                         (4 + 4 + 4 + 27 + 9) * B, (4 + 9 + 9) * B, 0.0};
+    const double L3 = 3.0 * kLinkCx;  // the three spatial links
+    const double b[7] = {(L3 + 9 + 4) * B, 8 * B, 8 * B, 12 * B,
+                         (4 + 4 + 4 + L3 + 9) * B, (4 + 9 + 9) * B, 0.0};
     for (int k = 0; k < 7; k++) {
       ms[k] = acc[k] / n;
       if (bytes) bytes[k] = b[k];
@@ -1374,7 +1377,7 @@ static int landau_attempt(Engine<double> *e64, const gfix_params *gp,
     if (!e32) return -1;
     // e32 runs on e64's stream order: synchronise the two streams
     CK(cudaStreamSynchronize(e64->s));
-    const size_t n = (size_t)e64->V * 36;
+    const size_t n = (size_t)e64->V * 4 * kLinkCx;
     k_convert<double, float><<<1184, 256, 0, e32->s>>>(e64->d_U, e32->d_U, n);
     k_identity<float><<<(e64->V + 255) / 256, 256, 0, e32->s>>>(e32->d_G,
                                                                 e64->V);
@@ -1634,7 +1637,7 @@ static int batch_run(Batch *b) {
       e32[i] = I.e32.get();
       CK(cudaStreamSynchronize(e64[i]->s));
       k_convert<double, float><<<1184, 256, 0, e32[i]->s>>>(
-          e64[i]->d_U, e32[i]->d_U, (size_t)e64[i]->V * 36);
+          e64[i]->d_U, e32[i]->d_U, (size_t)e64[i]->V * 4 * kLinkCx);
       k_identity<float><<<(e64[i]->V + 255) / 256, 256, 0, e32[i]->s>>>(
           e32[i]->d_G, e64[i]->V);
       LAUNCHED(2);
@@ -1908,8 +1911,8 @@ static int gf_check_resident(Engine<double> *e, double *out) {
 // latt_reunitU of the links resident in e
 static int reunit_resident(Engine<double> *e) {
   const size_t nl = (size_t)e->V * 4;
-  k_reunit_links<double><<<(unsigned)((nl + 255) / 256), 256, 0, e->s>>>(
-      e->d_U, nl, (size_t)e->V);
+  k_reunit_links<double><<<(unsigned)((nl + 255) / 256), 256, 0, e->s>>>(e->d_U,
+                                                                         e->V);
   LAUNCHED(1);
   CK(cudaGetLastError());
   return 0;
@@ -2003,7 +2006,7 @@ int gfix_profile_landau(const double *d_links, const size_t dims[4],
     if (!f) return -1;
     CK(cudaStreamSynchronize(e->s));
     k_convert<double, float><<<1184, 256, 0, f->s>>>(e->d_U, f->d_U,
-                                                     (size_t)e->V * 36);
+                                                     (size_t)e->V * 4 * kLinkCx);
     k_identity<float><<<(e->V + 255) / 256, 256, 0, f->s>>>(f->d_G, e->V);
     LAUNCHED(2);
     return f->profile_cg(q, iters, ms, bytes);
@@ -2035,7 +2038,7 @@ static int coulomb_staged(Engine<double> *e, const gfix_params *gp,
     if (!f) return -1;
     CK(cudaStreamSynchronize(e->s));
     k_convert<double, float><<<1184, 256, 0, f->s>>>(e->d_U, f->d_U,
-                                                     (size_t)e->V * 36);
+                                                     (size_t)e->V * 4 * kLinkCx);
     LAUNCHED(1);
     Params p32 = p;
     p32.acc = gp->switch_theta;
@@ -2051,8 +2054,8 @@ static int coulomb_staged(Engine<double> *e, const gfix_params *gp,
                                                        (size_t)e->V * 9);
       LAUNCHED(1);
       CK(cudaStreamSynchronize(f->s));
-      k_reunit_links<double><<<(e->V + 255) / 256, 256, 0, e->s>>>(
-          e->d_G, (size_t)e->V, (size_t)e->V);
+      k_reunit_mats<double><<<(e->V + 255) / 256, 256, 0, e->s>>>(
+          e->d_G, (size_t)e->V);
       LAUNCHED(1);
       from_g = true;
     } else {
@@ -2174,7 +2177,7 @@ int gfix_profile_coulomb(const double *d_links, const size_t dims[4],
     if (!f) return -1;
     CK(cudaStreamSynchronize(e->s));
     k_convert<double, float><<<1184, 256, 0, f->s>>>(e->d_U, f->d_U,
-                                                     (size_t)e->V * 36);
+                                                     (size_t)e->V * 4 * kLinkCx);
     LAUNCHED(1);
     return f->profile_coul(to_params(p), iters, ms, bytes);
   }

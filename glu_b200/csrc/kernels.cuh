@@ -16,7 +16,8 @@
 // of the iteration can be replayed past convergence as a no-op.
 //
 // HBM layout (SoA, site index s = x + Lx (y + Ly (z + Lz t))):
-//   U   cx<R>[4 mu][9 elements][V]        links
+//   U   cx<R>[4 mu][6 elements][V]        links: their first two columns
+//                                          (load_link rebuilds the third)
 //   fb  cx<R>[2][4 fields][V]             in / in_old (parity selects)
 //   sb  cx<R>[2][4 fields][V]             sn ping-pong (sparity selects)
 //   G   cx<R>[9][V]                        accumulated gauge transform
@@ -172,20 +173,39 @@ __device__ __forceinline__ void strides(const Ctx<R> &c, int *st) {
   st[3] = c.L[0] * c.L[1] * c.L[2];
 }
 
+// Links in HBM keep their first two columns only: the complex entries
+// 0, 1, 3, 4, 6, 7 of the row-major matrix, stored U[mu][k][V], k = 0..5
+// (96 of a link's 144 bytes in FP64).  The third column is rebuilt on every
+// load as the conjugate cross product of the first two -- the expression
+// with which GLU's update (gtransform, src/Gfix/gtrans.c:107-121) and this
+// library's own (su3.cuh) complete every link they write -- so a link that
+// has been updated once reads back bit for bit as it was computed, and an
+// SU(3) input differs from its stored third column by rounding only.
+constexpr int kLinkCx = 6;
+
 template <typename R>
 __device__ __forceinline__ void load_link(const cx<R> *U, int V, int mu, int s,
                                           cx<R> *u) {
-  const cx<R> *p = U + (size_t)mu * 9 * V + s;
-#pragma unroll
-  for (int e = 0; e < 9; e++) u[e] = p[(size_t)e * V];
+  const cx<R> *p = U + (size_t)mu * kLinkCx * V + s;
+  u[0] = p[0];
+  u[1] = p[(size_t)V];
+  u[3] = p[2 * (size_t)V];
+  u[4] = p[3 * (size_t)V];
+  u[6] = p[4 * (size_t)V];
+  u[7] = p[5 * (size_t)V];
+  complete_col2(u);
 }
 
 template <typename R>
 __device__ __forceinline__ void store_link(cx<R> *U, int V, int mu, int s,
                                            const cx<R> *u) {
-  cx<R> *p = U + (size_t)mu * 9 * V + s;
-#pragma unroll
-  for (int e = 0; e < 9; e++) p[(size_t)e * V] = u[e];
+  cx<R> *p = U + (size_t)mu * kLinkCx * V + s;
+  p[0] = u[0];
+  p[(size_t)V] = u[1];
+  p[2 * (size_t)V] = u[3];
+  p[3 * (size_t)V] = u[4];
+  p[4 * (size_t)V] = u[6];
+  p[5 * (size_t)V] = u[7];
 }
 
 // ---------------------------------------------------------------------
@@ -206,15 +226,13 @@ __global__ void __launch_bounds__(kSiteThreads)
     double re = 0.0;
 #pragma unroll
     for (int mu = 0; mu < 4; mu++) {
-      const cx<R> *q = c.U + (size_t)mu * 9 * c.V + s;
-      const cx<R> *b = c.U + (size_t)mu * 9 * c.V + bck_site(s, mu, x, c.L, sd);
-      const size_t V = c.V;
-      const cx<R> q0 = q[0], q1 = q[V], q2 = q[2 * V], q3 = q[3 * V],
-                  q4 = q[4 * V], q5 = q[5 * V], q6 = q[6 * V], q7 = q[7 * V],
-                  q8 = q[8 * V];
-      const cx<R> b0 = b[0], b1 = b[V], b2 = b[2 * V], b3 = b[3 * V],
-                  b4 = b[4 * V], b5 = b[5 * V], b6 = b[6 * V], b7 = b[7 * V],
-                  b8 = b[8 * V];
+      cx<R> q[9], b[9];
+      load_link(c.U, c.V, mu, s, q);
+      load_link(c.U, c.V, mu, bck_site(s, mu, x, c.L, sd), b);
+      const cx<R> q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3], q4 = q[4],
+                  q5 = q[5], q6 = q[6], q7 = q[7], q8 = q[8];
+      const cx<R> b0 = b[0], b1 = b[1], b2 = b[2], b3 = b[3], b4 = b[4],
+                  b5 = b[5], b6 = b[6], b7 = b[7], b8 = b[8];
       R0 += R(2) * b0.y - b4.y - b8.y;
       R0 += R(-2) * q0.y + q4.y + q8.y;
       R1 += b1.x - b3.x - q1.x + q3.x;
@@ -515,6 +533,9 @@ __global__ void __launch_bounds__(kScalarThreads)
 // (kTrSites contiguous numbers per element row) are accessed coalesced.
 constexpr int kTrSites = 64;
 
+// matrix entry of stored element k of a link (its first two columns)
+__device__ __forceinline__ int stored_entry(int k) { return (k >> 1) * 3 + (k & 1); }
+
 template <typename R>
 __global__ void __launch_bounds__(256) k_aos_to_soa(const double *__restrict__ aos,
                                                     cx<R> *U, int V) {
@@ -524,15 +545,19 @@ __global__ void __launch_bounds__(256) k_aos_to_soa(const double *__restrict__ a
   const double2 *src = reinterpret_cast<const double2 *>(aos) + s0 * 36;
   for (int i = threadIdx.x; i < ns * 36; i += blockDim.x) t[i] = src[i];
   __syncthreads();
-  for (int i = threadIdx.x; i < 36 * kTrSites; i += blockDim.x) {
+  // row r of the SoA links: direction r / 6, stored element r % 6
+  for (int i = threadIdx.x; i < 4 * kLinkCx * kTrSites; i += blockDim.x) {
     const int r = i / kTrSites, sl = i % kTrSites;
     if (sl < ns) {
-      const double2 v = t[sl * 36 + r];
+      const double2 v = t[sl * 36 + (r / kLinkCx) * 9 + stored_entry(r % kLinkCx)];
       U[(size_t)r * V + s0 + sl] = mk<R>((R)v.x, (R)v.y);
     }
   }
 }
 
+// one thread per (site, direction) of the block's kTrSites sites: the link
+// completed in R (third column rebuilt as in load_link), then staged in
+// shared memory for coalesced AoS stores
 template <typename R>
 __global__ void __launch_bounds__(256) k_soa_to_aos(const cx<R> *U,
                                                     double *__restrict__ aos,
@@ -540,11 +565,14 @@ __global__ void __launch_bounds__(256) k_soa_to_aos(const cx<R> *U,
   __shared__ double2 t[kTrSites * 36 + 1];
   const size_t s0 = (size_t)blockIdx.x * kTrSites;
   const int ns = (int)min((size_t)kTrSites, (size_t)V - s0);
-  for (int i = threadIdx.x; i < 36 * kTrSites; i += blockDim.x) {
-    const int r = i / kTrSites, sl = i % kTrSites;
+  for (int i = threadIdx.x; i < 4 * kTrSites; i += blockDim.x) {
+    const int mu = i / kTrSites, sl = i % kTrSites;
     if (sl < ns) {
-      const cx<R> v = U[(size_t)r * V + s0 + sl];
-      t[sl * 36 + r] = make_double2((double)v.x, (double)v.y);
+      cx<R> u[9];
+      load_link(U, V, mu, (int)(s0 + sl), u);
+#pragma unroll
+      for (int e = 0; e < 9; e++)
+        t[sl * 36 + mu * 9 + e] = make_double2((double)u[e].x, (double)u[e].y);
     }
   }
   __syncthreads();

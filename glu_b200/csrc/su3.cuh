@@ -106,6 +106,16 @@ __device__ __forceinline__ void set_gauge(cx<R> *g, cx<R> f0, cx<R> f1,
   gram_reunit(g);
 }
 
+// the third column of a matrix whose first two columns are set: the
+// conjugate cross product of the first two, the completion of gtransform
+// (src/Gfix/gtrans.c:107-121) and of gram_reunit
+template <typename R>
+__device__ __forceinline__ void complete_col2(cx<R> *u) {
+  u[2] = conjg(csub(cmul(u[3], u[7]), cmul(u[4], u[6])));
+  u[5] = conjg(csub(cmul(u[1], u[6]), cmul(u[0], u[7])));
+  u[8] = conjg(csub(cmul(u[0], u[4]), cmul(u[1], u[3])));
+}
+
 // b <- a b c^dag
 template <typename R>
 __device__ __forceinline__ void gtransform(const cx<R> *a, cx<R> *b,
@@ -130,9 +140,7 @@ __device__ __forceinline__ void gtransform(const cx<R> *a, cx<R> *b,
                           cmul(a[r * 3 + 2], bc[2 * 2 + k]));
     }
   }
-  b[2] = conjg(csub(cmul(b[3], b[7]), cmul(b[4], b[6])));
-  b[5] = conjg(csub(cmul(b[1], b[6]), cmul(b[0], b[7])));
-  b[8] = conjg(csub(cmul(b[0], b[4]), cmul(b[1], b[3])));
+  complete_col2(b);
 }
 
 // Re tr(a b c^dag), row 2 of (a b) completed by the cross product
