@@ -61,7 +61,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "polish"],
+                    help="mixed (default) or fp64; polish only with --profile-only: "
+                         "the kernels of a mixed solve's FP64-link phase")
     ap.add_argument("--workload", default="landau",
                     choices=["landau", "coulomb", "ensemble", "gluonprop", "heatbath"],
                     help="landau: 32^3x64 Landau FACG (the headline); coulomb: "
@@ -87,7 +89,10 @@ def parse():
     ap.add_argument("--profile-only", action="store_true",
                     help="only the per-kernel event timing of --profile-iters "
                          "CG iterations (a short, bounded launch list for ncu)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.precision == "polish" and not args.profile_only:
+        ap.error("--precision polish profiles kernels: it needs --profile-only")
+    return args
 
 
 class Clocks:
@@ -337,15 +342,19 @@ def gpu_arm(args, dims, rank, world, local):
     clocks = clk.summary()
     res = dict(out=out, clocks=clocks, V=V)
     # per-kernel device times for the roofline (events on the launch stream)
+    # fp64: the FP64 solve; fp32 and polish: the two phases of a mixed one
+    # (FP32 throughout; FP64 links with FP32 fields)
     prof = {}
-    for prec in ("fp64", "mixed"):
+    for tag, code in (("fp64", 0), ("fp32", 1), ("polish", 2)):
         ms = np.zeros(7)
         by = np.zeros(7)
+        p = _params("fp64")
+        p.precision = code
         check(lib.gfix_profile_landau(
-            dpristine[0].data_ptr(), cd, C.byref(_params(prec)), args.profile_iters,
+            dpristine[0].data_ptr(), cd, C.byref(p), args.profile_iters,
             ms.ctypes.data_as(C.POINTER(C.c_double)),
             by.ctypes.data_as(C.POINTER(C.c_double))))
-        prof["fp32" if prec == "mixed" else "fp64"] = (ms, by)
+        prof[tag] = (ms, by)
     res["prof"] = prof
     if dist is not None:
         dist.destroy_process_group()
@@ -524,7 +533,7 @@ def gpu_line(args, dims, world, res, cpu):
     it32 = sum(x[1] for x in o["per"]) if prec == "mixed" else 0
     it64 = sum(x[0] for x in o["per"]) - it32
     share = []
-    for tag, n in (("fp32", it32), ("fp64", it64)):
+    for tag, n in (("fp32", it32), ("polish" if prec == "mixed" else "fp64", it64)):
         ms, by = res["prof"][tag]
         for k in range(6):
             share.append((ms[k] * n, tag, k, ms[k], by[k]))
@@ -534,7 +543,7 @@ def gpu_line(args, dims, world, res, cpu):
     achieved = k_by / (k_ms * 1e-3) / 1e9
     traffic = traffic_from_profiles(KERNELS[k], tag, dims)
     per_kernel = {f"{KERNELS[j]}:{t}": {"ms": round(m, 5), "GB/s": round(b / (m * 1e-3) / 1e9, 1)}
-                  for t in ("fp32", "fp64") if (t != "fp32" or prec == "mixed")
+                  for t in ("fp32", "polish", "fp64") if (t == "fp64" or prec == "mixed")
                   for j, (m, b) in enumerate(zip(*res["prof"][t])) if j < 6}
     line = {
         "metric": metric_name(dims), "value": value, "unit": UNIT, "n_gpus": world,
@@ -589,11 +598,14 @@ def profile_only(args, dims):
     cd = (C.c_size_t * 4)(*dims)
     ms = np.zeros(7)
     by = np.zeros(7)
-    check(lib.gfix_profile_landau(d.data_ptr(), cd, C.byref(_params(args.precision)),
+    pp = _params(args.precision)
+    if args.precision == "polish":
+        pp.precision = 2
+    check(lib.gfix_profile_landau(d.data_ptr(), cd, C.byref(pp),
                                   args.profile_iters,
                                   ms.ctypes.data_as(C.POINTER(C.c_double)),
                                   by.ctypes.data_as(C.POINTER(C.c_double))))
-    tag = "fp32" if args.precision == "mixed" else "fp64"
+    tag = {"mixed": "fp32", "fp64": "fp64", "polish": "polish"}[args.precision]
     emit({"profile": tag, "dims": list(dims), "iters": args.profile_iters,
           "kernels": {f"{KERNELS[k]}:{tag}": {"ms": ms[k], "bytes": by[k],
                                               "GB/s": by[k] / (ms[k] * 1e-3) / 1e9 if ms[k] else None}

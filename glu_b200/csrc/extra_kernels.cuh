@@ -9,8 +9,8 @@ namespace gfix {
 
 // average plaquette partials: Re tr(U_mu(x) U_nu(x+mu) U_mu(x+nu)^dag
 // U_nu(x)^dag) summed over mu > nu (src/Field/plaqs_links.c:243-265)
-template <typename R>
-__global__ void __launch_bounds__(kSiteThreads) k_plaquette(Ctx<R> c) {
+template <typename R, typename F = R>
+__global__ void __launch_bounds__(kSiteThreads) k_plaquette(Ctx<R, F> c) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   double v[1] = {0.0};
   if (s < c.V) {
@@ -83,8 +83,8 @@ __global__ void k_reunit_mats(cx<R> *G, size_t n) {
 constexpr int kDiagThreads = 128;
 constexpr int kDiagVals = 19;
 
-template <typename R>
-__global__ void __launch_bounds__(kDiagThreads) k_link_diag(Ctx<R> c, int lcu,
+template <typename R, typename F = R>
+__global__ void __launch_bounds__(kDiagThreads) k_link_diag(Ctx<R, F> c, int lcu,
                                                              int nbs) {
   const int t = blockIdx.y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -164,10 +164,12 @@ __global__ void k_convert(const cx<RS> *a, cx<RD> *b, size_t n) {
     b[i] = mk<RD>((RD)a[i].x, (RD)a[i].y);
 }
 
-// U_mu(x) <- G(x) U_mu(x) G(x+mu)^dag with G reunitarised first (FP64);
-// used when the FP32 phase hands its accumulated transform to FP64
+// U_mu(x) <- G(x) U_mu(x) G(x+mu)^dag with G widened to FP64 and
+// reunitarised first; used when the FP32 phase hands its accumulated
+// transform (G in RG, FP32) to the FP64 links
+template <typename F, typename RG>
 __global__ void __launch_bounds__(kSiteThreads)
-    k_apply_gauge(Ctx<double> c, const cx<double> *G) {
+    k_apply_gauge(Ctx<double, F> c, const cx<RG> *G) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= c.V) return;
   int x[4], sd[4];
@@ -176,12 +178,14 @@ __global__ void __launch_bounds__(kSiteThreads)
   const size_t V = c.V;
   cx<double> A[9], B[9], U[9];
 #pragma unroll
-  for (int e = 0; e < 9; e++) A[e] = G[(size_t)e * V + s];
+  for (int e = 0; e < 9; e++)
+    A[e] = mk<double>((double)G[(size_t)e * V + s].x, (double)G[(size_t)e * V + s].y);
   gram_reunit(A);
   for (int mu = 0; mu < 4; mu++) {
     const int y = fwd_site(s, mu, x, c.L, sd);
 #pragma unroll
-    for (int e = 0; e < 9; e++) B[e] = G[(size_t)e * V + y];
+    for (int e = 0; e < 9; e++)
+      B[e] = mk<double>((double)G[(size_t)e * V + y].x, (double)G[(size_t)e * V + y].y);
     gram_reunit(B);
     load_link(c.U, c.V, mu, s, U);
     gtransform(A, U, B);
@@ -189,20 +193,17 @@ __global__ void __launch_bounds__(kSiteThreads)
   }
 }
 
-// Random SU(3) gauge matrices G[9][V] for a random restart of a Landau fix
-// (GLU's random_transform, src/Geometry/random_config.c:107-120, which
-// draws them from its own per-thread generator): per site nine complex
-// Gaussian entries (Box-Muller on a SplitMix64 stream keyed by the seed,
-// the attempt and the site), then the column Gram-Schmidt of gram_reunit
+// The random SU(3) gauge matrix of site s for a random restart of a Landau
+// fix (GLU's random_transform, src/Geometry/random_config.c:107-120, which
+// draws them from its own per-thread generator): nine complex Gaussian
+// entries (Box-Muller on a SplitMix64 stream keyed by the seed, the
+// attempt and the site), then the column Gram-Schmidt of gram_reunit
 // (columns 0 and 1 orthonormal, column 2 their conjugate cross product).
 // Reproducible for a given (seed, attempt); not GLU's stream.
-__global__ void k_random_gauge(cx<double> *G, int V, unsigned long long seed,
-                               int attempt) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= V) return;
+__device__ __forceinline__ void random_su3(cx<double> *g, unsigned long long seed,
+                                           int attempt, int s) {
   unsigned long long h =
       mix64(seed ^ mix64(((unsigned long long)attempt << 40) ^ (unsigned long long)s));
-  cx<double> g[9];
 #pragma unroll
   for (int e = 0; e < 9; e++) {
     h = mix64(h);
@@ -213,8 +214,27 @@ __global__ void k_random_gauge(cx<double> *G, int V, unsigned long long seed,
     g[e] = mk<double>(rad * cospi(2.0 * u2), rad * sinpi(2.0 * u2));
   }
   gram_reunit(g);
-#pragma unroll
-  for (int e = 0; e < 9; e++) G[(size_t)e * V + s] = g[e];
+}
+
+// U_mu(x) <- g(x) U_mu(x) g(x + mu)^dag with the random matrices of
+// random_su3 (each site's drawn again by its -mu neighbours: no buffer)
+template <typename F>
+__global__ void __launch_bounds__(kSiteThreads)
+    k_random_transform(Ctx<double, F> c, unsigned long long seed, int attempt) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= c.V) return;
+  int x[4], sd[4];
+  coords(s, c.L, x);
+  strides(c, sd);
+  cx<double> A[9], B[9], U[9];
+  random_su3(A, seed, attempt, s);
+#pragma unroll 1
+  for (int mu = 0; mu < 4; mu++) {
+    random_su3(B, seed, attempt, fwd_site(s, mu, x, c.L, sd));
+    load_link(c.U, c.V, mu, s, U);
+    gtransform(A, U, B);
+    store_link(c.U, c.V, mu, s, U);
+  }
 }
 
 // GLU's gauge-fixing accuracy report (gf_check, src/Wrappers/OBS_wrap.c:
@@ -263,7 +283,8 @@ __device__ __forceinline__ void gfc_log(const cx<double> *u, double *a) {
   a[7] = q[3].y;
 }
 
-__global__ void __launch_bounds__(kSiteThreads) k_gf_check(Ctx<double> c) {
+template <typename F>
+__global__ void __launch_bounds__(kSiteThreads) k_gf_check(Ctx<double, F> c) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   // {lin 4D, log 4D, lin 3D, log 3D}
   double v[4] = {0.0, 0.0, 0.0, 0.0};

@@ -20,6 +20,7 @@
 #include <memory>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/glu_gfix.h"
@@ -141,16 +142,19 @@ static void stall_rule(Params &p) {
   }
 }
 
-template <typename R>
+// R: links and their arithmetic; F: the su(3) fields and the FFT (F = R,
+// or float under FP64 links in the FP64 phase of a mixed-precision solve)
+template <typename R, typename F = R>
 class Engine {
  public:
   size_t dims[4] = {0, 0, 0, 0};
   int V = 0;
-  Ctx<R> c{};
+  Ctx<R, F> c{};
   cudaStream_t s = nullptr;
   DevState *d_st = nullptr, *h_st = nullptr;
   double *d_part = nullptr, *d_cs = nullptr, *d_traj = nullptr;
-  cx<R> *d_tw = nullptr, *d_U = nullptr, *d_F = nullptr, *d_G = nullptr;
+  cx<F> *d_tw = nullptr, *d_F = nullptr;
+  cx<R> *d_U = nullptr, *d_G = nullptr;
   double *d_aos = nullptr;  // AoS FP64 staging (only FP64 engines)
   size_t traj_alloc = 0;
   int nb_site = 0;
@@ -160,8 +164,8 @@ class Engine {
   bool odd = false;
   bool coul = false;
   int Lcu = 0;
-  XyFn<R> xy_ct = nullptr;
-  ZtFn<R> zt_ct = nullptr;
+  XyFn<F> xy_ct = nullptr;
+  ZtFn<F> zt_ct = nullptr;
   cudaGraphExec_t gx_cg = nullptr, gx_sd = nullptr;
   cudaGraph_t gr_cg = nullptr, gr_sd = nullptr;  // the same, uninstantiated
   int gx_sd_fixed = -1;
@@ -229,17 +233,17 @@ class Engine {
     // (GLU_definitions.h:414, 420)
     c.maxp = coul ? 4.0 * 3 / (double)Lcu : 4.0 * 4 / (double)V;
     // twiddle pool: one table per axis
-    std::vector<cx<R>> tw;
+    std::vector<cx<F>> tw;
     for (int a = 0; a < 4; a++) {
       c.ax[a].tw_off = (int)tw.size();
       const int n = c.L[a];
       for (int k = 0; k < n; k++) {
         const double ang = 6.283185307179586476925286766559 * k / n;
-        tw.push_back(mk<R>((R)std::cos(ang), (R)(-std::sin(ang))));
+        tw.push_back(mk<F>((F)std::cos(ang), (F)(-std::sin(ang))));
       }
     }
-    CK(cudaMalloc(&d_tw, tw.size() * sizeof(cx<R>)));
-    CK(cudaMemcpy(d_tw, tw.data(), tw.size() * sizeof(cx<R>),
+    CK(cudaMalloc(&d_tw, tw.size() * sizeof(cx<F>)));
+    CK(cudaMemcpy(d_tw, tw.data(), tw.size() * sizeof(cx<F>),
                   cudaMemcpyHostToDevice));
     c.tw = d_tw;
     // cos tables as GLU evaluates them: cos(n * (TWOPI / L)) (init.c:66,
@@ -267,7 +271,7 @@ class Engine {
         odd |= (c.ax[a].st[k].r == 5 || c.ax[a].st[k].r == 7);
     const int nt = coul ? 1 : c.L[3];
     int want_b = coul ? 16 : 2;
-    if (!coul && !odd && c.L[0] % 4 == 0 && ct_zt<R>(c.L[2], nt, 4) != nullptr &&
+    if (!coul && !odd && c.L[0] % 4 == 0 && ct_zt<F>(c.L[2], nt, 4) != nullptr &&
         zt_smem(4) <= 200u * 1024u)
       want_b = 4;
     c.zt_b = 1;
@@ -279,7 +283,7 @@ class Engine {
     // a compile-time pass takes the tile as chosen while its shared memory
     // fits (tiles up to 16384 elements); the generic passes hold one
     // element per thread and stage for 8 (16) elements: tiles up to 8192
-    const bool ct_tile = !odd && ct_zt<R>(c.L[2], nt, c.zt_b) != nullptr &&
+    const bool ct_tile = !odd && ct_zt<F>(c.L[2], nt, c.zt_b) != nullptr &&
                          zt_smem(c.zt_b) <= 200u * 1024u;
     if (!ct_tile) {
       while (c.zt_b > 1 && (size_t)c.zt_b * c.L[2] * nt > 4096u) c.zt_b /= 2;
@@ -288,7 +292,7 @@ class Engine {
     if ((size_t)c.L[0] * c.L[1] > 8192)
       return fail("FFT xy tile of %d elements exceeds 8192", c.L[0] * c.L[1]);
     // tile (padded) plus the twiddle tables of its two axes
-    sm_xy = ((size_t)c.xy_pitch * c.L[1] + c.L[0] + c.L[1]) * sizeof(cx<R>);
+    sm_xy = ((size_t)c.xy_pitch * c.L[1] + c.L[0] + c.L[1]) * sizeof(cx<F>);
     // the dynamic shared-memory limit is an attribute of the function, not
     // of a launch: raise it once to the largest tile any engine can use
     if (set_smem_limits()) return -1;
@@ -310,7 +314,7 @@ class Engine {
     memset(h_st, 0, sizeof(DevState));
     c.st = d_st;
     CK(cudaMalloc(&d_U, (size_t)V * 4 * kLinkCx * sizeof(cx<R>)));
-    CK(cudaMalloc(&d_F, (size_t)V * 16 * sizeof(cx<R>)));
+    CK(cudaMalloc(&d_F, (size_t)V * 16 * sizeof(cx<F>)));
     c.U = d_U;
     c.fb[0] = d_F;
     c.fb[1] = d_F + (size_t)4 * V;
@@ -325,9 +329,9 @@ class Engine {
 
   // --- FFT plans ------------------------------------------------------
   size_t zt_smem(int b) const {
-    return coul ? ((size_t)b * c.L[2] + c.L[2]) * sizeof(cx<R>)
+    return coul ? ((size_t)b * c.L[2] + c.L[2]) * sizeof(cx<F>)
                 : ((size_t)(b * c.L[2] + std::max(1, zt_pad(b))) * c.L[3] +
-                   c.L[2] + c.L[3]) * sizeof(cx<R>);
+                   c.L[2] + c.L[3]) * sizeof(cx<F>);
   }
   static size_t threads_for(size_t n, int pt) {
     size_t t = (n + pt - 1) / pt;
@@ -340,7 +344,7 @@ class Engine {
       if (factorize(c.L[a], c.ax[a], order)) return -1;
     const size_t n = (size_t)c.L[0] * c.L[1];
     if (use_ct) {
-      XyFn<R> fn = odd ? nullptr : ct_xy<R>(c.L[0], c.L[1]);
+      XyFn<F> fn = odd ? nullptr : ct_xy<F>(c.L[0], c.L[1]);
       if (!fn) return -1;
       xy_ct = fn;
       bd_xy = ct_threads((int)n);
@@ -364,7 +368,7 @@ class Engine {
       if (factorize(c.L[a], c.ax[a], order)) return -1;
     const size_t n = (size_t)b * c.L[2] * nt;
     if (use_ct) {
-      ZtFn<R> fn = odd ? nullptr : ct_zt<R>(c.L[2], nt, b);
+      ZtFn<F> fn = odd ? nullptr : ct_zt<F>(c.L[2], nt, b);
       if (!fn || zt_smem(b) > 200u * 1024u) return -1;
       zt_ct = fn;
       bd_zt = ct_threads((int)n);
@@ -423,7 +427,7 @@ class Engine {
     if (it == tuned().end()) {
       Params p;
       if (reset(p)) return -1;
-      CK(cudaMemsetAsync(d_F, 0, (size_t)V * 16 * sizeof(cx<R>), s));
+      CK(cudaMemsetAsync(d_F, 0, (size_t)V * 16 * sizeof(cx<F>), s));
       float best = 1e30f, t = 0.f;
       P = TunedPlan{xy_ct != nullptr, xy_plan < 0 ? 0 : xy_plan, c.zt_b,
                     zt_ct != nullptr, zt_plan < 0 ? 0 : zt_plan, 0.f, 0.f};
@@ -477,18 +481,18 @@ class Engine {
     LAUNCHED(1);
   }
   void theta(int op) {
-    k_deriv<R><<<nb_site, kSiteThreads, 0, s>>>(c);
+    k_deriv<R, F><<<nb_site, kSiteThreads, 0, s>>>(c);
     LAUNCHED(1);
     scalar(op, 2);
   }
   static int set_smem_limits() {
     static bool done = false;
     if (done) return 0;
-    const int lim = (8192 + 8192 / 8 + 1024) * (int)sizeof(cx<R>);
+    const int lim = (8192 + 8192 / 8 + 1024) * (int)sizeof(cx<F>);
     const void *fns[] = {
-        (const void *)k_fft_xy<R, 8, false>, (const void *)k_fft_xy<R, 16, false>,
-        (const void *)k_fft_xy<R, 16, true>, (const void *)k_fft_zt<R, 8, false>,
-        (const void *)k_fft_zt<R, 16, false>, (const void *)k_fft_zt<R, 16, true>};
+        (const void *)k_fft_xy<F, 8, false>, (const void *)k_fft_xy<F, 16, false>,
+        (const void *)k_fft_xy<F, 16, true>, (const void *)k_fft_zt<F, 8, false>,
+        (const void *)k_fft_zt<F, 16, false>, (const void *)k_fft_zt<F, 16, true>};
     for (const void *f : fns) {
       CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
       CK(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -497,26 +501,59 @@ class Engine {
     done = true;
     return 0;
   }
+  // the context the FFT passes and field-only kernels see: the fields'
+  // type throughout (they touch neither links nor G)
+  Ctx<F> cf() const {
+    if constexpr (std::is_same<R, F>::value) {
+      return c;
+    } else {
+      Ctx<F> v;
+      v.U = nullptr;
+      v.G = nullptr;
+      v.fb[0] = c.fb[0];
+      v.fb[1] = c.fb[1];
+      v.sb[0] = c.sb[0];
+      v.sb[1] = c.sb[1];
+      v.st = c.st;
+      v.part = c.part;
+      v.tw = c.tw;
+      v.cs = c.cs;
+      v.cs_ld = c.cs_ld;
+      for (int i = 0; i < 4; i++) {
+        v.L[i] = c.L[i];
+        v.ax[i] = c.ax[i];
+      }
+      v.V = c.V;
+      v.ndim = c.ndim;
+      v.zt_b = c.zt_b;
+      v.xy_pitch = c.xy_pitch;
+      v.maxp = c.maxp;
+      v.skip = c.skip;
+      return v;
+    }
+  }
   void fft_xy(int bwd, int prsum) {
+    const Ctx<F> v = cf();
     if (xy_ct)
-      xy_ct<<<g_xy, bd_xy, sm_xy, s>>>(c, bwd, prsum);
+      xy_ct<<<g_xy, bd_xy, sm_xy, s>>>(v, bwd, prsum);
     else if (odd)
-      k_fft_xy<R, 16, true><<<g_xy, bd_xy, sm_xy, s>>>(c, bwd, prsum);
+      k_fft_xy<F, 16, true><<<g_xy, bd_xy, sm_xy, s>>>(v, bwd, prsum);
     else if (pt_xy == 8)
-      k_fft_xy<R, 8, false><<<g_xy, bd_xy, sm_xy, s>>>(c, bwd, prsum);
+      k_fft_xy<F, 8, false><<<g_xy, bd_xy, sm_xy, s>>>(v, bwd, prsum);
     else
-      k_fft_xy<R, 16, false><<<g_xy, bd_xy, sm_xy, s>>>(c, bwd, prsum);
+      k_fft_xy<F, 16, false><<<g_xy, bd_xy, sm_xy, s>>>(v, bwd, prsum);
     LAUNCHED(1);
   }
   void fft_zt() {
+    const Ctx<F> v = cf();
     if (zt_ct)
-      zt_ct<<<g_zt, bd_zt, sm_zt, s>>>(c);
+      zt_ct<<<g_zt, bd_zt, sm_zt, s>>>(v);
     else if (odd)
-      k_fft_zt<R, 16, true><<<g_zt, bd_zt, sm_zt, s>>>(c);
+      k_fft_zt<F, 16, true><<<g_zt, bd_zt, sm_zt, s>>>(v);
     else if (pt_zt == 8)
-      k_fft_zt<R, 8, false><<<g_zt, bd_zt, sm_zt, s>>>(c);
+      k_fft_zt<F, 8, false><<<g_zt, bd_zt, sm_zt, s>>>(v);
     else
-      k_fft_zt<R, 16, false><<<g_zt, bd_zt, sm_zt, s>>>(c);
+      k_fft_zt<F, 16, false><<<g_zt, bd_zt, sm_zt, s>>>(v);
     LAUNCHED(1);
   }
   // direction + probes: FP64 storage one kernel; FP32 storage the FP32- and
@@ -524,10 +561,10 @@ class Engine {
   template <bool DIR>
   void probe() {
     if (sizeof(R) == 8) {
-      k_dir_probe<R, DIR, double><<<nb_site, kSiteThreads, 0, s>>>(c, SEL_ALWAYS);
+      k_dir_probe<R, DIR, double, F><<<nb_site, kSiteThreads, 0, s>>>(c, SEL_ALWAYS);
     } else {
-      k_dir_probe<R, DIR, R><<<nb_site, kSiteThreads, 0, s>>>(c, SEL_LOW);
-      k_dir_probe<R, DIR, double><<<nb_site, kSiteThreads, 0, s>>>(c, SEL_HIGH);
+      k_dir_probe<R, DIR, R, F><<<nb_site, kSiteThreads, 0, s>>>(c, SEL_LOW);
+      k_dir_probe<R, DIR, double, F><<<nb_site, kSiteThreads, 0, s>>>(c, SEL_HIGH);
       LAUNCHED(1);
     }
   }
@@ -548,7 +585,7 @@ class Engine {
       LAUNCHED(1);
       scalar(OP_PROBES, 2);
     }
-    k_update<R, false><<<nb_site, kSiteThreads, 0, s>>>(c);
+    k_update<R, false, F><<<nb_site, kSiteThreads, 0, s>>>(c);
     LAUNCHED(1);
     if (main) scalar(OP_END_SD, 0);
   }
@@ -560,7 +597,7 @@ class Engine {
     probe<true>();
     LAUNCHED(1);
     scalar(OP_PROBES, 2);
-    k_update<R, true><<<nb_site, kSiteThreads, 0, s>>>(c);
+    k_update<R, true, F><<<nb_site, kSiteThreads, 0, s>>>(c);
     LAUNCHED(1);
     scalar(OP_END_CG, 0);
   }
@@ -574,7 +611,7 @@ class Engine {
     cg_iter();
     sd_step(true, false);
     sd_step(true, true);
-    k_copy_der<R><<<nb_site, kSiteThreads, 0, s>>>(c);
+    k_copy_der<F><<<nb_site, kSiteThreads, 0, s>>>(cf());
     k_set_done<<<1, 1, 0, s>>>(d_st, 0);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
@@ -737,7 +774,7 @@ class Engine {
     LAUNCHED(1);
     if (run_cg) {
       sd_step(false, run_p.sd_fixed != 0);
-      k_copy_der<R><<<nb_site, kSiteThreads, 0, s>>>(c);
+      k_copy_der<F><<<nb_site, kSiteThreads, 0, s>>>(cf());
       LAUNCHED(1);
       scalar(OP_DER, 1);
     }
@@ -823,7 +860,7 @@ class Engine {
     if (reset(p)) return -1;
     k_begin_run<<<1, 1, 0, s>>>(d_st);
     sd_step(false, p.sd_fixed != 0);
-    k_copy_der<R><<<nb_site, kSiteThreads, 0, s>>>(c);
+    k_copy_der<F><<<nb_site, kSiteThreads, 0, s>>>(cf());
     scalar(OP_DER, 1);
     LAUNCHED(2);
     std::vector<cudaEvent_t> ev(8);
@@ -831,7 +868,7 @@ class Engine {
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
     for (int it = 0; it < n; it++) {
       CK(cudaEventRecord(ev[0], s));
-      k_deriv<R><<<nb_site, kSiteThreads, 0, s>>>(c);
+      k_deriv<R, F><<<nb_site, kSiteThreads, 0, s>>>(c);
       CK(cudaEventRecord(ev[1], s));
       scalar(OP_THETA_MAIN, 2);
       CK(cudaEventRecord(ev[2], s));
@@ -857,7 +894,7 @@ class Engine {
       CK(cudaEventRecord(ev[0], s));
       scalar(OP_PROBES, 2);
       CK(cudaEventRecord(ev[1], s));
-      k_update<R, true><<<nb_site, kSiteThreads, 0, s>>>(c);
+      k_update<R, true, F><<<nb_site, kSiteThreads, 0, s>>>(c);
       CK(cudaEventRecord(ev[2], s));
       scalar(OP_END_CG, 0);
       CK(cudaEventRecord(ev[3], s));
@@ -868,14 +905,15 @@ class Engine {
       LAUNCHED(10);
     }
     for (auto &e : ev) cudaEventDestroy(e);
-    const double B = sizeof(cx<R>) * (double)V;  // one complex per site
+    // one complex number per site: of the links' type and of the fields'
+    const double B = sizeof(cx<R>) * (double)V, BF = sizeof(cx<F>) * (double)V;
     // update: links in and out, the direction; with G (the FP32 phase of
     // mixed precision) also the accumulated transform in and out
     // (links: 4 kLinkCx complex numbers per site, their first two columns)
     const double L4 = 4.0 * kLinkCx;
-    const double b[7] = {(L4 + 4) * B, 8 * B, 8 * B, 12 * B,
-                         (L4 + 4 + 4 + 4) * B,
-                         (L4 + 4 + L4 + (c.G ? 18 : 0)) * B, 0.0};
+    const double b[7] = {L4 * B + 4 * BF, 8 * BF, 8 * BF, 12 * BF,
+                         L4 * B + 12 * BF,
+                         (2 * L4 + (c.G ? 18 : 0)) * B + 4 * BF, 0.0};
     for (int k = 0; k < 7; k++) {
       ms[k] = acc[k] / n;
       if (bytes) bytes[k] = b[k];
@@ -1231,6 +1269,26 @@ static Engine<double> *engine64(const size_t *d) {
   return p;
 }
 
+// the FP64-link engine of mixed-precision solves: FP64 links, theta and
+// updates, FP32 fields and FFT
+static std::map<Key, std::unique_ptr<Engine<double, float>>> g_e64m;
+
+static Engine<double, float> *engine64m(const size_t *d) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    fail("no CUDA device");
+    return nullptr;
+  }
+  Key k{dev, {d[0], d[1], d[2], d[3]}, 6432};
+  auto it = g_e64m.find(k);
+  if (it != g_e64m.end()) return it->second.get();
+  auto e = std::make_unique<Engine<double, float>>();
+  if (e->init(d, false, true)) return nullptr;
+  Engine<double, float> *p = e.get();
+  g_e64m[k] = std::move(e);
+  return p;
+}
+
 static Engine<float> *engine32(const size_t *d) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
@@ -1309,29 +1367,27 @@ static Params to_params(const gfix_params *p) {
 // d_aos); for a restart (attempt > 0) randomly gauge transformed, as GLU's
 // Landau driver re-reads its input and applies random_transform
 // (src/Gfix/Landau.c:241-257, src/Geometry/random_config.c:107-120).
-static int stage_input(Engine<double> *e, unsigned long long seed, int attempt) {
+template <typename E>
+static int stage_input(E *e, unsigned long long seed, int attempt) {
   if (e->from_aos(e->d_aos)) return -1;
   if (attempt > 0) {
-    cx<double> *G = e->c.fb[0];  // 9 V complex fit in the field pool
-    k_random_gauge<<<(e->V + 255) / 256, 256, 0, e->s>>>(G, e->V, seed, attempt);
-    k_apply_gauge<<<e->nb_site, kSiteThreads, 0, e->s>>>(e->c, G);
-    LAUNCHED(2);
+    k_random_transform<<<e->nb_site, kSiteThreads, 0, e->s>>>(e->c, seed, attempt);
+    LAUNCHED(1);
     CK(cudaGetLastError());
   }
   return 0;
 }
 
-static int mixed_handover(Engine<double> *e, Engine<float> *f, const Params &p64,
+// E: the FP64-link engine of the second phase (FP64 or FP32 fields)
+template <typename E>
+static int mixed_handover(E *e, Engine<float> *f, const Params &p64,
                           size_t *it32, double th32, int *restart,
                           unsigned long long seed, int attempt) {
   *restart = 0;
   if (!(*it32 == kSentinel || *it32 > 0)) return 0;
-  cx<double> *G64 = e->c.fb[0];  // 9 V complex fit in the field pool
-  k_convert<float, double><<<1184, 256, 0, f->s>>>(f->d_G, G64,
-                                                   (size_t)e->V * 9);
-  LAUNCHED(1);
+  // the FP32 phase's G, widened and reunitarised in FP64, on the FP64 links
   CK(cudaStreamSynchronize(f->s));
-  k_apply_gauge<<<e->nb_site, kSiteThreads, 0, e->s>>>(e->c, G64);
+  k_apply_gauge<<<e->nb_site, kSiteThreads, 0, e->s>>>(e->c, (const cx<float> *)f->d_G);
   LAUNCHED(1);
   double tt = 0.0;
   if (e->reset(p64) || e->theta_test(&tt)) return -1;
@@ -1347,10 +1403,8 @@ static int mixed_handover(Engine<double> *e, Engine<float> *f, const Params &p64
     if (f->read_state()) return -1;
     const cx<float> *in_old = f->c.fb[f->h_st->parity ^ 1];
     const cx<float> *sn_old = f->c.sb[f->h_st->sparity];
-    k_convert<float, double><<<1184, 256, 0, e->s>>>(in_old, e->c.fb[1],
-                                                     (size_t)e->V * 4);
-    k_convert<float, double><<<1184, 256, 0, e->s>>>(sn_old, e->c.sb[0],
-                                                     (size_t)e->V * 4);
+    k_convert<<<1184, 256, 0, e->s>>>(in_old, e->c.fb[1], (size_t)e->V * 4);
+    k_convert<<<1184, 256, 0, e->s>>>(sn_old, e->c.sb[0], (size_t)e->V * 4);
     LAUNCHED(2);
     CK(cudaStreamSynchronize(e->s));
     e->warm = true;
@@ -1362,8 +1416,9 @@ static int mixed_handover(Engine<double> *e, Engine<float> *f, const Params &p64
 // One Landau solve (GLU's FACG / FASD, or the mixed-precision pair of
 // them) from the staged input; the fixed links are left in e64's SoA
 // links.  attempt > 0: a random restart (stage_input).
-static int landau_attempt(Engine<double> *e64, const gfix_params *gp,
-                          int attempt, gfix_result *r) {
+template <typename E>
+static int landau_attempt(E *e64, const gfix_params *gp, int attempt,
+                          gfix_result *r) {
   Params p = to_params(gp);
   gfix_result res;
   memset(&res, 0, sizeof res);
@@ -1435,8 +1490,8 @@ void set_restart_log(bool on) { t_restart_log = on; }
 // the first attempt's sentinel, + max_iters per failed restart, + the
 // successful attempt's count; GLU_FAILURE when every attempt failed.  The
 // fixed links are left in e64's SoA links (resident) and in d_aos.
-static int landau_staged(Engine<double> *e64, const gfix_params *gp,
-                         gfix_result *r) {
+template <typename E>
+static int landau_staged(E *e64, const gfix_params *gp, gfix_result *r) {
   CK(cudaEventRecord(e64->ev0, e64->s));
   gfix_result res;
   if (landau_attempt(e64, gp, 0, &res)) return -1;
@@ -1485,8 +1540,8 @@ static int landau_staged(Engine<double> *e64, const gfix_params *gp,
 // finished.  Each configuration runs exactly the kernel sequence of a solve
 // of its own, so its results are those of gfix_landau.
 
-template <typename R>
-static int batch_solve(std::vector<Engine<R> *> &es, const Params &p,
+template <typename E>
+static int batch_solve(std::vector<E *> &es, const Params &p,
                        std::vector<size_t> &iters, std::vector<double> &th,
                        cudaStream_t bs) {
   const size_t n = es.size();
@@ -1583,9 +1638,12 @@ struct BatchInst {
   size_t dims[4];
   double *links = nullptr;  // host or device, double[V][4][9][2]
   bool device = false;
-  std::unique_ptr<Engine<double>> e64;
-  std::unique_ptr<Engine<float>> e32;
+  std::unique_ptr<Engine<double>> e64;           // GFIX_FP64
+  std::unique_ptr<Engine<double, float>> e64m;   // GFIX_MIXED: FP64 links
+  std::unique_ptr<Engine<float>> e32;            //   and the FP32 phase
   gfix_result res;
+  Engine<double> *fp64(Engine<double> *) { return e64.get(); }
+  Engine<double, float> *fp64(Engine<double, float> *) { return e64m.get(); }
 };
 
 struct Batch {
@@ -1600,7 +1658,9 @@ struct Batch {
 
 // mixed precision for a whole batch, phase by phase as landau_staged does
 // it for one configuration
-static int batch_run(Batch *b) {
+// E: the FP64-link engine type of the batch's precision
+template <typename E>
+static int batch_run_t(Batch *b) {
   const Params p = to_params(&b->p);
   const size_t n = b->inst.size();
   if (!n) return 0;
@@ -1610,11 +1670,11 @@ static int batch_run(Batch *b) {
   CK(cudaEventCreate(&t1));
   CK(cudaDeviceSynchronize());
   CK(cudaEventRecord(t0, b->bs));
-  std::vector<Engine<double> *> e64(n);
+  std::vector<E *> e64(n);
   for (size_t i = 0; i < n; i++) {
     BatchInst &I = *b->inst[i];
     memset(&I.res, 0, sizeof I.res);
-    Engine<double> *e = I.e64.get();
+    E *e = I.fp64((E *)nullptr);
     e64[i] = e;
     const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
     CK(cudaMemcpyAsync(e->d_aos, I.links, bytes,
@@ -1657,7 +1717,7 @@ static int batch_run(Batch *b) {
   if (batch_solve(e64, p64, it64, th64, b->bs)) return -1;
   for (size_t i = 0; i < n; i++) {
     BatchInst &I = *b->inst[i];
-    Engine<double> *e = e64[i];
+    E *e = e64[i];
     if (e->to_aos(e->d_aos)) return -1;
     const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
     CK(cudaMemcpyAsync(I.links, e->d_aos, bytes,
@@ -1669,8 +1729,8 @@ static int batch_run(Batch *b) {
     I.res.theta = th64[i];
   }
   for (size_t i = 0; i < n; i++) {
-    CK(cudaEventRecord(b->inst[i]->e64->ev1, e64[i]->s));
-    CK(cudaStreamWaitEvent(b->bs, b->inst[i]->e64->ev1, 0));
+    CK(cudaEventRecord(e64[i]->ev1, e64[i]->s));
+    CK(cudaStreamWaitEvent(b->bs, e64[i]->ev1, 0));
   }
   CK(cudaEventRecord(t1, b->bs));
   CK(cudaEventSynchronize(t1));
@@ -1680,6 +1740,11 @@ static int batch_run(Batch *b) {
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   return 0;
+}
+
+static int batch_run(Batch *b) {
+  return b->p.precision == GFIX_MIXED ? batch_run_t<Engine<double, float>>(b)
+                                      : batch_run_t<Engine<double>>(b);
 }
 
 }  // namespace gfix
@@ -1741,6 +1806,7 @@ void gfix_release(void) {
   gfix_cuts_release();
   gfix_update_release();
   g_e64.clear();
+  g_e64m.clear();
   g_e32.clear();
   g_ec.clear();
   g_ec32.clear();
@@ -1758,39 +1824,60 @@ static int check_params(const size_t *dims, const gfix_params *p) {
   return 0;
 }
 
+}  // extern "C"
+
+// The engine that stages a Landau solve's links and runs its FP64-link
+// phase: FP64 fields under GFIX_FP64, FP32 fields under GFIX_MIXED (whose
+// FP32 phase runs on a further, all-FP32 engine)
+template <typename Fn>
+static int with_landau_engine(const size_t *dims, int precision, Fn &&fn) {
+  if (precision == GFIX_MIXED) {
+    Engine<double, float> *e = engine64m(dims);
+    return e ? fn(e) : -1;
+  }
+  Engine<double> *e = engine64(dims);
+  return e ? fn(e) : -1;
+}
+
+extern "C" {
+
 int gfix_landau(double *links, const size_t dims[4], const gfix_params *p,
                 gfix_result *r) {
   if (check_params(dims, p)) return -1;
   if (!links) return fail("null links");
-  Engine<double> *e = engine64(dims);
-  if (!e) return -1;
-  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
-  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
-  if (landau_staged(e, p, r)) return -1;
-  CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
-  CK(cudaStreamSynchronize(e->s));
-  return 0;
+  return with_landau_engine(dims, p->precision, [&](auto *e) -> int {
+    const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+    CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
+    if (landau_staged(e, p, r)) return -1;
+    CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
+    CK(cudaStreamSynchronize(e->s));
+    return 0;
+  });
 }
 
 int gfix_landau_device(double *d_links, const size_t dims[4],
                        const gfix_params *p, gfix_result *r) {
   if (check_params(dims, p)) return -1;
   if (!d_links) return fail("null links");
-  Engine<double> *e = engine64(dims);
-  if (!e) return -1;
-  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
-  // the caller's buffer is on the legacy default stream order
-  CK(cudaDeviceSynchronize());
-  CK(cudaMemcpyAsync(e->d_aos, d_links, bytes, cudaMemcpyDeviceToDevice, e->s));
-  if (landau_staged(e, p, r)) return -1;
-  CK(cudaMemcpyAsync(d_links, e->d_aos, bytes, cudaMemcpyDeviceToDevice, e->s));
-  CK(cudaStreamSynchronize(e->s));
-  return 0;
+  return with_landau_engine(dims, p->precision, [&](auto *e) -> int {
+    const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+    // the caller's buffer is on the legacy default stream order
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpyAsync(e->d_aos, d_links, bytes, cudaMemcpyDeviceToDevice, e->s));
+    if (landau_staged(e, p, r)) return -1;
+    CK(cudaMemcpyAsync(d_links, e->d_aos, bytes, cudaMemcpyDeviceToDevice, e->s));
+    CK(cudaStreamSynchronize(e->s));
+    return 0;
+  });
 }
+
+// (templates: C++ linkage inside the C ABI block)
+extern "C++" {
 
 // theta_test_lin, functional and plaquette of the links resident in e's
 // SoA buffer (out[0..2])
-static int observables_resident(Engine<double> *e, double *out) {
+template <typename E>
+static int observables_resident(E *e, double *out) {
   Params p;
   if (e->reset(p)) return -1;
   double tt = 0;
@@ -1798,7 +1885,7 @@ static int observables_resident(Engine<double> *e, double *out) {
   // theta_test leaves the functional sum of the same links in func
   out[0] = tt;
   out[1] = e->h_st->func;
-  k_plaquette<double><<<e->nb_site, kSiteThreads, 0, e->s>>>(e->c);
+  k_plaquette<<<e->nb_site, kSiteThreads, 0, e->s>>>(e->c);
   LAUNCHED(1);
   std::vector<double> part(e->nb_site);
   CK(cudaMemcpyAsync(part.data(), e->d_part, part.size() * sizeof(double),
@@ -1811,7 +1898,8 @@ static int observables_resident(Engine<double> *e, double *out) {
 }
 
 // host links -> e's AoS staging -> e's SoA links
-static int stage_host(Engine<double> *e, const double *links) {
+template <typename E>
+static int stage_host(E *e, const double *links) {
   const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
   CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
   return e->from_aos(e->d_aos);
@@ -1819,15 +1907,16 @@ static int stage_host(Engine<double> *e, const double *links) {
 
 // GLU's post-fix link diagnostics of the links resident in e (out[0..5],
 // as gfix_link_diagnostics)
-static int diagnostics_resident(Engine<double> *e, double *out) {
+template <typename E>
+static int diagnostics_resident(E *e, double *out) {
   const int T = e->c.L[3], lcu = e->V / T;
   const int nbs = (lcu + kDiagThreads - 1) / kDiagThreads;
   std::vector<double> part((size_t)kDiagVals * nbs * T);
   double *d_p = nullptr;
   CK(cudaMalloc(&d_p, part.size() * sizeof(double)));
-  Ctx<double> c = e->c;
+  auto c = e->c;
   c.part = d_p;
-  k_link_diag<double><<<dim3(nbs, T), kDiagThreads, 0, e->s>>>(c, lcu, nbs);
+  k_link_diag<<<dim3(nbs, T), kDiagThreads, 0, e->s>>>(c, lcu, nbs);
   LAUNCHED(1);
   CK(cudaMemcpyAsync(part.data(), d_p, part.size() * sizeof(double),
                      cudaMemcpyDeviceToHost, e->s));
@@ -1870,11 +1959,12 @@ static int diagnostics_resident(Engine<double> *e, double *out) {
 }
 
 // gf_check of the links resident in e: out[0..9] as gfix_gf_check
-static int gf_check_resident(Engine<double> *e, double *out) {
+template <typename E>
+static int gf_check_resident(E *e, double *out) {
   const int nb = e->nb_site;
   double *d_p = nullptr;
   CK(cudaMalloc(&d_p, (size_t)nb * kGfcVals * sizeof(double)));
-  Ctx<double> c = e->c;
+  auto c = e->c;
   c.part = d_p;
   k_gf_check<<<nb, kSiteThreads, 0, e->s>>>(c);
   LAUNCHED(1);
@@ -1909,7 +1999,8 @@ static int gf_check_resident(Engine<double> *e, double *out) {
 }
 
 // latt_reunitU of the links resident in e
-static int reunit_resident(Engine<double> *e) {
+template <typename E>
+static int reunit_resident(E *e) {
   const size_t nl = (size_t)e->V * 4;
   k_reunit_links<double><<<(unsigned)((nl + 255) / 256), 256, 0, e->s>>>(e->d_U,
                                                                          e->V);
@@ -1917,6 +2008,8 @@ static int reunit_resident(Engine<double> *e) {
   CK(cudaGetLastError());
   return 0;
 }
+
+}  // extern "C++"
 
 int gfix_observables(const double *links, const size_t dims[4], double *out) {
   if (!links || !dims || !out) return fail("null argument");
@@ -1991,7 +2084,10 @@ int gfix_fourier_accelerate(double *fields, const size_t dims[4], int ndim) {
 int gfix_profile_landau(const double *d_links, const size_t dims[4],
                         const gfix_params *p, int iters, double *ms,
                         double *bytes) {
-  if (check_params(dims, p)) return -1;
+  if (!p) return fail("null params");
+  gfix_params pc = *p;  // GFIX_PROFILE_POLISH is a profiling-only value
+  if (pc.precision == GFIX_PROFILE_POLISH) pc.precision = GFIX_MIXED;
+  if (check_params(dims, &pc)) return -1;
   if (!d_links || !ms || iters < 1) return fail("bad profile arguments");
   Engine<double> *e = engine64(dims);
   if (!e) return -1;
@@ -2001,6 +2097,14 @@ int gfix_profile_landau(const double *d_links, const size_t dims[4],
   if (e->from_aos(e->d_aos)) return -1;
   Params q = to_params(p);
   q.traj_cap = 0;
+  if (p->precision == GFIX_PROFILE_POLISH) {
+    // the second phase of a mixed solve: FP64 links, FP32 fields
+    Engine<double, float> *m = engine64m(dims);
+    if (!m) return -1;
+    CK(cudaMemcpyAsync(m->d_aos, d_links, n, cudaMemcpyDeviceToDevice, m->s));
+    if (m->from_aos(m->d_aos)) return -1;
+    return m->profile_cg(q, iters, ms, bytes);
+  }
   if (p->precision == GFIX_MIXED) {
     Engine<float> *f = engine32(dims);
     if (!f) return -1;
@@ -2111,25 +2215,25 @@ int gfix_landau_driver(double *links, const size_t dims[4], const gfix_params *p
                        gfix_result *r, double *obs, double *diag) {
   if (check_params(dims, p)) return -1;
   if (!links) return fail("null links");
-  Engine<double> *e = engine64(dims);
-  if (!e) return -1;
-  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
-  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
-  gfix_result res;
-  if (landau_staged(e, p, &res)) return -1;
-  if (res.iters != kSentinel && res.iters != kGluFailure) {
-    if (reunit_resident(e)) return -1;
-    if (obs && observables_resident(e, obs)) return -1;
-    if (diag && diagnostics_resident(e, diag)) return -1;
-    if (e->to_aos(e->d_aos)) return -1;
-  } else {
-    if (obs) memset(obs, 0, 3 * sizeof(double));
-    if (diag) memset(diag, 0, 6 * sizeof(double));
-  }
-  CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
-  CK(cudaStreamSynchronize(e->s));
-  if (r) *r = res;
-  return 0;
+  return with_landau_engine(dims, p->precision, [&](auto *e) -> int {
+    const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+    CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
+    gfix_result res;
+    if (landau_staged(e, p, &res)) return -1;
+    if (res.iters != kSentinel && res.iters != kGluFailure) {
+      if (reunit_resident(e)) return -1;
+      if (obs && observables_resident(e, obs)) return -1;
+      if (diag && diagnostics_resident(e, diag)) return -1;
+      if (e->to_aos(e->d_aos)) return -1;
+    } else {
+      if (obs) memset(obs, 0, 3 * sizeof(double));
+      if (diag) memset(diag, 0, 6 * sizeof(double));
+    }
+    CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
+    CK(cudaStreamSynchronize(e->s));
+    if (r) *r = res;
+    return 0;
+  });
 }
 
 // GLU's Coulomb driver in one device-resident sequence: the diagnostics of
@@ -2271,8 +2375,13 @@ static int batch_add(gfix_batch *b, double *links, const size_t dims[4],
   for (int k = 0; k < 4; k++) I->dims[k] = dims[k];
   I->links = links;
   I->device = device;
-  I->e64 = std::make_unique<Engine<double>>();
-  if (I->e64->init(dims, false, true)) return -1;
+  if (b->b.p.precision == GFIX_MIXED) {
+    I->e64m = std::make_unique<Engine<double, float>>();
+    if (I->e64m->init(dims, false, true)) return -1;
+  } else {
+    I->e64 = std::make_unique<Engine<double>>();
+    if (I->e64->init(dims, false, true)) return -1;
+  }
   b->b.inst.push_back(std::move(I));
   return (int)b->b.inst.size() - 1;
 }

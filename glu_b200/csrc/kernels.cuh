@@ -18,10 +18,14 @@
 // HBM layout (SoA, site index s = x + Lx (y + Ly (z + Lz t))):
 //   U   cx<R>[4 mu][6 elements][V]        links: their first two columns
 //                                          (load_link rebuilds the third)
-//   fb  cx<R>[2][4 fields][V]             in / in_old (parity selects)
-//   sb  cx<R>[2][4 fields][V]             sn ping-pong (sparity selects)
+//   fb  cx<F>[2][4 fields][V]             in / in_old (parity selects)
+//   sb  cx<F>[2][4 fields][V]             sn ping-pong (sparity selects)
 //   G   cx<R>[9][V]                        accumulated gauge transform
 //                                          (mixed precision only)
+// R is the type of the links (and of the link arithmetic), F that of the
+// su(3) fields and of the FFT: F = R except in the FP64 phase of a
+// mixed-precision solve, which keeps FP64 links, theta and updates but
+// carries its search directions and their Fourier acceleration in FP32.
 #pragma once
 
 #include "fft.cuh"
@@ -94,15 +98,15 @@ __global__ void k_begin_run(DevState *st) {
   st->use_ls = !st->sd_fixed;
 }
 
-template <typename R>
+template <typename R, typename F = R>
 struct Ctx {
   cx<R> *U;
-  cx<R> *fb[2];
-  cx<R> *sb[2];
+  cx<F> *fb[2];
+  cx<F> *sb[2];
   cx<R> *G;
   DevState *st;
   double *part;       // [nblocks][2] per-block partial sums
-  const cx<R> *tw;    // twiddle pool
+  const cx<F> *tw;    // twiddle pool
   const double *cs;   // cos tables, cs[mu * cs_ld + n] = cos(n 2pi/L_mu)
   int cs_ld;
   int L[4];
@@ -165,8 +169,8 @@ __device__ __forceinline__ int bck_site(int s, int mu, const int *x,
   return x[mu] == 0 ? s + (L[mu] - 1) * stride[mu] : s - stride[mu];
 }
 
-template <typename R>
-__device__ __forceinline__ void strides(const Ctx<R> &c, int *st) {
+template <typename CT>
+__device__ __forceinline__ void strides(const CT &c, int *st) {
   st[0] = 1;
   st[1] = c.L[0];
   st[2] = c.L[0] * c.L[1];
@@ -212,9 +216,9 @@ __device__ __forceinline__ void store_link(cx<R> *U, int V, int mu, int s,
 // K1: the gauge derivative, fused with the theta and functional sums
 // (src/Gfix/lin_derivs.c:74-193 packed as src/Gfix/FACG.c:54-60)
 
-template <typename R>
+template <typename R, typename F = R>
 __global__ void __launch_bounds__(kSiteThreads)
-    k_deriv(Ctx<R> c) {
+    k_deriv(Ctx<R, F> c) {
   if (c.st->done) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   double v[2] = {0.0, 0.0};
@@ -245,12 +249,12 @@ __global__ void __launch_bounds__(kSiteThreads)
       I4 += b5.y + b7.y - q5.y - q7.y;
       re += (double)q0.x + (double)q4.x + (double)q8.x;
     }
-    cx<R> *f = c.fb[c.st->parity];
+    cx<F> *f = c.fb[c.st->parity];
     const size_t V = c.V;
-    f[s] = mk<R>(-(R3 / R(3)), R0 / R(3));
-    f[V + s] = mk<R>(R(0.5) * R1, R(0.5) * I1);
-    f[2 * V + s] = mk<R>(R(0.5) * R2, R(0.5) * I2);
-    f[3 * V + s] = mk<R>(R(0.5) * R4, R(0.5) * I4);
+    f[s] = mk<F>((F)(-(R3 / R(3))), (F)(R0 / R(3)));
+    f[V + s] = mk<F>((F)(R(0.5) * R1), (F)(R(0.5) * I1));
+    f[2 * V + s] = mk<F>((F)(R(0.5) * R2), (F)(R(0.5) * I2));
+    f[3 * V + s] = mk<F>((F)(R(0.5) * R4), (F)(R(0.5) * I4));
     const double d0 = R0, d1 = R1, e1 = I1, d2 = R2, e2 = I2, d3 = R3,
                  d4 = R4, e4 = I4;
     v[0] = kVal49 * (d0 * d0 + d3 * (d3 + d0)) +
@@ -275,20 +279,25 @@ __global__ void __launch_bounds__(kSiteThreads)
 // accumulated as differences to the alpha = 0 value, which leaves the
 // parabola of approx_minimum unchanged and avoids cancelling large sums.
 
-template <typename R, bool DIR>
-__device__ __forceinline__ void dir_at(const Ctx<R> &c, const cx<R> *in,
-                                       const cx<R> *so, R beta, int s,
-                                       cx<R> *f) {
+// the direction at site s as stored (type F): computed in R, rounded to F;
+// f receives it back in R, so the probes use the direction the update reads
+template <typename R, bool DIR, typename F>
+__device__ __forceinline__ void dir_at(const Ctx<R, F> &c, const cx<F> *in,
+                                       const cx<F> *so, R beta, int s,
+                                       cx<R> *f, cx<F> *fs = nullptr) {
   const size_t V = c.V;
 #pragma unroll
   for (int k = 0; k < 4; k++) {
-    const cx<R> a = in[k * V + s];
+    const cx<F> a = in[k * V + s];
+    cx<F> r;
     if (DIR) {
-      const cx<R> b = so[k * V + s];
-      f[k] = mk<R>(fma(beta, b.x, a.x), fma(beta, b.y, a.y));
+      const cx<F> b = so[k * V + s];
+      r = mk<F>((F)fma(beta, (R)b.x, (R)a.x), (F)fma(beta, (R)b.y, (R)a.y));
     } else {
-      f[k] = a;
+      r = a;
     }
+    if (fs) fs[k] = r;
+    f[k] = mk<R>((R)r.x, (R)r.y);
   }
 }
 
@@ -297,23 +306,24 @@ __device__ __forceinline__ void dir_at(const Ctx<R> &c, const cx<R> *in,
 // theta < hp_below (1e-5), because per-site probe differences fall below
 // FP32 rounding once theta < ~1e-6; above it FP32 arithmetic serves.  Both
 // variants are launched, `sel` lets the one that fits the step run.
-template <typename R, bool DIR, typename C = R>
-__global__ void __launch_bounds__(kSiteThreads) k_dir_probe(Ctx<R> c, int sel) {
+template <typename R, bool DIR, typename C = R, typename F = R>
+__global__ void __launch_bounds__(kSiteThreads) k_dir_probe(Ctx<R, F> c, int sel) {
   if (c.st->done || arith_skip(sel, c.st->tr, c.st->hp_below)) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int par = c.st->parity, spar = c.st->sparity;
-  const cx<R> *in = c.fb[par];
-  const cx<R> *so = c.sb[spar];
-  cx<R> *sn = c.sb[spar ^ 1];
+  const cx<F> *in = c.fb[par];
+  const cx<F> *so = c.sb[spar];
+  cx<F> *sn = c.sb[spar ^ 1];
   const R beta = (R)c.st->beta;
   const bool probes = c.st->use_ls != 0;
   double v[2] = {0.0, 0.0};
   if (s < c.V) {
     cx<R> f[4];
-    dir_at<R, DIR>(c, in, so, beta, s, f);
+    cx<F> fs[4];
+    dir_at<R, DIR>(c, in, so, beta, s, f, fs);
     if (DIR) {
 #pragma unroll
-      for (int k = 0; k < 4; k++) sn[(size_t)k * c.V + s] = f[k];
+      for (int k = 0; k < 4; k++) sn[(size_t)k * c.V + s] = fs[k];
     }
     if (probes) {
       int x[4], sd[4];
@@ -358,23 +368,24 @@ __global__ void __launch_bounds__(kSiteThreads) k_dir_probe(Ctx<R> c, int sel) {
 // SN selects the direction: the new conjugate direction or `in`.
 // With G (mixed precision) the transform is accumulated, G(x) <- g(x) G(x).
 
-template <typename R, bool SN>
-__global__ void __launch_bounds__(kSiteThreads) k_update(Ctx<R> c) {
+template <typename R, bool SN, typename F = R>
+__global__ void __launch_bounds__(kSiteThreads) k_update(Ctx<R, F> c) {
   if (c.st->done) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= c.V) return;
-  const cx<R> *d = SN ? c.sb[c.st->sparity ^ 1] : c.fb[c.st->parity];
+  const cx<F> *d = SN ? c.sb[c.st->sparity ^ 1] : c.fb[c.st->parity];
   const R alpha = (R)c.st->alpha;
   const size_t V = c.V;
   int x[4], sd[4];
   coords(s, c.L, x);
   strides(c, sd);
+  auto up = [](cx<F> a) { return mk<R>((R)a.x, (R)a.y); };
   cx<R> A[9], Bm[9], U[9];
-  set_gauge(A, d[s], d[V + s], d[2 * V + s], d[3 * V + s], alpha);
+  set_gauge(A, up(d[s]), up(d[V + s]), up(d[2 * V + s]), up(d[3 * V + s]), alpha);
 #pragma unroll 1
   for (int mu = 0; mu < 4; mu++) {
     const int y = fwd_site(s, mu, x, c.L, sd);
-    set_gauge(Bm, d[y], d[V + y], d[2 * V + y], d[3 * V + y], alpha);
+    set_gauge(Bm, up(d[y]), up(d[V + y]), up(d[2 * V + y]), up(d[3 * V + y]), alpha);
     load_link(c.U, c.V, mu, s, U);
     gtransform(A, U, Bm);
     store_link(c.U, c.V, mu, s, U);

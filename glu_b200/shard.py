@@ -18,18 +18,46 @@ from dataclasses import dataclass
 import numpy as np
 
 
-def slice_blocks(lt: int, world: int) -> list[tuple[int, int]]:
-    """Contiguous, balanced blocks [t0, t1) of the lt slices, one per rank;
-    every block holds at least two slices."""
+def slice_blocks(lt: int, world: int, costs=None) -> list[tuple[int, int]]:
+    """Contiguous blocks [t0, t1) of the lt slices, one per rank, every block
+    holding at least two slices.
+
+    Without costs the blocks hold equal numbers of slices.  With costs (the
+    expected cost of each slice, e.g. its volume times the iterations it is
+    expected to take: per-slice counts vary severalfold within one
+    configuration) the blocks minimise the largest block cost, exactly (a
+    linear-partition dynamic programme over the prefix sums)."""
     if world < 1 or lt < 2 * world:
         raise ValueError(f"{lt} time slices cannot give {world} ranks two each")
-    base, extra = divmod(lt, world)
-    out, t0 = [], 0
-    for r in range(world):
-        n = base + (1 if r < extra else 0)
-        out.append((t0, t0 + n))
-        t0 += n
-    return out
+    if costs is None:
+        base, extra = divmod(lt, world)
+        out, t0 = [], 0
+        for r in range(world):
+            n = base + (1 if r < extra else 0)
+            out.append((t0, t0 + n))
+            t0 += n
+        return out
+    c = np.asarray(costs, dtype=np.float64)
+    if c.shape != (lt,) or not np.all(np.isfinite(c)) or np.any(c < 0):
+        raise ValueError("costs must be lt finite, non-negative numbers")
+    pre = np.concatenate([[0.0], np.cumsum(c)])
+    inf = float("inf")
+    # best[r][t]: the least largest block cost of slices [0, t) in r blocks
+    best = np.full((world + 1, lt + 1), inf)
+    cut = np.zeros((world + 1, lt + 1), dtype=np.int64)
+    best[0][0] = 0.0
+    for r in range(1, world + 1):
+        for t in range(2 * r, lt - 2 * (world - r) + 1):
+            s = np.arange(2 * (r - 1), t - 1)  # the last block is [s, t)
+            cand = np.maximum(best[r - 1][s], pre[t] - pre[s])
+            k = int(np.argmin(cand))
+            best[r][t], cut[r][t] = cand[k], s[k]
+    out, t = [], lt
+    for r in range(world, 0, -1):
+        s = int(cut[r][t])
+        out.append((s, t))
+        t = s
+    return out[::-1]
 
 
 @dataclass

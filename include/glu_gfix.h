@@ -104,7 +104,13 @@ int cuts_struct(struct site *A, const struct cut_info CUTINFO);
  * ------------------------------------------------------------------- */
 
 enum gfix_algo { GFIX_CG = 0, GFIX_SD = 1 };
-enum gfix_precision { GFIX_FP64 = 0, GFIX_MIXED = 1 };
+/* GFIX_MIXED: FP32 links, fields and FFT until theta < switch_theta (or a
+ * stall of the FP32 run), then FP64 links, theta and updates to the
+ * requested accuracy with the search directions and their Fourier
+ * acceleration in FP32 (their relative precision is all a descent
+ * direction needs).  GFIX_PROFILE_POLISH: gfix_profile_landau only, the
+ * kernels of that second phase. */
+enum gfix_precision { GFIX_FP64 = 0, GFIX_MIXED = 1, GFIX_PROFILE_POLISH = 2 };
 
 typedef struct gfix_params {
   double gf_alpha;       /* GLU's GF_TUNE (Latt.gf_alpha)                  */
@@ -274,7 +280,8 @@ int gfix_fourier_accelerate(double *fields, const size_t dims[4], int ndim);
  * HBM bytes of one launch, for k = 0 derivative+theta, 1 xy FFT forward,
  * 2 zt FFT with psq, 3 xy FFT inverse + PR sums, 4 direction + line-search
  * probes, 5 link update, 6 the scalar-control launches of one iteration.
- * precision GFIX_MIXED profiles the FP32 kernels. */
+ * precision GFIX_MIXED profiles the FP32 kernels, GFIX_PROFILE_POLISH those
+ * of a mixed solve's FP64-link phase. */
 int gfix_profile_landau(const double *d_links, const size_t dims[4],
                         const gfix_params *p, int iters, double *ms,
                         double *bytes);

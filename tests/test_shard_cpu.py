@@ -148,3 +148,78 @@ def test_sharded_transform_equals_whole_lattice(tmp_path, world):
     ref = _transform_whole(_links())
     assert np.abs(got - ref).max() < 1e-13
     assert iters == DIMS[3]  # each mock slice reports one iteration
+
+
+def test_slice_blocks_by_cost_minimise_the_largest_block():
+    # exact optimum of the linear partition, checked by exhaustion
+    import itertools
+    rng = np.random.default_rng(5)
+    for lt, world in ((8, 2), (9, 3), (12, 4), (10, 2)):
+        c = rng.uniform(0.2, 5.0, size=lt)
+        got = slice_blocks(lt, world, c)
+        assert got[0][0] == 0 and got[-1][1] == lt
+        assert all(b - a >= 2 for a, b in got)
+        assert all(got[i][1] == got[i + 1][0] for i in range(world - 1))
+        worst = max(c[a:b].sum() for a, b in got)
+        best = min(
+            max(c[a:b].sum() for a, b in zip((0,) + cuts, cuts + (lt,)))
+            for cuts in itertools.combinations(range(2, lt - 1), world - 1)
+            if all(b - a >= 2 for a, b in zip((0,) + cuts, cuts + (lt,))))
+        assert abs(worst - best) < 1e-12
+    with pytest.raises(ValueError):
+        slice_blocks(8, 2, np.ones(7))
+
+
+COSTS = np.array([6.0, 4.0, 1.0, 1.0, 1.0, 1.0, 1.0, 5.0])  # slices of DIMS
+UNIT_S = 0.05  # seconds of mock solving per unit of cost
+
+
+def _timed_rank(rank, world, port, out, weighted):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import time
+        U = _links()
+        lcu = DIMS[0] * DIMS[1] * DIMS[2]
+        t0, t1 = slice_blocks(DIMS[3], world, COSTS if weighted else None)[rank]
+        block = torch.from_numpy(
+            np.ascontiguousarray(U[t0 * lcu:t1 * lcu]).view(np.float64).reshape(-1).copy())
+        dims = (DIMS[0], DIMS[1], DIMS[2], t1 - t0)
+        solve, finish = _mock_solver(t0)
+
+        def slow_solve(links, d, g_first, g_last):
+            # a slice costs UNIT_S x its cost: uneven per-slice iterations
+            time.sleep(UNIT_S * COSTS[t0:t1].sum())
+            return solve(links, d, g_first, g_last)
+
+        dist.barrier()
+        start = time.perf_counter()
+        coulomb_sharded(block, dims, solver=(slow_solve, finish))
+        mine = torch.tensor([time.perf_counter() - start], dtype=torch.float64)
+        times = [torch.zeros(1, dtype=torch.float64) for _ in range(world)]
+        dist.all_gather(times, mine)
+        if rank == 0:
+            np.save(out, np.array([float(t.item()) for t in times]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_cost_weighted_blocks_balance_uneven_slices(tmp_path):
+    """Two gloo ranks, slices of uneven cost (a mock solver whose time is
+    proportional to the block's cost): the count-balanced split leaves one
+    rank 12 of 20 units; the cost-weighted split gives each 10, and the
+    ranks' solve times agree within 10%."""
+    import torch.multiprocessing as mp
+    res = {}
+    for weighted in (False, True):
+        out = str(tmp_path / f"t{int(weighted)}.npy")
+        mp.spawn(_timed_rank, args=(2, _free_port(), out, weighted), nprocs=2, join=True)
+        res[weighted] = np.load(out)
+    # each rank's own time includes its wait for the boundary exchange, so
+    # compare through the busier rank's time
+    even, weighted = res[False], res[True]
+    assert max(even) > 1.1 * max(weighted)
+    blocks = slice_blocks(DIMS[3], 2, COSTS)
+    costs = [COSTS[a:b].sum() for a, b in blocks]
+    assert max(costs) <= 1.1 * min(costs)
