@@ -21,7 +21,8 @@ class GfixParams(C.Structure):
                 ("sd_fixed_step", C.c_int), ("precision", C.c_int),
                 ("switch_theta", C.c_double), ("traj_theta", _dp),
                 ("traj_func", _dp), ("traj_cap", C.c_size_t),
-                ("max_restarts", C.c_int), ("restart_seed", C.c_uint64)]
+                ("max_restarts", C.c_int), ("restart_seed", C.c_uint64),
+                ("luxury_copies", C.c_int), ("luxury_best", C.c_int)]
 
 
 class GfixCutInfo(C.Structure):

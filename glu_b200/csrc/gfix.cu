@@ -156,6 +156,7 @@ class Engine {
   cx<F> *d_tw = nullptr, *d_F = nullptr;
   cx<R> *d_U = nullptr, *d_G = nullptr;
   double *d_aos = nullptr;  // AoS FP64 staging (only FP64 engines)
+  cx<R> *d_best = nullptr;  // luxury copies: the kept copy's links
   size_t traj_alloc = 0;
   int nb_site = 0;
   dim3 g_xy, g_zt;
@@ -202,6 +203,8 @@ class Engine {
     cudaFree(d_F);
     cudaFree(d_G);
     cudaFree(d_aos);
+    cudaFree(d_best);
+    d_best = nullptr;
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (s) cudaStreamDestroy(s);
@@ -1414,15 +1417,14 @@ static int mixed_handover(E *e, Engine<float> *f, const Params &p64,
 }
 
 // One Landau solve (GLU's FACG / FASD, or the mixed-precision pair of
-// them) from the staged input; the fixed links are left in e64's SoA
-// links.  attempt > 0: a random restart (stage_input).
+// them) of the links resident in e64's SoA buffer, to the accuracy and
+// iteration bound of p; the fixed links are left there.  attempt: the
+// random restart whose start a failed mixed first phase goes back to.
 template <typename E>
-static int landau_attempt(E *e64, const gfix_params *gp, int attempt,
-                          gfix_result *r) {
-  Params p = to_params(gp);
+static int solve_resident(E *e64, const gfix_params *gp, const Params &p,
+                          int attempt, gfix_result *r) {
   gfix_result res;
   memset(&res, 0, sizeof res);
-  if (stage_input(e64, gp->restart_seed, attempt)) return -1;
   size_t iters = 0;
   double th = 0.0;
   size_t tl = 0;
@@ -1479,9 +1481,92 @@ static int landau_attempt(E *e64, const gfix_params *gp, int attempt,
 }
 
 // GLU's Landau driver prints every failed attempt (print_failure_info,
-// src/Gfix/Landau.c:70-86); the flat entry points stay silent
+// src/Gfix/Landau.c:70-86) and every gauge copy; the flat entry points
+// stay silent
 static thread_local bool t_restart_log = false;
 void set_restart_log(bool on) { t_restart_log = on; }
+
+// GLU's luxury_copy_fast (src/Gfix/Landau.c:92-211, compiled in with
+// LUXURY_GAUGE): gp->luxury_copies random gauge copies of the attempt's
+// start, each fixed to theta < 1e-6 in at most 1000 iterations; of the
+// copies that converged within the bound, the one with the largest gauge
+// functional is kept -- the smallest with gp->luxury_best (GLU's
+// BEST_COPY) -- and fixed to the requested accuracy.  The count is GLU's:
+// the last copy's iterations plus the final fix's.  Copies are transformed
+// by this library's generator; if no copy is kept, the final fix starts
+// from the attempt's start (GLU's would start from an unset lattice).
+template <typename E>
+static int luxury_resident(E *e64, const gfix_params *gp, int attempt,
+                           gfix_result *r) {
+  constexpr double kCopyAcc = 1E-6;    // Landau.c:142
+  constexpr size_t kCopyMax = 1000;    // Landau.c:143
+  Params pc = to_params(gp);
+  pc.acc = kCopyAcc;
+  pc.max_iters = kCopyMax;
+  pc.traj_cap = 0;
+  pc.traj_theta = pc.traj_func = nullptr;
+  gfix_params gc = *gp;
+  gc.accuracy = kCopyAcc;
+  gc.max_iters = kCopyMax;
+  gc.traj_cap = 0;
+  gc.traj_theta = gc.traj_func = nullptr;
+  if (!e64->d_best)
+    CK(cudaMalloc(&e64->d_best, (size_t)e64->V * 4 * kLinkCx * sizeof(cx<double>)));
+  const size_t bytes = (size_t)e64->V * 4 * kLinkCx * sizeof(cx<double>);
+  double keep = gp->luxury_best ? 1.0 : 0.0;  // Landau.c:122-126
+  bool kept = false;
+  size_t iters = 0;
+  int restarts = 0;
+  for (int copy = 0; copy < gp->luxury_copies; copy++) {
+    if (stage_input(e64, gp->restart_seed, attempt)) return -1;
+    const int id = (1 << 20) + attempt * 4096 + copy;  // distinct from restarts
+    k_random_transform<<<e64->nb_site, kSiteThreads, 0, e64->s>>>(
+        e64->c, gp->restart_seed, id);
+    LAUNCHED(1);
+    gfix_result rc;
+    if (solve_resident(e64, &gc, pc, attempt, &rc)) return -1;
+    restarts += rc.restarts;
+    iters = rc.iters;
+    double tt = 0.0;
+    Params q;
+    if (e64->reset(q) || e64->theta_test(&tt)) return -1;
+    const double f = e64->h_st->func;  // gauge_functional of the copy
+    const bool ok = iters != kCopyMax && iters != kSentinel &&
+                    (gp->luxury_best ? f < keep : f > keep);
+    if (t_restart_log)
+      fprintf(stdout, "  [COPY] %d [FUNCTIONAL] %1.15f [ITER] %zu %s", copy, f,
+              iters, ok ? " -> Copy accepted\n" : "");
+    if (ok) {
+      keep = f;
+      kept = true;
+      CK(cudaMemcpyAsync(e64->d_best, e64->d_U, bytes, cudaMemcpyDeviceToDevice,
+                         e64->s));
+    } else if (t_restart_log) {
+      fprintf(stdout, " -> Copy rejected %e\n", f - keep);
+    }
+  }
+  if (kept) {
+    CK(cudaMemcpyAsync(e64->d_U, e64->d_best, bytes, cudaMemcpyDeviceToDevice, e64->s));
+  } else if (stage_input(e64, gp->restart_seed, attempt)) {
+    return -1;
+  }
+  gfix_result rf;
+  if (solve_resident(e64, gp, to_params(gp), attempt, &rf)) return -1;
+  rf.iters = rf.iters + iters;  // Landau.c:187-191: added to the last copy's
+  rf.restarts += restarts;
+  *r = rf;
+  return 0;
+}
+
+// One Landau attempt: the staged input (a restart's random transform of it
+// for attempt > 0), then GLU's solve or its luxury copies
+template <typename E>
+static int landau_attempt(E *e64, const gfix_params *gp, int attempt,
+                          gfix_result *r) {
+  if (stage_input(e64, gp->restart_seed, attempt)) return -1;
+  if (gp->luxury_copies > 0) return luxury_resident(e64, gp, attempt, r);
+  return solve_resident(e64, gp, to_params(gp), attempt, r);
+}
 
 // A Landau fix of the links staged in e64->d_aos, with GLU's random
 // restarts (src/Gfix/Landau.c:303-340) when p->max_restarts > 0: after a
@@ -1821,6 +1906,7 @@ static int check_params(const size_t *dims, const gfix_params *p) {
     return fail("unknown precision %d", p->precision);
   if (p->traj_cap && !p->traj_theta) return fail("traj_cap without traj_theta");
   if (p->max_restarts < 0) return fail("max_restarts %d below 0", p->max_restarts);
+  if (p->luxury_copies < 0) return fail("luxury_copies %d below 0", p->luxury_copies);
   return 0;
 }
 

@@ -9,6 +9,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -46,6 +47,17 @@ void env_precision(gfix_params *p) {
     const double x = atof(s);
     if (x > 0) p->switch_theta = pow(10.0, -x);
   }
+}
+
+// GLU's compile-time Landau options, which a program linked against this
+// library sets at run time instead (GLU's own #defines do not reach here):
+//   GLU_GFIX_LUXURY   = N  (LUXURY_GAUGE: N random gauge copies per attempt)
+//   GLU_GFIX_BEST_COPY = 1 (BEST_COPY: keep the copy of least functional)
+void env_luxury(gfix_params *p) {
+  p->luxury_copies = 0;
+  p->luxury_best = 0;
+  if (const char *s = getenv("GLU_GFIX_LUXURY")) p->luxury_copies = std::max(0, atoi(s));
+  if (const char *s = getenv("GLU_GFIX_BEST_COPY")) p->luxury_best = atoi(s) != 0;
 }
 
 void dims_of(size_t *d) {
@@ -193,6 +205,7 @@ size_t Landau(struct site *lat, const double accuracy, const size_t iter,
   p.max_restarts = kGfGluFailures - 1;
   p.restart_seed = Latt.Seed[0];
   env_precision(&p);
+  env_luxury(&p);
   gfix_result r;
   double obs[3] = {0, 0, 0}, dg[6] = {0, 0, 0, 0, 0, 0};
   gfix::set_restart_log(true);

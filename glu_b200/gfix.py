@@ -60,7 +60,7 @@ def _links(links, d):
 
 
 def _params(alpha, acc, max_iters, algo, sd_fixed, precision, switch, cap,
-            max_restarts=0, restart_seed=0):
+            max_restarts=0, restart_seed=0, luxury_copies=0, luxury_best=False):
     tt = np.zeros(max(cap, 1))
     tf = np.zeros(max(cap, 1))
     p = GfixParams()
@@ -78,23 +78,30 @@ def _params(alpha, acc, max_iters, algo, sd_fixed, precision, switch, cap,
         raise ValueError("max_restarts must be >= 0")
     p.max_restarts = int(max_restarts)
     p.restart_seed = int(restart_seed) & 0xFFFFFFFFFFFFFFFF
+    if int(luxury_copies) < 0:
+        raise ValueError("luxury_copies must be >= 0")
+    p.luxury_copies = int(luxury_copies)
+    p.luxury_best = int(bool(luxury_best))
     return p, tt, tf
 
 
 def landau_fix(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
                algo="FACG", sd_fixed_step=False, precision="FP64",
                switch_theta=1e-9, traj_cap=0, max_restarts=0,
-               restart_seed=0) -> FixResult:
+               restart_seed=0, luxury_copies=0, luxury_best=False) -> FixResult:
     """Landau FA gauge fixing (GLU's FACG/FASD) of a copy of `links`.
     max_restarts > 0 adds GLU's random restarts after a failed solve (its
     Landau driver, src/Gfix/Landau.c:303-340); iters then follows GLU's
-    sums and is GLU_FAILURE when every attempt failed."""
+    sums and is GLU_FAILURE when every attempt failed.  luxury_copies > 0
+    makes each attempt GLU's luxury_copy_fast (Landau.c:92-211): that many
+    random gauge copies fixed to 1e-6, the one of largest functional kept
+    (smallest with luxury_best, GLU's BEST_COPY) and fixed to accuracy."""
     lib = _lib.load()
     cd, d = _dims(dims)
     U = _links(links, d)
     p, tt, tf = _params(gf_alpha, accuracy, max_iters, algo, sd_fixed_step,
                         precision, switch_theta, traj_cap, max_restarts,
-                        restart_seed)
+                        restart_seed, luxury_copies, luxury_best)
     r = GfixResult()
     check(lib.gfix_landau(U.ctypes.data, cd, C.byref(p), C.byref(r)))
     n = r.traj_len
@@ -211,7 +218,7 @@ class DriverResult:
 def landau_driver(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
                   algo="FACG", sd_fixed_step=False, precision="FP64",
                   switch_theta=1e-9, max_restarts=GF_GLU_FAILURES - 1,
-                  restart_seed=1) -> DriverResult:
+                  restart_seed=1, luxury_copies=0, luxury_best=False) -> DriverResult:
     """GLU's Landau driver (src/Gfix/Landau.c:261-374) in one pass on the GPU
     (gfix_landau_driver): the solve with random restarts, then the
     reunitarised links and output_fixing_info's numbers."""
@@ -219,7 +226,8 @@ def landau_driver(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
     cd, d = _dims(dims)
     U = _links(links, d)
     p, _, _ = _params(gf_alpha, accuracy, max_iters, algo, sd_fixed_step,
-                      precision, switch_theta, 0, max_restarts, restart_seed)
+                      precision, switch_theta, 0, max_restarts, restart_seed,
+                      luxury_copies, luxury_best)
     r = GfixResult()
     obs = np.zeros(3)
     dg = np.zeros(6)

@@ -127,6 +127,8 @@ typedef struct gfix_params {
                          /*   (0: none, as GLU's FACG/FASD; GLU's Landau   */
                          /*   driver makes GF_GLU_FAILURES - 1 = 6)        */
   uint64_t restart_seed; /* seed of the restarts' random gauge transforms  */
+  int luxury_copies;     /* Landau: GLU's LUXURY_GAUGE copies (0: none)     */
+  int luxury_best;       /* 1: keep the copy of least functional (BEST_COPY)*/
 } gfix_params;
 
 typedef struct gfix_result {
@@ -155,7 +157,17 @@ typedef struct gfix_result {
  * r->iters then follows GLU's accounting: the first attempt's sentinel,
  * plus max_iters per failed restart, plus the successful attempt's count;
  * (size_t)-1 (GLU_FAILURE) when every attempt failed, the links then being
- * the last attempt's.  r->restarts counts the restarts made. */
+ * the last attempt's.  r->restarts counts the restarts made.
+ *
+ * With p->luxury_copies = N > 0 each attempt is GLU's luxury_copy_fast
+ * (src/Gfix/Landau.c:92-211, a LUXURY_GAUGE build): N random gauge copies
+ * of the attempt's start (this library's generator), each fixed to theta <
+ * 1e-6 in at most 1000 iterations; of the copies that converged within that
+ * bound the one with the largest gauge functional is kept (GLU's default;
+ * the smallest with p->luxury_best, GLU's BEST_COPY) and fixed to
+ * p->accuracy.  r->iters is then GLU's sum: the last copy's iterations plus
+ * the final fix's.  If no copy is kept the final fix starts from the
+ * attempt's start.  Batches ignore both restarts and copies. */
 int gfix_landau(double *links, const size_t dims[4], const gfix_params *p,
                 gfix_result *r);
 

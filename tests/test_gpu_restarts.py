@@ -88,3 +88,29 @@ def test_a_restart_converges_where_the_first_attempt_failed(hb8):
         if found:
             break
     assert found is not None, "no restart converged"
+
+
+def test_luxury_copies(hb8):
+    """GLU's luxury_copy_fast (LUXURY_GAUGE, src/Gfix/Landau.c:92-211):
+    random gauge copies fixed to 1e-6, one kept -- the largest functional by
+    default, the smallest under BEST_COPY -- then fixed to the accuracy.
+    With the same seed both rules choose among the same copies, so the
+    BEST_COPY result's functional is not above the default's."""
+    g = hb8
+    d = _dims(g)
+    runs = {}
+    for best in (False, True):
+        r = gfix.landau_fix(g["links"], d, 0.08, 1e-14, 2000, "FACG",
+                            luxury_copies=4, luxury_best=best, restart_seed=9)
+        assert r.iters != gfix.SENTINEL and r.iters > 0
+        assert r.theta < 1e-14
+        fixed = gfix.latt_reunitU(r.links, d)
+        assert abs(gfix.av_plaquette(fixed, d) - g["plaquette"]) < 1e-13
+        runs[best] = gfix.gauge_functional(r.links, d)
+    assert runs[True] <= runs[False] + 1e-9
+    # the copies start from random points of the orbit: the kept copy is
+    # not the plain fix of the input
+    plain = gfix.landau_fix(g["links"], d, 0.08, 1e-14, 2000, "FACG")
+    r = gfix.landau_fix(g["links"], d, 0.08, 1e-14, 2000, "FACG",
+                        luxury_copies=1, restart_seed=9)
+    assert np.abs(r.links - plain.links).max() > 1e-3
