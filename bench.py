@@ -625,6 +625,21 @@ C_KERNELS = ["k_cderiv", "k_fft_xy_fwd_c", "k_fft_z_c", "k_fft_xy_bwd_sums_c",
              "k_cprobe", "k_cupdate", "k_cscalar"]
 
 
+# the input of the Coulomb workload: a beta 6.0 heatbath configuration
+# generated on the GPU (seed 4, rank r: 4 + r), C_HB_ITERS iterations of one
+# heatbath and four over-relaxation sweeps from the unit start -- 1000 at
+# 64^3x128 would take ~3.5 minutes of GPU time per run, and its plaquette is
+# settled well before 200
+C_HB_ITERS = 200
+C_INPUT = "heatbath beta 6.0, %d x (HB + 4 OR), unit start, seed %%d" % C_HB_ITERS
+
+
+def coulomb_input(dims, seed):
+    """the Coulomb workload's input, on the device (no host copy)"""
+    from glu_b200.workload import heatbath_config_device
+    return heatbath_config_device(dims, seed=seed, iterations=C_HB_ITERS, beta=6.0, n_or=4)
+
+
 def _cparams(prec: str = "fp64"):
     p = _params(prec)
     p.gf_alpha = C_ALPHA
@@ -638,7 +653,7 @@ def coulomb_steps_record(dims):
     f = ROOT / "profiles" / "coulomb_full_fix.json"
     if f.exists():
         for e in json.loads(f.read_text()):
-            if tuple(e["dims"]) == tuple(dims):
+            if tuple(e["dims"]) == tuple(dims) and e.get("input") == C_INPUT % 4:
                 return int(e["slice_steps"]), e
     return None, None
 
@@ -669,7 +684,6 @@ def coulomb_gpu(args, dims, rank, world, local):
     torch.cuda.set_device(local)
     from glu_b200 import _lib
     from glu_b200._lib import GfixResult, check
-    from glu_b200.workload import tiled_config_device
     lib = _lib.load()
     dist = None
     if world > 1:
@@ -690,7 +704,7 @@ def coulomb_gpu(args, dims, rank, world, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    U = tiled_config_device(dims, seed=4 + rank)
+    U = coulomb_input(dims, 4 + rank)
     dpristine = torch.view_as_real(U).reshape(-1).contiguous()
     del U
     dwork = torch.empty_like(dpristine)
@@ -709,21 +723,6 @@ def coulomb_gpu(args, dims, rank, world, local):
                  sth.ctypes.data_as(C.POINTER(C.c_double)),
                  sit.ctypes.data_as(C.POINTER(C.c_size_t))))
         return r
-
-    def plaquette(ptr, reunit=False):
-        if reunit:
-            check(lib.gfix_reunit(ptr, cd))
-        o = np.zeros(3)
-        check(lib.gfix_observables(ptr, cd, o.ctypes.data_as(C.POINTER(C.c_double))))
-        return float(o[2])
-
-    # every fixed configuration must stay on its input's gauge orbit: the
-    # average plaquette of the last step's fixed links (host side, after
-    # the timed region), reunitarised as GLU's Landau driver does before it
-    # reports (output_fixing_info: over a long fix the links drift off
-    # SU(3) through GLU's update, which rebuilds one column from the other
-    # two), against the input's
-    plaq_in = [plaquette(h.data_ptr()) for h in hosts]
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     out = {}
@@ -806,7 +805,8 @@ def coulomb_line(args, dims, world, res, cpu):
         "ms_per_step": res["ms"] / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if args.precision == "mixed" else "f64",
-        "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled + seeded random gauge transform, on device)",
+        "data": "synthetic: %s (generated on the GPU before timing; rank r: seed 4 + r)"
+                % (C_INPUT % 4),
         "config": {"workload": "Coulomb FACG theta<1e-14 per slice, %s" % "x".join(map(str, dims)),
                    "dims": list(dims), "gf_alpha": C_ALPHA, "accuracy": ACC,
                    "precision": args.precision, "iters": res["iters"][-1],
@@ -869,13 +869,12 @@ def coulomb_shard(args, dims, rank, world, local):
     import torch.distributed as dist
     torch.cuda.set_device(local)
     from glu_b200.shard import coulomb_sharded, slice_blocks
-    from glu_b200.workload import tiled_config_device
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     t0, t1 = slice_blocks(dims[3], world)[rank]
     lcu = dims[0] * dims[1] * dims[2]
-    U = tiled_config_device(dims, seed=4)
+    U = coulomb_input(dims, 4)
     block = torch.view_as_real(U[t0 * lcu:t1 * lcu]).reshape(-1).contiguous()
     del U
     bdims = (dims[0], dims[1], dims[2], t1 - t0)
@@ -933,7 +932,7 @@ def coulomb_shard(args, dims, rank, world, local):
               "n_gpus": world, "steps": steps, "warmup": args.warmup,
               "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "strong",
               "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64",
-              "data": "synthetic (8^4 GLU heatbath beta 6.0 tiled + seeded random gauge transform, on device)",
+              "data": "synthetic: %s (generated on the GPU before timing)" % (C_INPUT % 4),
               "config": {"workload": "Coulomb FACG theta<1e-14 per slice, %s, slices split over ranks"
                                      % "x".join(map(str, dims)),
                          "dims": list(dims), "precision": args.precision, "iters": iters,
@@ -1124,21 +1123,6 @@ def ensemble_main(args, rank, world, local):
     cds = [(C.c_size_t * 4)(*d) for d, _ in cfgs]
     nbytes = sum(t.numel() * 8 for t in pristine)
     sites = sum(int(np.prod(d)) for d, _ in cfgs)
-    def plaquette(ptr, reunit=False):
-        if reunit:
-            check(lib.gfix_reunit(ptr, cd))
-        o = np.zeros(3)
-        check(lib.gfix_observables(ptr, cd, o.ctypes.data_as(C.POINTER(C.c_double))))
-        return float(o[2])
-
-    # every fixed configuration must stay on its input's gauge orbit: the
-    # average plaquette of the last step's fixed links (host side, after
-    # the timed region), reunitarised as GLU's Landau driver does before it
-    # reports (output_fixing_info: over a long fix the links drift off
-    # SU(3) through GLU's update, which rebuilds one column from the other
-    # two), against the input's
-    plaq_in = [plaquette(h.data_ptr()) for h in hosts]
-
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
     out = {}
     with Clocks(local) as clk:
