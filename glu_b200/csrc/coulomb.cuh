@@ -382,33 +382,55 @@ __global__ void __launch_bounds__(kCoulThreads) k_cmaint(CCtx<R> c, int what) {
 
 enum CoulOp : int { C_SUMS = 0, C_PROBES = 1, C_END1 = 2, C_END2 = 3 };
 
-// one thread per slice: fixed-order sums of the slice's partials and GLU's
-// control flow of steep_step_FACG / _FASD and steep_fix
-// (src/Gfix/CFACG.c:285-529)
+// one warp per slice: fixed-order sums of the slice's partials (each lane
+// a strided subset in order, then a fixed shuffle tree), and GLU's control
+// flow of steep_step_FACG / _FASD and steep_fix (src/Gfix/CFACG.c:285-529)
+// on lane 0.
 // Partials: C_SUMS reads the inverse xy FFT pass's per-plane pairs (plane
 // index field * nplanes + t * lz + z), C_PROBES the probe kernel's per-block
 // pairs (t * nbs + block).
-__global__ void k_cscalar(CoulState *cs, Slice *sl, const double *part,
-                          int nbs, int lz, int nplanes, int op, double Lcu,
-                          DevState *st) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+constexpr int kCScalarSlices = 4;  // slices (warps) per block
+
+__global__ void __launch_bounds__(32 * kCScalarSlices)
+    k_cscalar(CoulState *cs, Slice *sl, const double *part, int nbs, int lz,
+              int nplanes, int op, double Lcu, DevState *st) {
+  const int t = blockIdx.x * kCScalarSlices + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   if (t < cs->nslices) {
     Slice &S = sl[t];
     if (S.mode != SL_DONE) {
       double a0 = 0.0, a1 = 0.0;
       if (op == C_SUMS) {
-        for (int f = 0; f < 4; f++)
-          for (int z = 0; z < lz; z++) {
-            const size_t b = (size_t)f * nplanes + (size_t)t * lz + z;
-            a0 += part[2 * b];
-            a1 += part[2 * b + 1];
-          }
+        const int n = 4 * lz;  // (field, z) pairs, field-major
+        for (int j = lane; j < n; j += 32) {
+          const int f = j / lz, z = j % lz;
+          const size_t b = (size_t)f * nplanes + (size_t)t * lz + z;
+          a0 += part[2 * b];
+          a1 += part[2 * b + 1];
+        }
       } else if (op == C_PROBES) {
-        for (int b = 0; b < nbs; b++) {
-          a0 += part[2 * ((size_t)t * nbs + b)];
-          a1 += part[2 * ((size_t)t * nbs + b) + 1];
+        constexpr int kU = 4;
+        for (int b0 = lane; b0 < nbs; b0 += 32 * kU) {
+          double x0[kU], x1[kU];
+#pragma unroll
+          for (int k = 0; k < kU; k++) {
+            const int b = b0 + 32 * k;
+            x0[k] = b < nbs ? part[2 * ((size_t)t * nbs + b)] : 0.0;
+            x1[k] = b < nbs ? part[2 * ((size_t)t * nbs + b) + 1] : 0.0;
+          }
+#pragma unroll
+          for (int k = 0; k < kU; k++) {
+            a0 += x0[k];
+            a1 += x1[k];
+          }
         }
       }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_down_sync(0xffffffffu, a0, o);
+        a1 += __shfl_down_sync(0xffffffffu, a1, o);
+      }
+      if (lane != 0) return;
       switch (op) {
         case C_SUMS: {
           S.insum = a0;

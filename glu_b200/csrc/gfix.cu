@@ -973,8 +973,8 @@ class Engine {
 
   void cscalar(int op) {
     const int T = c.L[3];
-    k_cscalar<<<(T + 127) / 128, 128, 0, s>>>(d_cst, d_sl, d_part, nbs, c.L[2],
-                                              c.L[2] * T, op, (double)Lcu, d_st);
+    k_cscalar<<<(T + kCScalarSlices - 1) / kCScalarSlices, 32 * kCScalarSlices, 0, s>>>(
+        d_cst, d_sl, d_part, nbs, c.L[2], c.L[2] * T, op, (double)Lcu, d_st);
     LAUNCHED(1);
   }
 

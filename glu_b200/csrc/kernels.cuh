@@ -446,9 +446,24 @@ __global__ void __launch_bounds__(kScalarThreads)
   const int nb = st->nblocks;
   double a[2] = {0.0, 0.0};
   if (op != OP_END_CG && op != OP_END_SD && op != OP_ALPHA_FIXED) {
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
-      a[0] += part[(size_t)nv * i];
-      if (nv > 1) a[1] += part[(size_t)nv * i + 1];
+    // eight independent loads in flight per thread and round, then added
+    // in a fixed order: the sum is deterministic and pays the L2 latency
+    // once per eight partials instead of once per partial
+    constexpr int kU = 8;
+    const int B = blockDim.x;
+    for (int i0 = threadIdx.x; i0 < nb; i0 += kU * B) {
+      double x0[kU], x1[kU];
+#pragma unroll
+      for (int k = 0; k < kU; k++) {
+        const int i = i0 + k * B;
+        x0[k] = i < nb ? part[(size_t)nv * i] : 0.0;
+        x1[k] = (nv > 1 && i < nb) ? part[(size_t)nv * i + 1] : 0.0;
+      }
+#pragma unroll
+      for (int k = 0; k < kU; k++) {
+        a[0] += x0[k];
+        a[1] += x1[k];
+      }
     }
     __shared__ double tot[2];
     block_sum_store<2>(a, tot);
