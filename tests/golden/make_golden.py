@@ -46,6 +46,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 from oracle.oracle import REF_BIN, Reference  # noqa: E402
 
+# the reference's source tree: an overridable default (GLU_REFERENCE)
 REF = Path(os.environ.get("GLU_REFERENCE", "/root/reference"))
 OUT = Path(__file__).resolve().parent
 ENVELOPE_ITERS = 60
