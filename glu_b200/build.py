@@ -20,7 +20,7 @@ LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libglu_gfix.so"
 SOURCES = ["gfix.cu", "glu_abi.cu", "noalloc.cu", "nersc.cu", "cuts.cu", "update.cu"]
 HEADERS = ["su3.cuh", "fft.cuh", "fft_pass.cuh", "fft_ct.cuh", "kernels.cuh", "extra_kernels.cuh",
-           "coulomb.cuh", "glu_compat.h", "su3_log.cuh"]
+           "coulomb.cuh", "glu_compat.h", "su3_log.cuh", "drop_in.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

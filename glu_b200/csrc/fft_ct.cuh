@@ -64,14 +64,14 @@ __global__ void __launch_bounds__(ct_threads(LX *LY), ct_minb(LX *LY))
 // z(,t) pass with compile-time extents (see k_fft_zt).  NT = Lt for Landau
 // (z and t transformed); NT = 1 for Coulomb (z only, one slice per tile).
 template <typename R, int LZ, int NT, int B>
-__global__ void __launch_bounds__(ct_threads(B *LZ *NT), ct_minb(B *LZ *NT))
+__global__ void __launch_bounds__(zt_threads<R>(B *LZ *NT), zt_minb<R>(B *LZ *NT))
     k_fft_zt_ct(Ctx<R> c) {
   if (c.st->done) return;
   if constexpr (NT == 1)
     if (c.skip && c.skip[blockIdx.x / ((c.L[0] / B) * c.L[1])]) return;
   constexpr bool FOUR = NT > 1;
   constexpr int TS = FOUR ? LZ * B + zt_pad(B) : LZ * B;  // padded t-stride
-  constexpr int N = B * LZ * NT, BD = ct_threads(N);
+  constexpr int N = B * LZ * NT, BD = zt_threads<R>(N);
   constexpr int EPT = (N + BD - 1) / BD;
   extern __shared__ unsigned char smem_raw[];
   cx<R> *A = reinterpret_cast<cx<R> *>(smem_raw);

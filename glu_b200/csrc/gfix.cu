@@ -25,6 +25,7 @@
 
 #include "../../include/glu_gfix.h"
 #include "coulomb.cuh"
+#include "drop_in.h"
 #include "extra_kernels.cuh"
 #include "kernels.cuh"
 
@@ -374,7 +375,7 @@ class Engine {
       ZtFn<F> fn = odd ? nullptr : ct_zt<F>(c.L[2], nt, b);
       if (!fn || zt_smem(b) > 200u * 1024u) return -1;
       zt_ct = fn;
-      bd_zt = ct_threads((int)n);
+      bd_zt = zt_threads<F>((int)n);
       CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)zt_smem(b)));
       CK(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -1912,6 +1913,47 @@ static int check_params(const size_t *dims, const gfix_params *p) {
 
 }  // extern "C"
 
+namespace gfix {
+
+int cuda_failure(const char *what, cudaError_t e) {
+  return fail("%s: %s", what, cudaGetErrorString(e));
+}
+
+static thread_local PhaseMark t_mark = nullptr;
+static thread_local void *t_mark_ctx = nullptr;
+void set_phase_mark(PhaseMark fn, void *ctx) {
+  t_mark = fn;
+  t_mark_ctx = ctx;
+}
+// the phase's work complete on s, then the caller's mark
+static int mark(cudaStream_t s, const char *phase) {
+  if (!t_mark) return 0;
+  CK(cudaStreamSynchronize(s));
+  t_mark(t_mark_ctx, phase);
+  return 0;
+}
+
+}  // namespace gfix
+
+namespace {
+// the links of the flat entry points: one contiguous host array
+struct HostArray final : gfix::LinkIO {
+  double *links;
+  explicit HostArray(double *l) : links(l) {}
+  int to_device(double *d_aos, size_t V, cudaStream_t s) override {
+    CK(cudaMemcpyAsync(d_aos, links, V * 36 * sizeof(double2),
+                       cudaMemcpyHostToDevice, s));
+    return 0;
+  }
+  int to_host(const double *d_aos, size_t V, cudaStream_t s) override {
+    CK(cudaMemcpyAsync(links, d_aos, V * 36 * sizeof(double2),
+                       cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return 0;
+  }
+};
+}  // namespace
+
 // The engine that stages a Landau solve's links and runs its FP64-link
 // phase: FP64 fields under GFIX_FP64, FP32 fields under GFIX_MIXED (whose
 // FP32 phase runs on a further, all-FP32 engine)
@@ -1931,14 +1973,8 @@ int gfix_landau(double *links, const size_t dims[4], const gfix_params *p,
                 gfix_result *r) {
   if (check_params(dims, p)) return -1;
   if (!links) return fail("null links");
-  return with_landau_engine(dims, p->precision, [&](auto *e) -> int {
-    const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
-    CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
-    if (landau_staged(e, p, r)) return -1;
-    CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
-    CK(cudaStreamSynchronize(e->s));
-    return 0;
-  });
+  HostArray io(links);
+  return gfix::landau_io(io, dims, p, r);
 }
 
 int gfix_landau_device(double *d_links, const size_t dims[4],
@@ -2283,72 +2319,26 @@ int gfix_coulomb(double *links, const size_t dims[4], const gfix_params *p,
                  gfix_result *r, double *slice_theta, size_t *slice_iters) {
   if (check_params(dims, p)) return -1;
   if (!links) return fail("null links");
-  Engine<double> *e = engine_coul(dims);
-  if (!e) return -1;
-  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
-  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
-  if (coulomb_staged(e, p, r, slice_theta, slice_iters)) return -1;
-  CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
-  CK(cudaStreamSynchronize(e->s));
-  return 0;
+  HostArray io(links);
+  return gfix::coulomb_io(io, dims, p, r, slice_theta, slice_iters);
 }
 
-// GLU's Landau driver in one device-resident sequence: the solve with its
-// random restarts, then -- when it converged -- output_fixing_info's
-// reunitarisation and diagnostics, all on the links in HBM, so the links
-// cross PCIe once each way.
+// (the host-array forms of gfix::landau_driver_io and coulomb_driver_io)
 int gfix_landau_driver(double *links, const size_t dims[4], const gfix_params *p,
                        gfix_result *r, double *obs, double *diag) {
   if (check_params(dims, p)) return -1;
   if (!links) return fail("null links");
-  return with_landau_engine(dims, p->precision, [&](auto *e) -> int {
-    const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
-    CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
-    gfix_result res;
-    if (landau_staged(e, p, &res)) return -1;
-    if (res.iters != kSentinel && res.iters != kGluFailure) {
-      if (reunit_resident(e)) return -1;
-      if (obs && observables_resident(e, obs)) return -1;
-      if (diag && diagnostics_resident(e, diag)) return -1;
-      if (e->to_aos(e->d_aos)) return -1;
-    } else {
-      if (obs) memset(obs, 0, 3 * sizeof(double));
-      if (diag) memset(diag, 0, 6 * sizeof(double));
-    }
-    CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
-    CK(cudaStreamSynchronize(e->s));
-    if (r) *r = res;
-    return 0;
-  });
+  HostArray io(links);
+  return gfix::landau_driver_io(io, dims, p, r, obs, diag);
 }
 
-// GLU's Coulomb driver in one device-resident sequence: the diagnostics of
-// the input, the solve of every slice with the slice transforms, the final
-// reunitarisation and the diagnostics of the result.
 int gfix_coulomb_driver(double *links, const size_t dims[4], const gfix_params *p,
                         gfix_result *r, double *obs_in, double *diag_in,
                         double *obs, double *diag) {
   if (check_params(dims, p)) return -1;
   if (!links) return fail("null links");
-  Engine<double> *e = engine_coul(dims);
-  if (!e) return -1;
-  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
-  CK(cudaMemcpyAsync(e->d_aos, links, bytes, cudaMemcpyHostToDevice, e->s));
-  if (obs_in || diag_in) {
-    if (e->from_aos(e->d_aos)) return -1;
-    if (obs_in && observables_resident(e, obs_in)) return -1;
-    if (diag_in && diagnostics_resident(e, diag_in)) return -1;
-  }
-  gfix_result res;
-  if (coulomb_staged(e, p, &res, nullptr, nullptr)) return -1;
-  if (reunit_resident(e)) return -1;
-  if (obs && observables_resident(e, obs)) return -1;
-  if (diag && diagnostics_resident(e, diag)) return -1;
-  if (e->to_aos(e->d_aos)) return -1;
-  CK(cudaMemcpyAsync(links, e->d_aos, bytes, cudaMemcpyDeviceToHost, e->s));
-  CK(cudaStreamSynchronize(e->s));
-  if (r) *r = res;
-  return 0;
+  HostArray io(links);
+  return gfix::coulomb_driver_io(io, dims, p, r, obs_in, diag_in, obs, diag);
 }
 
 int gfix_profile_coulomb(const double *d_links, const size_t dims[4],
@@ -2495,3 +2485,95 @@ int gfix_batch_result(const gfix_batch *b, int i, gfix_result *r) {
 void gfix_batch_destroy(gfix_batch *b) { delete b; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------
+// the solves with the links moved by a LinkIO (the flat host entry points
+// above, and GLU's own entry points)
+
+namespace gfix {
+
+int landau_io(LinkIO &io, const size_t dims[4], const gfix_params *p,
+              gfix_result *r) {
+  if (check_params(dims, p)) return -1;
+  return with_landau_engine(dims, p->precision, [&](auto *e) -> int {
+    // (a mixed solve's FP32 engine is made here too, not inside the solve)
+    if (p->precision == GFIX_MIXED && !engine32(dims)) return -1;
+    if (mark(e->s, "engine") || io.to_device(e->d_aos, e->V, e->s) ||
+        mark(e->s, "to device"))
+      return -1;
+    if (landau_staged(e, p, r) || mark(e->s, "solve")) return -1;
+    return (io.to_host(e->d_aos, e->V, e->s) || mark(e->s, "to host")) ? -1 : 0;
+  });
+}
+
+// GLU's Landau driver in one device-resident sequence: the solve with its
+// random restarts, then -- when it converged -- output_fixing_info's
+// reunitarisation and diagnostics, all on the links in HBM, so the links
+// cross PCIe once each way.
+int landau_driver_io(LinkIO &io, const size_t dims[4], const gfix_params *p,
+                     gfix_result *r, double *obs, double *diag) {
+  if (check_params(dims, p)) return -1;
+  return with_landau_engine(dims, p->precision, [&](auto *e) -> int {
+    if (p->precision == GFIX_MIXED && !engine32(dims)) return -1;
+    if (mark(e->s, "engine") || io.to_device(e->d_aos, e->V, e->s) ||
+        mark(e->s, "to device"))
+      return -1;
+    gfix_result res;
+    if (landau_staged(e, p, &res) || mark(e->s, "solve")) return -1;
+    if (res.iters != kSentinel && res.iters != kGluFailure) {
+      if (reunit_resident(e)) return -1;
+      if (obs && observables_resident(e, obs)) return -1;
+      if (diag && diagnostics_resident(e, diag)) return -1;
+      if (e->to_aos(e->d_aos)) return -1;
+    } else {
+      if (obs) memset(obs, 0, 3 * sizeof(double));
+      if (diag) memset(diag, 0, 6 * sizeof(double));
+    }
+    if (mark(e->s, "post") || io.to_host(e->d_aos, e->V, e->s) ||
+        mark(e->s, "to host"))
+      return -1;
+    if (r) *r = res;
+    return 0;
+  });
+}
+
+int coulomb_io(LinkIO &io, const size_t dims[4], const gfix_params *p,
+               gfix_result *r, double *slice_theta, size_t *slice_iters) {
+  if (check_params(dims, p)) return -1;
+  Engine<double> *e = engine_coul(dims);
+  if (!e || mark(e->s, "engine") || io.to_device(e->d_aos, e->V, e->s) ||
+      mark(e->s, "to device"))
+    return -1;
+  if (coulomb_staged(e, p, r, slice_theta, slice_iters) || mark(e->s, "solve"))
+    return -1;
+  return (io.to_host(e->d_aos, e->V, e->s) || mark(e->s, "to host")) ? -1 : 0;
+}
+
+// GLU's Coulomb driver in one device-resident sequence: the diagnostics of
+// the input, the solve of every slice with the slice transforms, the final
+// reunitarisation and the diagnostics of the result.
+int coulomb_driver_io(LinkIO &io, const size_t dims[4], const gfix_params *p,
+                      gfix_result *r, double *obs_in, double *diag_in,
+                      double *obs, double *diag) {
+  if (check_params(dims, p)) return -1;
+  Engine<double> *e = engine_coul(dims);
+  if (!e || mark(e->s, "engine") || io.to_device(e->d_aos, e->V, e->s) ||
+      mark(e->s, "to device"))
+    return -1;
+  if (obs_in || diag_in) {
+    if (e->from_aos(e->d_aos)) return -1;
+    if (obs_in && observables_resident(e, obs_in)) return -1;
+    if (diag_in && diagnostics_resident(e, diag_in)) return -1;
+  }
+  gfix_result res;
+  if (coulomb_staged(e, p, &res, nullptr, nullptr) || mark(e->s, "solve")) return -1;
+  if (reunit_resident(e)) return -1;
+  if (obs && observables_resident(e, obs)) return -1;
+  if (diag && diagnostics_resident(e, diag)) return -1;
+  if (e->to_aos(e->d_aos) || mark(e->s, "post")) return -1;
+  if (io.to_host(e->d_aos, e->V, e->s) || mark(e->s, "to host")) return -1;
+  if (r) *r = res;
+  return 0;
+}
+
+}  // namespace gfix

@@ -2,23 +2,28 @@
 //
 // The caller is GLU (or a program built like it): `lat` is GLU's AoS
 // lattice, the lattice shape and GF_TUNE are read from GLU's global Latt.
-// Each call gathers the links into one contiguous buffer, runs the GPU
-// solve, scatters them back, and follows GLU's return conventions.
+// Each solve gathers the links chunk by chunk into pinned memory on their
+// way to the device, runs the GPU solve, scatters them back the same way,
+// and follows GLU's return conventions.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 #include <omp.h>
 
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
+#include <chrono>
+#include <condition_variable>
 #include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <thread>
 #include <vector>
 
 #include "../../include/glu_gfix.h"
+#include "drop_in.h"
 #include "glu_compat.h"
-
-namespace gfix {
-void set_restart_log(bool on);  // gfix.cu: print GLU's restart messages
-}
 
 using gfix::glu_fftw_stuff;
 using gfix::glu_latt_info;
@@ -81,47 +86,197 @@ void scatter(glu_site *lat, const double *buf, size_t V) {
       memcpy(lat[i].O[mu], buf + ((size_t)i * 4 + mu) * 18, 18 * sizeof(double));
 }
 
-// One pinned staging buffer for the whole process, grown on demand: GLU
-// calls these entry points once per configuration with the same lattice,
-// and a fresh cudaMallocHost of the link payload per call costs more than
-// the copies themselves.  Freed at exit.
-struct Staging {
-  double *p = nullptr;
-  size_t n = 0;
-  ~Staging() {
-    if (p) cudaFreeHost(p);
-  }
-  double *get(size_t need) {
-    if (need <= n) return p;
-    if (p) cudaFreeHost(p);
-    p = nullptr;
-    n = 0;
-    if (cudaMallocHost(&p, need * sizeof(double)) != cudaSuccess) {
-      p = nullptr;
-      return nullptr;
+// --- GLU's site lattice to and from the device ---------------------------
+
+constexpr size_t kSiteDoubles = 72;       // 4 links x 9 complex numbers
+constexpr size_t kChunkSites = 1u << 16;  // 36 MB of links per chunk
+constexpr int kSlots = 3;
+
+// A ring of pinned chunks for the whole process: the gather of chunk k+1
+// from GLU's per-link allocations overlaps the copy of chunk k to the
+// device, and the scatter of chunk k the copy of chunk k+1 back, so no
+// pinned buffer of a whole lattice (1.2 GB at 32^3x64, which takes 0.5-0.9 s
+// to pin) is made.  Left to the process's exit, like the engines.
+struct Ring {
+  std::mutex m;  // one transfer at a time
+  double *slot[kSlots] = {};
+  cudaEvent_t done[kSlots] = {};
+  bool ready = false;
+  int init() {
+    std::lock_guard<std::mutex> lk(m);
+    if (ready) return 0;
+    for (int i = 0; i < kSlots; i++) {
+      cudaError_t e = cudaSuccess;
+      if (!slot[i])
+        e = cudaMallocHost(&slot[i], kChunkSites * kSiteDoubles * sizeof(double));
+      if (e == cudaSuccess && !done[i])
+        e = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
+      if (e != cudaSuccess) return gfix::cuda_failure("pinned staging chunks", e);
     }
-    n = need;
-    return p;
+    ready = true;
+    return 0;
   }
 };
-Staging g_stage;
 
-struct Buf {
-  double *p;
-  explicit Buf(size_t n) : p(g_stage.get(n)) {}
+Ring &ring() {
+  static Ring *r = new Ring;  // never destroyed: see Warmup
+  return *r;
+}
+
+// lat[i].O[mu] (separate 144-byte allocations) <-> chunks of double[n][4][18]
+struct SiteLinks final : gfix::LinkIO {
+  glu_site *lat;
+  explicit SiteLinks(glu_site *l) : lat(l) {}
+  int to_device(double *d_aos, size_t V, cudaStream_t s) override {
+    Ring &R = ring();
+    std::lock_guard<std::mutex> lk(R.m);
+    for (size_t i0 = 0, k = 0; i0 < V; i0 += kChunkSites, k++) {
+      const int j = (int)(k % kSlots);
+      const size_t n = std::min(kChunkSites, V - i0);
+      // the slot's previous copy has left it
+      cudaError_t e = cudaEventSynchronize(R.done[j]);
+      if (e != cudaSuccess) return gfix::cuda_failure("staging copy", e);
+      gather(lat + i0, R.slot[j], n);
+      e = cudaMemcpyAsync(d_aos + i0 * kSiteDoubles, R.slot[j],
+                          n * kSiteDoubles * sizeof(double), cudaMemcpyHostToDevice, s);
+      if (e == cudaSuccess) e = cudaEventRecord(R.done[j], s);
+      if (e != cudaSuccess) return gfix::cuda_failure("staging copy", e);
+    }
+    return 0;
+  }
+  int to_host(const double *d_aos, size_t V, cudaStream_t s) override {
+    Ring &R = ring();
+    std::lock_guard<std::mutex> lk(R.m);
+    const size_t nch = (V + kChunkSites - 1) / kChunkSites;
+    auto issue = [&](size_t k) {
+      const int j = (int)(k % kSlots);
+      const size_t i0 = k * kChunkSites, n = std::min(kChunkSites, V - i0);
+      cudaError_t e = cudaMemcpyAsync(R.slot[j], d_aos + i0 * kSiteDoubles,
+                                      n * kSiteDoubles * sizeof(double),
+                                      cudaMemcpyDeviceToHost, s);
+      return e == cudaSuccess ? cudaEventRecord(R.done[j], s) : e;
+    };
+    for (size_t k = 0; k < nch && k < (size_t)kSlots; k++)
+      if (cudaError_t e = issue(k)) return gfix::cuda_failure("return copy", e);
+    for (size_t k = 0; k < nch; k++) {
+      const int j = (int)(k % kSlots);
+      const size_t i0 = k * kChunkSites;
+      if (cudaError_t e = cudaEventSynchronize(R.done[j]))
+        return gfix::cuda_failure("return copy", e);
+      scatter(lat + i0, R.slot[j], std::min(kChunkSites, V - i0));
+      if (k + kSlots < nch)
+        if (cudaError_t e = issue(k + kSlots)) return gfix::cuda_failure("return copy", e);
+    }
+    return 0;
+  }
+};
+
+// Inside a GLU program the device context is created, and the ring
+// allocated, on a thread started when the library is loaded, while the
+// program reads its configuration (the context alone takes 1.3-1.9 s to
+// create on a B200); every entry point waits for that thread before its
+// own first CUDA call.  The program's CUDA modules -- this library's -- are
+// loaded with the context (CUDA_MODULE_LOADING=EAGER unless the
+// environment sets it), not at each kernel's first launch inside the
+// call: at 32^3x64 Landau() then took 0.85 s (FP64) and 0.58 s (mixed)
+// inside GLU's program, against 0.79 and 0.53 s for the flat driver on
+// links already in pinned memory with its workspaces warm.  A program
+// is GLU's when its own definition of Latt overrides the library's weak
+// one.  GLU_GFIX_PREINIT=0 turns all this off.  The thread is detached and
+// its state never destroyed, so that a program which exits without
+// calling in does not wait for it.
+struct Warmup {
+  std::mutex m;
+  std::condition_variable cv;
+  bool running = false;
+  void start() {
+    running = true;
+    std::thread([this] {
+      if (cudaFree(nullptr) == cudaSuccess) ring().init();
+      cudaGetLastError();  // a failure is met again, and reported, by the call
+      std::lock_guard<std::mutex> lk(m);
+      running = false;
+      cv.notify_all();
+    }).detach();
+  }
+  void wait() {
+    std::unique_lock<std::mutex> lk(m);
+    cv.wait(lk, [this] { return !running; });
+  }
+};
+
+Warmup &warmup() {
+  static Warmup *w = new Warmup;
+  return *w;
+}
+
+bool in_glu_program() {
+  Dl_info latt{}, self{};
+  if (!dladdr((const void *)&Latt, &latt) || !dladdr((const void *)&in_glu_program, &self))
+    return false;
+  return latt.dli_fbase != self.dli_fbase;
+}
+
+__attribute__((constructor)) void preinit_in_glu_program() {
+  const char *s = getenv("GLU_GFIX_PREINIT");
+  if ((s && atoi(s) == 0) || !in_glu_program()) return;
+  setenv("CUDA_MODULE_LOADING", "EAGER", 0);  // before the runtime starts
+  warmup().start();
+}
+
+// the device, then the ring; 0, or -1 with the reason printed under tag
+int ready_to_stage(const char *tag) {
+  warmup().wait();
+  if (ring().init() == 0) return 0;
+  fprintf(stderr, "[%s] allocation of the GPU staging chunks failed: %s\n", tag,
+          gfix_last_error());
+  return -1;
+}
+
+// GLU_GFIX_TIMING=1: one line per GLU-named solve with the wall time of
+// each of its phases -- waiting for the device, the staging chunks, the
+// workspaces ("engine"), the links' way to the device with their gather,
+// the solve, the reunitarisation and diagnostics ("post"), the way back
+// with the scatter -- for a program whose own timer covers the whole call
+struct Phases {
+  bool on = false;
+  double last = 0.0;
+  char line[320] = {0};
+  size_t len = 0;
+  static double now() {
+    return std::chrono::duration<double>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+  }
+  static void mark_cb(void *self, const char *phase) {
+    static_cast<Phases *>(self)->mark(phase);
+  }
+  Phases() {
+    const char *s = getenv("GLU_GFIX_TIMING");
+    on = s && atoi(s) != 0;
+    last = now();
+    if (on) gfix::set_phase_mark(mark_cb, this);
+  }
+  ~Phases() {
+    if (on) gfix::set_phase_mark(nullptr, nullptr);
+  }
+  void mark(const char *name) {
+    if (!on) return;
+    const double t = now();
+    if (len < sizeof line)
+      len += snprintf(line + len, sizeof line - len, " || %s %.3e s", name, t - last);
+    last = t;
+  }
+  void print() const {
+    if (on) printf("[GF] GPU timing%s\n", line);
+  }
 };
 
 size_t landau_fa(glu_site *lat, double *th, double acc, size_t max_iters,
                  int algo) {
   size_t d[4];
   dims_of(d);
-  const size_t V = volume();
-  Buf buf(V * 72);
-  if (!buf.p) {
-    fprintf(stderr, "[FACG] allocation of temporaries failed\n");
-    return 0;
-  }
-  gather(lat, buf.p, V);
+  if (ready_to_stage("FACG")) return 0;
   gfix_params p;
   memset(&p, 0, sizeof p);
   p.gf_alpha = Latt.gf_alpha;
@@ -133,11 +288,11 @@ size_t landau_fa(glu_site *lat, double *th, double acc, size_t max_iters,
 #endif
   env_precision(&p);
   gfix_result r;
-  if (gfix_landau(buf.p, d, &p, &r) != 0) {
+  SiteLinks io(lat);
+  if (gfix::landau_io(io, d, &p, &r) != 0) {
     fprintf(stderr, "[GF] GPU gauge fixing failed: %s\n", gfix_last_error());
     return 0;
   }
-  scatter(lat, buf.p, V);
   *th = r.theta;
   return r.iters;
 }
@@ -168,6 +323,7 @@ void FOURIER_ACCELERATE3(struct fftw_stuff *FFTW) {
   std::vector<double> f(V * 8);
   for (int k = 0; k < 4; k++)
     memcpy(f.data() + (size_t)k * V * 2, F->in[k], V * 2 * sizeof(double));
+  warmup().wait();
   if (gfix_fourier_accelerate(f.data(), d, 4) != 0) {
     fprintf(stderr, "[GF] GPU Fourier acceleration failed: %s\n",
             gfix_last_error());
@@ -183,13 +339,11 @@ size_t Landau(struct site *lat, const double accuracy, const size_t iter,
   glu_site *L = reinterpret_cast<glu_site *>(lat);
   size_t d[4];
   dims_of(d);
-  const size_t V = volume();
-  Buf buf(V * 72);
-  if (!buf.p) {
-    fprintf(stderr, "[GF] allocation of the GPU staging buffer failed\n");
-    return kGluFailure;
-  }
-  gather(L, buf.p, V);
+  Phases ph;
+  warmup().wait();
+  ph.mark("device");
+  if (ready_to_stage("GF")) return kGluFailure;
+  ph.mark("chunks");
   gfix_params p;
   memset(&p, 0, sizeof p);
   p.gf_alpha = Latt.gf_alpha;
@@ -208,15 +362,16 @@ size_t Landau(struct site *lat, const double accuracy, const size_t iter,
   env_luxury(&p);
   gfix_result r;
   double obs[3] = {0, 0, 0}, dg[6] = {0, 0, 0, 0, 0, 0};
+  SiteLinks io(L);
   gfix::set_restart_log(true);
-  const int rc = gfix_landau_driver(buf.p, d, &p, &r, obs, dg);
+  // the links of the last attempt go back to the caller either way
+  const int rc = gfix::landau_driver_io(io, d, &p, &r, obs, dg);
   gfix::set_restart_log(false);
   if (rc != 0) {
     fprintf(stderr, "[GF] GPU gauge fixing failed: %s\n", gfix_last_error());
     return kGluFailure;
   }
-  // the links of the last attempt go back to the caller either way
-  scatter(L, buf.p, V);
+  ph.print();
   if (r.iters == kGluFailure) {
     printf("\n[GF] Failure to converge to a sufficient solution \n"
            "[GF] Please lower the GF_TUNE parameter from %g \n",
@@ -242,13 +397,7 @@ size_t Coulomb_FA(struct site *lat, struct fftw_stuff *FFTW,
   glu_site *L = reinterpret_cast<glu_site *>(lat);
   size_t d[4];
   dims_of(d);
-  const size_t V = volume();
-  Buf buf(V * 72);
-  if (!buf.p) {
-    fprintf(stderr, "[CG] allocation of the GPU staging buffer failed\n");
-    return 0;
-  }
-  gather(L, buf.p, V);
+  if (ready_to_stage("CG")) return 0;
   gfix_params p;
   memset(&p, 0, sizeof p);
   p.gf_alpha = Latt.gf_alpha;
@@ -260,12 +409,12 @@ size_t Coulomb_FA(struct site *lat, struct fftw_stuff *FFTW,
 #endif
   env_precision(&p);
   gfix_result r;
-  if (gfix_coulomb(buf.p, d, &p, &r, nullptr, nullptr) != 0) {
+  SiteLinks io(L);
+  if (gfix::coulomb_io(io, d, &p, &r, nullptr, nullptr) != 0) {
     fprintf(stderr, "[CG] GPU Coulomb gauge fixing failed: %s\n",
             gfix_last_error());
     return 0;
   }
-  scatter(L, buf.p, V);
   return r.iters;
 }
 
@@ -273,13 +422,11 @@ size_t Coulomb(struct site *lat, const double accuracy, const size_t iter) {
   glu_site *L = reinterpret_cast<glu_site *>(lat);
   size_t d[4];
   dims_of(d);
-  const size_t V = volume();
-  Buf buf(V * 72);
-  if (!buf.p) {
-    fprintf(stderr, "[CG] allocation of the GPU staging buffer failed\n");
-    return 0;
-  }
-  gather(L, buf.p, V);
+  Phases ph;
+  warmup().wait();
+  ph.mark("device");
+  if (ready_to_stage("CG")) return 0;
+  ph.mark("chunks");
   gfix_params p;
   memset(&p, 0, sizeof p);
   p.gf_alpha = Latt.gf_alpha;
@@ -298,14 +445,15 @@ size_t Coulomb(struct site *lat, const double accuracy, const size_t iter) {
   gfix_result r;
   double obs0[3] = {0, 0, 0}, dg0[6] = {0, 0, 0, 0, 0, 0};
   double obs[3] = {0, 0, 0}, dg[6] = {0, 0, 0, 0, 0, 0};
-  if (gfix_coulomb_driver(buf.p, d, &p, &r, obs0, dg0, obs, dg) != 0) {
+  SiteLinks io(L);
+  if (gfix::coulomb_driver_io(io, d, &p, &r, obs0, dg0, obs, dg) != 0) {
     fprintf(stderr, "[CG] GPU Coulomb gauge fixing failed: %s\n",
             gfix_last_error());
     return 0;
   }
+  ph.print();
   printf("[GF] Initial Tlink :: %1.15f || Slink :: %1.15f \n"
          "[GF] Plaquette :: %1.15f \n", dg0[1], dg0[0], obs0[2]);
-  scatter(L, buf.p, V);
   printf("[GF] Tuning :: %f || Iterations :: %zu ||\n[GF] Final Tlink :: %1.15f "
          "|| Slink :: %1.15f \n[GF] Plaquette :: %1.15f \n",
          Latt.gf_alpha, r.iters, dg[1], dg[0], obs[2]);
@@ -321,6 +469,7 @@ void FOURIER_ACCELERATE2(struct fftw_stuff *FFTW) {
   std::vector<double> f(lcu * 8);
   for (int k = 0; k < 4; k++)
     memcpy(f.data() + (size_t)k * lcu * 2, F->in[k], lcu * 2 * sizeof(double));
+  warmup().wait();
   if (gfix_fourier_accelerate(f.data(), d, 3) != 0) {
     fprintf(stderr, "[GF] GPU Fourier acceleration failed: %s\n",
             gfix_last_error());
@@ -351,15 +500,16 @@ int cuts_struct(struct site *lat, const struct cut_info CUTINFO) {
   ci.definition = CUTINFO.definition;
   ci.angle = CUTINFO.angle;
   ci.cyl_width = CUTINFO.cyl_width;
-  Buf buf(V * 72);
-  if (!buf.p) {
+  std::unique_ptr<double[]> buf(new (std::nothrow) double[V * kSiteDoubles]);
+  if (!buf) {
     fprintf(stderr, "[CUTS] allocation of temporaries failed\n");
     return -1;
   }
-  gather(A, buf.p, V);
+  gather(A, buf.get(), V);
+  warmup().wait();
   double err = 0.0;
   char path[1024];
-  if (gfix_cuts_write(buf.p, d, &ci, "./", Latt.flow, &err, path, sizeof path) != 0) {
+  if (gfix_cuts_write(buf.get(), d, &ci, "./", Latt.flow, &err, path, sizeof path) != 0) {
     fprintf(stderr, "[CUTS] %s\n", gfix_cuts_error());
     return -1;
   }

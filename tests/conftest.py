@@ -53,3 +53,12 @@ def lat400():
 @pytest.fixture(scope="session")
 def hb8():
     return dict(np.load(GOLDEN / "hb8.npz"))
+
+
+@pytest.fixture(scope="session")
+def headline_config():
+    """The first configuration of the 32^3x64 Landau benchmark (GPU tests
+    only): beta 6.0, 1000 heatbath + 4 over-relaxation iterations from the
+    unit start, seed 2, generated on the GPU."""
+    from glu_b200.workload import heatbath_config
+    return heatbath_config((32, 32, 32, 64), seed=2, iterations=1000, beta=6.0, n_or=4)

@@ -52,14 +52,6 @@ def test_fourier_accelerate2_at_benchmark_slices(oracle, dims):
     assert np.abs(got - ref).max() < 1e-13 * np.abs(ref).max()
 
 
-@pytest.fixture(scope="module")
-def headline_config():
-    """The first configuration of the headline benchmark: beta 6.0, 1000
-    heatbath + 4 over-relaxation iterations from the unit start, seed 2."""
-    from glu_b200.workload import heatbath_config
-    return heatbath_config(HEADLINE, seed=2, iterations=1000, beta=6.0, n_or=4)
-
-
 def test_headline_links_match_oracle_after_two_iterations(oracle, headline_config):
     """Links after exactly two FACG iterations (SD start, then CG) at the
     headline shape, against the oracle, at the same iteration count."""

@@ -10,6 +10,7 @@ import ctypes as C
 import os
 import re
 import subprocess
+import time
 from pathlib import Path
 
 import numpy as np
@@ -164,6 +165,50 @@ def test_coulomb_entry_points_on_a_site_lattice(lib, lat400, capfd):
     assert f"Iterations :: {it2} ||" in out
 
 
+@pytest.fixture(scope="module")
+def hb24x16():
+    """A 24^3x16 heatbath configuration: 221184 sites, 3.4 staging chunks
+    of 65536 sites (every slot of the ring of three used, one reused, the
+    last chunk short)."""
+    from glu_b200.workload import heatbath_config
+    d = (24, 24, 24, 16)
+    return d, heatbath_config(d, seed=5, iterations=30, beta=6.0, n_or=4)
+
+
+def test_chunked_staging_of_a_large_site_lattice(lib, hb24x16, capfd):
+    """The links travel between lat[i].O[mu] and the device in chunks
+    through pinned buffers (gather of one chunk overlapping the copy of the
+    last): Landau, FACG, Coulomb_FA and Coulomb on a lattice of several
+    chunks return, bit for bit, what the flat entry points return for the
+    same contiguous links."""
+    d, U = hb24x16
+    set_latt(lib, d, gf_alpha=0.08, seed=3)
+    L = SiteLattice(U)
+    it = lib.Landau(L.sites, 1e-12, 3000, b"unused")
+    ref = gfix.landau_driver(U, d, 0.08, 1e-12, 3000, restart_seed=3)
+    assert it == ref.iters != GLU_FAILURE
+    assert np.array_equal(L.U, ref.links)
+    L = SiteLattice(U)
+    th = C.c_double(0.0)
+    it = lib.FACG(L.sites, None, C.byref(th), 1e-12, 3000)
+    flat = gfix.landau_fix(U, d, 0.08, 1e-12, 3000, "FACG")
+    assert it == flat.iters and th.value == flat.theta
+    assert np.array_equal(L.U, flat.links)
+    set_latt(lib, d, gf_alpha=0.09)
+    L = SiteLattice(U)
+    it = lib.Coulomb_FA(L.sites, None, 1e-12, 3000, 1)
+    flat = gfix.coulomb_fix(U, d, 0.09, 1e-12, 3000, "FACG")
+    assert it == flat.iters
+    assert np.array_equal(L.U, flat.links)
+    L = SiteLattice(U)
+    it = lib.Coulomb(L.sites, 1e-12, 3000)
+    _, fin = gfix.coulomb_driver(U, d, 0.09, 1e-12, 3000)
+    assert it == fin.iters
+    assert np.array_equal(L.U, fin.links)
+    flush_c_stdio()
+    capfd.readouterr()
+
+
 # --- GLU's own program, relinked ------------------------------------------
 
 INPUT = """MODE = GAUGE_FIXING
@@ -178,7 +223,7 @@ SEED = 0
 GFTYPE = {gftype}
 	GF_TUNE = {tune}
 	ACCURACY = 14
-	MAX_ITERS = 650
+	MAX_ITERS = {max_iters}
 CUTTYPE = GLUON_PROPS
 	FIELD_DEFINITION = LINEAR
 	MOM_CUT = CYLINDER_CUT
@@ -211,7 +256,7 @@ def _run(binary, tmp_path, gftype, tune, tag):
     d = (4, 4, 4, 8)
     inp = tmp_path / f"in_{gftype}"
     inp.write_text(INPUT.format(d0=d[0], d1=d[1], d2=d[2], d3=d[3], gftype=gftype,
-                                tune=tune))
+                                tune=tune, max_iters=650))
     out = tmp_path / f"{tag}_{gftype}.nersc"
     env = dict(os.environ, OMP_NUM_THREADS="4")
     p = subprocess.run([str(binary), "-i", str(inp), "-c", str(GOLDEN / "lat400.nersc"),
@@ -260,3 +305,68 @@ def test_relinked_glu_program_runs_the_gpu_path(reference, tmp_path, gftype, tun
     if gftype == "LANDAU":
         # GLU's own theta_test_lin on the GPU-fixed configuration
         assert reference.theta_test_lin() < 1e-13
+
+
+@pytest.mark.parametrize("precision", ["FP64", "MIXED"])
+def test_relinked_program_at_the_headline_shape(headline_config, tmp_path, precision):
+    """GLU's relinked program on the 32^3x64 benchmark configuration (the
+    links written as a NERSC 3x3 file, which GLU reads back exactly):
+    Landau() reports the iteration count, plaquette and functional of
+    gfix_landau_driver on the same links.  The wall time of the call --
+    GLU's own [TIMER] around Landau(), which covers whatever of the device
+    context's creation the configuration's read did not hide, the
+    workspaces, the gather and scatter of GLU's site lattice and the solve
+    -- is printed beside gfix_landau_driver's end-to-end time (pinned host
+    links, warm engine), with the phases of the call (GLU_GFIX_TIMING)."""
+    from glu_b200 import nersc
+    from glu_b200._lib import GfixParams, GfixResult, check
+    gpu = ROOT / "oracle" / "_ref" / "glu_gpu"
+    if not gpu.exists():
+        pytest.skip("oracle/_ref/glu_gpu not built")
+    d = (32, 32, 32, 64)
+    cfg = tmp_path / "hb.nersc"
+    nersc.write(cfg, headline_config, d, datatype="4D_SU3_GAUGE_3x3")
+    inp = tmp_path / "in"
+    inp.write_text(INPUT.format(d0=d[0], d1=d[1], d2=d[2], d3=d[3], gftype="LANDAU",
+                                tune=0.08, max_iters=4000))
+    env = dict(os.environ, GLU_GFIX_TIMING="1", GLU_GFIX_PRECISION=precision)
+    p = subprocess.run([str(gpu), "-i", str(inp), "-c", str(cfg)], cwd=tmp_path,
+                       env=env, capture_output=True, text=True, timeout=900)
+    assert p.returncode == 0, p.stderr[-2000:]
+    out = p.stdout
+    # [TIMER] lines: the read of the configuration, then Landau()
+    timers = [float(x) for x in re.findall(r"\[TIMER\] elapsed :: ([0-9.e+-]+) s", out)]
+    assert len(timers) >= 2
+    t_call = timers[1]
+    phases = re.search(r"\[GF\] GPU timing(.*)", out).group(1)
+    it = int(re.search(r"\[GF\] Iters :: (\d+)", out).group(1))
+    plaq = float(re.findall(r"\[GF\] Plaquette :: ([0-9.]+)", out)[-1])
+    func = float(re.search(r"\[GF\] Functional :: ([0-9.]+)", out).group(1))
+
+    # the same fix through the flat driver: pinned host links, warm engine
+    lib = _lib.load()
+    V = int(np.prod(d))
+    host = torch.from_numpy(headline_config.view(np.float64).reshape(-1)).pin_memory()
+    work = torch.empty_like(host).pin_memory()
+    cd = (C.c_size_t * 4)(*d)
+    prm = GfixParams()
+    prm.gf_alpha, prm.accuracy, prm.max_iters = 0.08, 1e-14, 4000
+    prm.precision = 1 if precision == "MIXED" else 0
+    prm.switch_theta = 1e-9
+    prm.max_restarts, prm.restart_seed = 6, 0
+    r = GfixResult()
+    obs, dg = np.zeros(3), np.zeros(6)
+    dp = C.POINTER(C.c_double)
+    times = []
+    for _ in range(3):
+        work.copy_(host)
+        t0 = time.perf_counter()
+        check(lib.gfix_landau_driver(work.data_ptr(), cd, C.byref(prm), C.byref(r),
+                                     obs.ctypes.data_as(dp), dg.ctypes.data_as(dp)))
+        times.append(time.perf_counter() - t0)
+    assert it == r.iters
+    assert abs(plaq - obs[2]) < 1e-13
+    assert abs(func - obs[1]) < 1e-12
+    print("\n[%s] Landau() in GLU's program %.3f s (%d iterations;%s); "
+          "gfix_landau_driver end to end %.3f s (best of %d after the first %.3f s)"
+          % (precision, t_call, it, phases, min(times[1:]), len(times) - 1, times[0]))
