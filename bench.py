@@ -256,7 +256,7 @@ def gpu_arm(args, dims, rank, world, local):
     Us = [workload(dims, rank, i) for i in range(E_CONFIGS)]
     U = Us[0]
     hosts = [torch.from_numpy(u.view(np.float64).reshape(-1)).pin_memory() for u in Us]
-    hwork = torch.empty_like(hosts[0]).pin_memory()
+    hworks = [torch.empty_like(h).pin_memory() for h in hosts]
     dpristine = [h.to("cuda") for h in hosts]
     dwork = torch.empty_like(dpristine[0])
     cd = (C.c_size_t * 4)(*dims)
@@ -272,11 +272,15 @@ def gpu_arm(args, dims, rank, world, local):
         check(lib.gfix_landau_device(dwork.data_ptr(), cd, C.byref(p), C.byref(r)))
         return r
 
-    def host_fix(prec):
-        r = GfixResult()
+    def host_fix_all(prec):
+        # the step's configurations through one gfix_landau_sequence call:
+        # host links in, fixed links back, each configuration's copies
+        # overlapping its neighbours' solves
+        rs = (GfixResult * E_CONFIGS)()
         p = _params(prec)
-        check(lib.gfix_landau(hwork.data_ptr(), cd, C.byref(p), C.byref(r)))
-        return r
+        ptrs = (C.c_void_p * E_CONFIGS)(*[h.data_ptr() for h in hworks])
+        check(lib.gfix_landau_sequence(ptrs, E_CONFIGS, cd, C.byref(p), rs))
+        return rs
 
     def plaquette(ptr, reunit=False):
         if reunit:
@@ -317,21 +321,26 @@ def gpu_arm(args, dims, rank, world, local):
             barrier()
             launches = lib.gfix_kernel_launches() - launches0
             ms = max_over_ranks(a.elapsed_time(b))
-            # end to end: pinned host buffers, H2D + D2H inside each fix
+            # end to end: pinned host buffers, every step's H2D + D2H of its
+            # configurations inside the timed call
             e_ms = 0.0
             drift = 0.0
             for k in range(args.steps):
                 for i in range(E_CONFIGS):
-                    hwork.copy_(hosts[i])
-                    barrier()
-                    a2, b2 = ev(), ev()
-                    a2.record()
-                    host_fix(prec)
-                    b2.record()
-                    torch.cuda.synchronize()
-                    e_ms += a2.elapsed_time(b2)
-                    if k == args.steps - 1:
-                        drift = max(drift, abs(plaquette(hwork.data_ptr(), True)
+                    hworks[i].copy_(hosts[i])
+                barrier()
+                a2, b2 = ev(), ev()
+                a2.record()
+                rs = host_fix_all(prec)
+                b2.record()
+                torch.cuda.synchronize()
+                e_ms += a2.elapsed_time(b2)
+                if [int(r.iters) for r in rs] != [x[0] for x in per]:
+                    raise RuntimeError(f"{prec}: the end-to-end fixes took other iteration "
+                                       f"counts than the device-resident ones")
+                if k == args.steps - 1:
+                    for i in range(E_CONFIGS):
+                        drift = max(drift, abs(plaquette(hworks[i].data_ptr(), True)
                                                - plaq_in[i]))
             e_ms = max_over_ranks(e_ms)
             if not drift < PLAQ_TOL:

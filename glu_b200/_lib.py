@@ -40,7 +40,7 @@ class GfixResult(C.Structure):
 # every symbol include/glu_gfix.h declares
 EXPORTS = ("FACG", "FASD", "FOURIER_ACCELERATE3", "Landau", "Coulomb",
            "Coulomb_FA", "FOURIER_ACCELERATE2", "cuts_struct", "gfix_landau",
-           "gfix_landau_device", "gfix_landau_driver", "gfix_coulomb",
+           "gfix_landau_sequence", "gfix_landau_device", "gfix_landau_driver", "gfix_coulomb",
            "gfix_coulomb_device", "gfix_coulomb_driver",
            "gfix_observables", "gfix_reunit", "gfix_fourier_accelerate",
            "gfix_profile_landau", "gfix_profile_coulomb",
@@ -85,6 +85,9 @@ def load(path: Path | str | None = None):
         getattr(lib, fn).restype = C.c_int
         getattr(lib, fn).argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
                                      C.POINTER(GfixResult), _dp, _szp]
+    lib.gfix_landau_sequence.restype = C.c_int
+    lib.gfix_landau_sequence.argtypes = [C.POINTER(C.c_void_p), C.c_size_t, _szp,
+                                         C.POINTER(GfixParams), C.POINTER(GfixResult)]
     lib.gfix_landau_driver.restype = C.c_int
     lib.gfix_landau_driver.argtypes = [C.c_void_p, _szp, C.POINTER(GfixParams),
                                        C.POINTER(GfixResult), _dp, _dp]

@@ -158,6 +158,10 @@ class Engine {
   cx<R> *d_U = nullptr, *d_G = nullptr;
   double *d_aos = nullptr;  // AoS FP64 staging (only FP64 engines)
   cx<R> *d_best = nullptr;  // luxury copies: the kept copy's links
+  // sequences (landau_sequence): a second AoS buffer and a copy stream
+  double *d_aos2 = nullptr;
+  cudaStream_t s_copy = nullptr;
+  cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_solved = nullptr;
   size_t traj_alloc = 0;
   int nb_site = 0;
   dim3 g_xy, g_zt;
@@ -206,6 +210,12 @@ class Engine {
     cudaFree(d_aos);
     cudaFree(d_best);
     d_best = nullptr;
+    cudaFree(d_aos2);
+    d_aos2 = nullptr;
+    for (cudaEvent_t &ev : ev_in)
+      if (ev) cudaEventDestroy(ev), ev = nullptr;
+    if (ev_solved) cudaEventDestroy(ev_solved), ev_solved = nullptr;
+    if (s_copy) cudaStreamDestroy(s_copy), s_copy = nullptr;
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (s) cudaStreamDestroy(s);
@@ -1615,6 +1625,49 @@ static int landau_staged(E *e64, const gfix_params *gp, gfix_result *r) {
   return 0;
 }
 
+// n configurations of one shape fixed one after another by one engine
+// (each as landau_staged, results r[0..n-1]), the host links of the next
+// configuration crossing to the device, and those of the previous one back,
+// on a copy stream while the current one is being solved.  The engine's AoS
+// buffer alternates with a second one: configuration i is staged into
+// buffer i % 2, whose previous contents (configuration i - 2) left it
+// earlier on the same copy stream.
+template <typename E>
+static int sequence_staged(E *e, double *const *links, size_t n,
+                           const gfix_params *gp, gfix_result *r) {
+  const size_t bytes = (size_t)e->V * 36 * sizeof(double2);
+  if (!e->d_aos2) CK(cudaMalloc(&e->d_aos2, bytes));
+  if (!e->s_copy) {
+    CK(cudaStreamCreateWithFlags(&e->s_copy, cudaStreamNonBlocking));
+    for (cudaEvent_t &ev : e->ev_in)
+      CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&e->ev_solved, cudaEventDisableTiming));
+  }
+  double *const buf[2] = {e->d_aos, e->d_aos2};
+  CK(cudaStreamSynchronize(e->s));
+  CK(cudaMemcpyAsync(buf[0], links[0], bytes, cudaMemcpyHostToDevice, e->s_copy));
+  CK(cudaEventRecord(e->ev_in[0], e->s_copy));
+  int rc = 0;
+  for (size_t i = 0; i < n && rc == 0; i++) {
+    const int j = (int)(i & 1);
+    if (i + 1 < n) {
+      CK(cudaMemcpyAsync(buf[j ^ 1], links[i + 1], bytes, cudaMemcpyHostToDevice,
+                         e->s_copy));
+      CK(cudaEventRecord(e->ev_in[j ^ 1], e->s_copy));
+    }
+    CK(cudaStreamWaitEvent(e->s, e->ev_in[j], 0));
+    e->d_aos = buf[j];
+    rc = landau_staged(e, gp, &r[i]);
+    e->d_aos = buf[0];
+    if (rc) break;
+    CK(cudaEventRecord(e->ev_solved, e->s));
+    CK(cudaStreamWaitEvent(e->s_copy, e->ev_solved, 0));
+    CK(cudaMemcpyAsync(links[i], buf[j], bytes, cudaMemcpyDeviceToHost, e->s_copy));
+  }
+  CK(cudaStreamSynchronize(e->s_copy));
+  return rc;
+}
+
 // ---------------------------------------------------------------------
 // Batches: many configurations, of any shapes, fixed together.  Every
 // configuration keeps its own engine (buffers, device control block,
@@ -1975,6 +2028,19 @@ int gfix_landau(double *links, const size_t dims[4], const gfix_params *p,
   if (!links) return fail("null links");
   HostArray io(links);
   return gfix::landau_io(io, dims, p, r);
+}
+
+int gfix_landau_sequence(double *const *links, size_t n, const size_t dims[4],
+                         const gfix_params *p, gfix_result *r) {
+  if (check_params(dims, p)) return -1;
+  if (n == 0) return 0;
+  if (!links || !r) return fail("null argument");
+  for (size_t i = 0; i < n; i++)
+    if (!links[i]) return fail("null links of configuration %zu", i);
+  return with_landau_engine(dims, p->precision, [&](auto *e) -> int {
+    if (p->precision == GFIX_MIXED && !engine32(dims)) return -1;
+    return sequence_staged(e, links, n, p, r);
+  });
 }
 
 int gfix_landau_device(double *d_links, const size_t dims[4],

@@ -110,6 +110,26 @@ def landau_fix(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
                      restarts=int(r.restarts))
 
 
+def landau_sequence(configs, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
+                    algo="FACG", sd_fixed_step=False, precision="FP64",
+                    switch_theta=1e-9, max_restarts=0, restart_seed=0) -> list:
+    """Copies of `configs` (same shape) fixed one after another through
+    gfix_landau_sequence, each exactly as landau_fix would fix it; the host
+    copies of neighbouring configurations overlap the solves."""
+    lib = _lib.load()
+    cd, d = _dims(dims)
+    Us = [_links(u, d) for u in configs]
+    p, _, _ = _params(gf_alpha, accuracy, max_iters, algo, sd_fixed_step,
+                      precision, switch_theta, 0, max_restarts, restart_seed, 0, False)
+    n = len(Us)
+    ptrs = (C.c_void_p * max(n, 1))(*[u.ctypes.data for u in Us])
+    rs = (GfixResult * max(n, 1))()
+    check(lib.gfix_landau_sequence(ptrs, n, cd, C.byref(p), rs))
+    return [FixResult(U, int(r.iters), float(r.theta), int(r.iters_fp32),
+                      float(r.gpu_ms), np.zeros(0), np.zeros(0), restarts=int(r.restarts))
+            for U, r in zip(Us, rs)]
+
+
 def coulomb_fix(links, dims, gf_alpha=0.08, accuracy=1e-14, max_iters=1000,
                 algo="FACG", sd_fixed_step=False, precision="FP64",
                 switch_theta=1e-9, traj_cap=0) -> FixResult:

@@ -171,6 +171,19 @@ typedef struct gfix_result {
 int gfix_landau(double *links, const size_t dims[4], const gfix_params *p,
                 gfix_result *r);
 
+/* n configurations of one lattice shape fixed one after another, exactly as
+ * n gfix_landau calls would fix them (results r[0..n-1], links[i] written
+ * back in place), through one set of device workspaces: while
+ * configuration i is solved, the links of configuration i+1 cross to the
+ * device and those of i-1 back on a copy stream.  The copies overlap the
+ * solves when the host arrays are pinned (cudaHostAlloc, cudaHostRegister);
+ * from pageable memory the results are the same, the overlap is lost.  A
+ * trajectory, when asked for, is the last configuration's.  n = 0 does
+ * nothing.  No reference counterpart: GLU's program fixes one
+ * configuration per run. */
+int gfix_landau_sequence(double *const *links, size_t n, const size_t dims[4],
+                         const gfix_params *p, gfix_result *r);
+
 /* GLU's Landau driver (src/Gfix/Landau.c:261-374) as one device-resident
  * sequence: gfix_landau (with p->max_restarts random restarts; Landau()
  * passes GF_GLU_FAILURES - 1 = 6) and, when it converged, output_fixing_info

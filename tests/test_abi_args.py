@@ -1,6 +1,7 @@
 """Argument errors of the C-ABI entry points are reported before any device work.
 
-The solvers (gfix_landau, gfix_coulomb and their _device forms), the
+The solvers (gfix_landau, gfix_coulomb and their _device forms,
+gfix_landau_sequence), the
 allocation-free theta/functional, the NERSC codec, the gluon-propagator
 measurement and the heatbath generator validate their dimensions, parameters
 and pointers first: a bad call returns -1 with a message in the matching
@@ -75,6 +76,21 @@ def test_null_links_and_params_rejected(lib, fn):
     assert rc == -1 and "null links" in err
     rc, err = _call(lib, fn, (2, 2, 2, 2), None)
     assert rc == -1 and "null dims or params" in err
+
+
+def test_sequence_arguments_rejected(lib):
+    """gfix_landau_sequence: the parameters as gfix_landau's, then the
+    pointer array and every configuration's pointer; n = 0 is a no-op."""
+    cd = (C.c_size_t * 4)(2, 2, 2, 2)
+    r = (GfixResult * 2)()
+    assert lib.gfix_landau_sequence(None, 0, cd, C.byref(_params()), r) == 0
+    assert lib.gfix_landau_sequence(None, 2, cd, C.byref(_params(algo=7)), r) == -1
+    assert "unknown algo 7" in lib.gfix_last_error().decode()
+    assert lib.gfix_landau_sequence(None, 2, cd, C.byref(_params()), r) == -1
+    assert "null argument" in lib.gfix_last_error().decode()
+    ptrs = (C.c_void_p * 2)(LINKS.ctypes.data, None)
+    assert lib.gfix_landau_sequence(ptrs, 2, cd, C.byref(_params()), r) == -1
+    assert "null links of configuration 1" in lib.gfix_last_error().decode()
 
 
 def test_null_batch_rejected(lib):

@@ -1,7 +1,9 @@
 """Batches of configurations (gfix_batch_*): every configuration of a batch
 must come out exactly as from its own gfix_landau call -- the batch runs
 each configuration's kernel sequence unchanged, only concurrently, with
-converged configurations masked out.  All calls go through the C ABI."""
+converged configurations masked out.  Sequences (gfix_landau_sequence) the
+same, one configuration after another with overlapped copies.  All calls go
+through the C ABI."""
 import numpy as np
 import pytest
 
@@ -88,3 +90,37 @@ def test_empty_batch_and_bad_index():
             _lib.check(lib.gfix_batch_result(b, 3, C.byref(r)))
     finally:
         lib.gfix_batch_destroy(b)
+
+
+@pytest.mark.parametrize("precision", ["FP64", "MIXED"])
+def test_sequence_equals_single_fixes(precision):
+    """gfix_landau_sequence on pinned host links (the copies of neighbouring
+    configurations then overlap the solves): every configuration exactly as
+    its own gfix_landau call -- links bit for bit, iterations, theta -- and
+    its links written back to its own array."""
+    import ctypes as C
+    from glu_b200 import _lib
+    from glu_b200._lib import GfixParams, GfixResult, check
+    from glu_b200.workload import heatbath_config
+    d = (16, 16, 16, 32)
+    Us = [heatbath_config(d, seed=s, iterations=40) for s in (11, 12, 13)]
+    lib = _lib.load()
+    host = [torch.from_numpy(u.view(np.float64).reshape(-1).copy()).pin_memory() for u in Us]
+    p = GfixParams()
+    p.gf_alpha, p.accuracy, p.max_iters = 0.08, 1e-12, 2000
+    p.precision = 1 if precision == "MIXED" else 0
+    p.switch_theta = 1e-9
+    ptrs = (C.c_void_p * 3)(*[h.data_ptr() for h in host])
+    rs = (GfixResult * 3)()
+    cd = (C.c_size_t * 4)(*d)
+    check(lib.gfix_landau_sequence(ptrs, 3, cd, C.byref(p), rs))
+    for U, h, r in zip(Us, host, rs):
+        ref = gfix.landau_fix(U, d, 0.08, 1e-12, 2000, "FACG", precision=precision)
+        assert r.iters == ref.iters != gfix.SENTINEL
+        assert r.theta == ref.theta
+        assert np.array_equal(h.numpy().view(np.complex128).reshape(-1, 4, 3, 3), ref.links)
+    # pageable arrays through the Python wrapper: the same results
+    seq = gfix.landau_sequence(Us[:2], d, 0.08, 1e-12, 2000, precision=precision)
+    for U, s in zip(Us[:2], seq):
+        ref = gfix.landau_fix(U, d, 0.08, 1e-12, 2000, "FACG", precision=precision)
+        assert s.iters == ref.iters and np.array_equal(s.links, ref.links)
