@@ -53,6 +53,9 @@ MAX_ITERS = 20000
 # gauge invariance: the average plaquette of a fixed configuration equals
 # the input's to this absolute tolerance
 PLAQ_TOL = 1e-13
+# the B200's nominal HBM3e bandwidth (GB/s), reported beside the fraction of
+# the measured copy peak
+HBM_NOMINAL_GBS = 8000.0
 
 
 def parse():
@@ -582,6 +585,7 @@ def gpu_line(args, dims, world, res, cpu):
         "roofline": {"bound": "hbm", "kernel": f"{KERNELS[k]} ({tag})",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src,
+                     "frac_of_nominal": achieved / HBM_NOMINAL_GBS,
                      "traffic": traffic, "algorithmic_bytes": k_by,
                      "share_of_fix": top[0] / tot if tot else None,
                      "per_kernel": per_kernel},
@@ -836,6 +840,7 @@ def coulomb_line(args, dims, world, res, cpu):
         "roofline": {"bound": "hbm", "kernel": "%s (%s)" % (C_KERNELS[k], tag),
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src,
+                     "frac_of_nominal": achieved / HBM_NOMINAL_GBS,
                      "traffic": traffic, "algorithmic_bytes": pb[k],
                      "per_kernel": {"%s:%s" % (C_KERNELS[j], t):
                                     {"ms": round(res["prof"][t][0][j], 5),
@@ -1417,6 +1422,7 @@ def gluonprop_main(args, dims, rank, world, local):
                        parallelism="one configuration per GPU" if world > 1 else "single GPU"),
         "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                     "frac_of_nominal": achieved / HBM_NOMINAL_GBS,
                      "peak_source": peak_src,
                      "other": {"k_cut_zt" if dom[0] == "k_cut_xy" else "k_cut_xy":
                                ((zt_bytes / zt_ms if dom[0] == "k_cut_xy" else xy_bytes / xy_ms)
@@ -1574,6 +1580,7 @@ def heatbath_main(args, dims, rank, world, local):
                        parallelism="one lattice per GPU" if world > 1 else "single GPU"),
         "roofline": {"bound": "hbm", "kernel": "k_update", "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "frac_of_nominal": achieved / HBM_NOMINAL_GBS,
                      "traffic": traffic_from_profiles("k_update_hb", "fp64", dims),
                      "peak_source": peak_src},
         "e2e": {"value": world * steps * 3600e3 / ms_host, "unit": H_UNIT,
