@@ -124,3 +124,20 @@ def test_sequence_equals_single_fixes(precision):
     for U, s in zip(Us[:2], seq):
         ref = gfix.landau_fix(U, d, 0.08, 1e-12, 2000, "FACG", precision=precision)
         assert s.iters == ref.iters and np.array_equal(s.links, ref.links)
+
+
+def test_sequence_keeps_restart_accounting(hb8):
+    """A sequence passes every parameter on: with max_iters below what the
+    configurations need and random restarts allowed, each configuration's
+    count, restarts and links equal its own gfix_landau call's (GLU's
+    accounting: sentinel + max_iters per failed restart + the successful
+    count, or GLU_FAILURE)."""
+    d = _dims(hb8)
+    Us = [hb8["links"], _transformed(hb8["links"], d, 21)]
+    seq = gfix.landau_sequence(Us, d, 0.08, 1e-14, 40, max_restarts=3, restart_seed=7)
+    for U, s in zip(Us, seq):
+        ref = gfix.landau_fix(U, d, 0.08, 1e-14, 40, "FACG", max_restarts=3,
+                              restart_seed=7)
+        assert ref.iters != gfix.SENTINEL
+        assert (s.iters, s.restarts) == (ref.iters, ref.restarts)
+        assert np.array_equal(s.links, ref.links)
