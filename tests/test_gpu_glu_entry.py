@@ -370,3 +370,55 @@ def test_relinked_program_at_the_headline_shape(headline_config, tmp_path, preci
     print("\n[%s] Landau() in GLU's program %.3f s (%d iterations;%s); "
           "gfix_landau_driver end to end %.3f s (best of %d after the first %.3f s)"
           % (precision, t_call, it, phases, min(times[1:]), len(times) - 1, times[0]))
+
+
+def test_relinked_program_coulomb_at_the_headline_shape(headline_config, tmp_path):
+    """GLU's relinked program fixing every time slice of the 32^3x64
+    benchmark configuration to Coulomb gauge through Coulomb() (FP64): the
+    reported iteration total and final plaquette equal gfix_coulomb_driver's
+    on the same links; GLU's [TIMER] around the call is printed beside the
+    flat driver's end-to-end time, with the phases of the call."""
+    from glu_b200 import nersc
+    from glu_b200._lib import GfixParams, GfixResult, check
+    gpu = ROOT / "oracle" / "_ref" / "glu_gpu"
+    if not gpu.exists():
+        pytest.skip("oracle/_ref/glu_gpu not built")
+    d = (32, 32, 32, 64)
+    cfg = tmp_path / "hb.nersc"
+    nersc.write(cfg, headline_config, d, datatype="4D_SU3_GAUGE_3x3")
+    inp = tmp_path / "in"
+    inp.write_text(INPUT.format(d0=d[0], d1=d[1], d2=d[2], d3=d[3], gftype="COULOMB",
+                                tune=0.08, max_iters=4000))
+    env = dict(os.environ, GLU_GFIX_TIMING="1")
+    p = subprocess.run([str(gpu), "-i", str(inp), "-c", str(cfg)], cwd=tmp_path,
+                       env=env, capture_output=True, text=True, timeout=900)
+    assert p.returncode == 0, p.stderr[-2000:]
+    out = p.stdout
+    timers = [float(x) for x in re.findall(r"\[TIMER\] elapsed :: ([0-9.e+-]+) s", out)]
+    assert len(timers) >= 2
+    phases = re.search(r"\[GF\] GPU timing(.*)", out).group(1)
+    it = int(re.search(r"\[GF\] Tuning :: [0-9.]+ \|\| Iterations :: (\d+)", out).group(1))
+    plaq = float(re.findall(r"\[GF\] Plaquette :: ([0-9.]+)", out)[-1])
+
+    lib = _lib.load()
+    host = torch.from_numpy(headline_config.view(np.float64).reshape(-1)).pin_memory()
+    work = torch.empty_like(host).pin_memory()
+    cd = (C.c_size_t * 4)(*d)
+    prm = GfixParams()
+    prm.gf_alpha, prm.accuracy, prm.max_iters = 0.08, 1e-14, 4000
+    r = GfixResult()
+    o0, g0, o1, g1 = np.zeros(3), np.zeros(6), np.zeros(3), np.zeros(6)
+    dp = C.POINTER(C.c_double)
+    times = []
+    for _ in range(2):
+        work.copy_(host)
+        t0 = time.perf_counter()
+        check(lib.gfix_coulomb_driver(work.data_ptr(), cd, C.byref(prm), C.byref(r),
+                                      o0.ctypes.data_as(dp), g0.ctypes.data_as(dp),
+                                      o1.ctypes.data_as(dp), g1.ctypes.data_as(dp)))
+        times.append(time.perf_counter() - t0)
+    assert it == r.iters
+    assert abs(plaq - o1[2]) < 1e-13
+    print("\n[COULOMB] Coulomb() in GLU's program %.3f s (%d slice iterations;%s); "
+          "gfix_coulomb_driver end to end %.3f s (after a first call of %.3f s)"
+          % (timers[1], it, phases, times[1], times[0]))
