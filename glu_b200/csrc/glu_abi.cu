@@ -173,14 +173,15 @@ struct SiteLinks final : gfix::LinkIO {
 
 // Inside a GLU program the device context is created, and the ring
 // allocated, on a thread started when the library is loaded, while the
-// program reads its configuration (the context alone takes 1.3-1.9 s to
-// create on a B200); every entry point waits for that thread before its
-// own first CUDA call.  The program's CUDA modules -- this library's -- are
-// loaded with the context (CUDA_MODULE_LOADING=EAGER unless the
-// environment sets it), not at each kernel's first launch inside the
-// call: at 32^3x64 Landau() then took 0.85 s (FP64) and 0.58 s (mixed)
-// inside GLU's program, against 0.79 and 0.53 s for the flat driver on
-// links already in pinned memory with its workspaces warm.  A program
+// program starts up, reads and checks its configuration (creating the
+// context takes up to 1.9 s on a B200); every entry point waits for that
+// thread before its own first CUDA call.  The program's CUDA modules --
+// this library's -- are loaded with the context (CUDA_MODULE_LOADING=EAGER
+// unless the environment sets it), not at each kernel's first launch
+// inside the call: at 32^3x64 Landau() then took 0.82-0.85 s (FP64) and
+// 0.56-0.64 s (mixed) inside GLU's program in most runs, against 0.79 and
+// 0.53 s for the flat driver on links already in pinned memory with its
+// workspaces warm.  A program
 // is GLU's when its own definition of Latt overrides the library's weak
 // one.  GLU_GFIX_PREINIT=0 turns all this off.  The thread is detached and
 // its state never destroyed, so that a program which exits without
