@@ -436,18 +436,25 @@ __host__ __device__ constexpr int ct_threads(int n) {
 __host__ __device__ constexpr int ct_minb(int n) {
   return 1024 / ct_threads(n) < 1 ? 1 : 1024 / ct_threads(n);
 }
-// threads of a z(,t) tile of n elements of type R: FP32 tiles of 8192
-// elements (66 KB of shared memory) take 512 threads, 16 elements each, so
-// that two blocks share an SM and each runs while the other waits at a
-// barrier (0.094 against 0.105 ms per 32^3x64 pass with one 1024-thread
-// block); FP64 tiles of that size fill an SM's shared memory alone
+// z(,t) tiles of n elements of type R that take two blocks per SM: FP32
+// tiles of 8192 elements and more whose shared memory fits twice (the
+// 4x32x64 and 2x48x96 tiles, 66 and 74 KB) run n/16 threads, 16 elements
+// each, so that each block's stages run while the other waits at a barrier:
+// 0.094 against 0.105 ms per 32^3x64 pass with one 1024-thread block, 0.768
+// against 0.864 ms per 48^3x96 pass with one 576-thread block.  FP64 tiles
+// of those sizes fill an SM's shared memory alone.
+template <typename R>
+__host__ __device__ constexpr bool zt_two_blocks(int n) {
+  return sizeof(R) == 4 && n >= 8192 && 2 * n * 8 <= 200 * 1024;
+}
 template <typename R>
 __host__ __device__ constexpr int zt_threads(int n) {
-  return (sizeof(R) == 4 && n == 8192) ? 512 : ct_threads(n);
+  return zt_two_blocks<R>(n) ? n / 16 : ct_threads(n);
 }
 template <typename R>
 __host__ __device__ constexpr int zt_minb(int n) {
-  return 1024 / zt_threads<R>(n) < 1 ? 1 : 1024 / zt_threads<R>(n);
+  return zt_two_blocks<R>(n) ? 2
+                             : (1024 / zt_threads<R>(n) < 1 ? 1 : 1024 / zt_threads<R>(n));
 }
 // padding of the t-stride of a zt tile of B x columns: t-planes start B
 // elements apart modulo 8, so the z-stage pencils of 8 (FP64) or 16 (FP32)
