@@ -1601,6 +1601,81 @@ def heatbath_main(args, dims, rank, world, local):
         emit(line)
 
 
+# The other configurations of the benchmark table, each run as its own
+# bench.py process after the headline's measurement (rank 0 of a one-GPU
+# default run), so that the default run's line records them too: the
+# ensemble (FASD, mixed), Landau 48^3x96 (one beta 6.2 configuration) and
+# Coulomb 64^3x128.  Bounded by OTHERS_BUDGET_S seconds in all
+# (GLU_GFIX_BENCH_OTHERS_S overrides; 0 turns this off); a workload that
+# would not fit, fails or prints no line is listed as skipped, with why.
+OTHERS_BUDGET_S = 780.0
+OTHER_WORKLOADS = [
+    ("ensemble", ["--workload", "ensemble"], 300.0),
+    ("landau 48x48x48x96", ["--dims", "48,48,48,96", "--beta", "6.2", "--configs", "1"], 300.0),
+    ("coulomb 64x64x64x128", ["--workload", "coulomb"], 360.0),
+]
+
+
+def compact_line(line: dict) -> dict:
+    """The figures of another workload's bench line kept in the default
+    line: metric, value, end-to-end value, step time, iteration counts,
+    the FP64 comparison, the roofline fraction and the clocks."""
+    c = line.get("config", {})
+    keep = {k: line.get(k) for k in ("metric", "value", "unit", "steps", "warmup",
+                                     "ms_per_step", "dtype", "data")}
+    keep["e2e"] = (line.get("e2e") or {}).get("value")
+    keep["workload"] = c.get("workload")
+    for k in ("iters_per_config", "iters_total", "iters_min_max", "slice_iters_max",
+              "iters", "final_theta_max", "plaquette_change_max"):
+        if k in c:
+            keep[k] = c[k]
+    f64 = c.get("fp64_only")
+    if isinstance(f64, dict):
+        keep["fp64_only"] = {k: f64.get(k) for k in ("value", "e2e")}
+    r = line.get("roofline") or {}
+    keep["roofline"] = {k: r.get(k) for k in ("kernel", "frac", "unit", "achieved")}
+    keep["clocks"] = line.get("clocks")
+    return keep
+
+
+def other_workloads() -> list:
+    budget = float(os.environ.get("GLU_GFIX_BENCH_OTHERS_S", OTHERS_BUDGET_S))
+    if budget <= 0:
+        return []
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "LOCAL_WORLD_SIZE")}
+    t0 = time.monotonic()
+    out = []
+    for name, extra, limit in OTHER_WORKLOADS:
+        left = budget - (time.monotonic() - t0)
+        if left < 60.0:
+            out.append({"workload": name, "skipped": "the default run's time budget "
+                        "(%.0f s) is spent" % budget})
+            continue
+        cmd = [sys.executable, str(ROOT / "bench.py"), *extra, "--steps", "1",
+               "--warmup", "3", "--no-cpu-baseline"]
+        t1 = time.monotonic()
+        try:
+            p = subprocess.run(cmd, capture_output=True, text=True, cwd=str(ROOT),
+                               env=env, timeout=min(limit, left))
+            lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+            if p.returncode != 0 or not lines:
+                tail = (p.stderr or p.stdout).strip().splitlines()[-1:] or [""]
+                out.append({"workload": name, "skipped": "exit %d: %s" % (p.returncode,
+                                                                           tail[0][:200])})
+                continue
+            rec = compact_line(json.loads(lines[-1]))
+            rec["command"] = "python bench.py " + " ".join(cmd[2:])
+            rec["wall_s"] = round(time.monotonic() - t1, 1)
+            out.append(rec)
+        except subprocess.TimeoutExpired:
+            out.append({"workload": name, "skipped": "did not finish within %.0f s"
+                        % min(limit, left)})
+        except Exception as e:  # reported, never fatal to the headline line
+            out.append({"workload": name, "skipped": str(e)[:200]})
+    return out
+
+
 def main():
     args = parse()
     if args.dims is None:
@@ -1650,7 +1725,16 @@ def main():
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "kind": "unavailable", "sample": str(e)}
     if rank == 0:
-        emit(gpu_line(args, dims, world, res, cpu))
+        line = gpu_line(args, dims, world, res, cpu)
+        if world == 1 and args.dims == "32,32,32,64":
+            # the headline's workspaces and tensors go before the others run
+            import torch
+            from glu_b200 import _lib
+            del res, U
+            _lib.load().gfix_release()
+            torch.cuda.empty_cache()
+            line["other_workloads"] = other_workloads()
+        emit(line)
 
 
 if __name__ == "__main__":

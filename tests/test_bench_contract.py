@@ -111,3 +111,42 @@ def test_gpu_arm_fails_loudly_without_cuda(workload):
                        cwd=ROOT, env=env, capture_output=True, text=True, timeout=240)
     assert r.returncode != 0
     assert _lines(r.stdout) == []
+
+
+def _bench_module():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_under_test", ROOT / "bench.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_other_workloads_are_bounded(monkeypatch):
+    """The default run's section for the benchmark table's other
+    configurations: off at a budget of 0, and every workload listed as
+    skipped (none started) when the budget cannot hold one."""
+    b = _bench_module()
+    monkeypatch.setenv("GLU_GFIX_BENCH_OTHERS_S", "0")
+    assert b.other_workloads() == []
+    monkeypatch.setenv("GLU_GFIX_BENCH_OTHERS_S", "30")
+    recs = b.other_workloads()
+    assert [r["workload"] for r in recs] == [w[0] for w in b.OTHER_WORKLOADS]
+    assert all("time budget" in r["skipped"] for r in recs)
+
+
+def test_compact_line_keeps_the_figures():
+    b = _bench_module()
+    line = {"metric": "m", "value": 2.0, "unit": "configs/hour", "steps": 1, "warmup": 3,
+            "ms_per_step": 5.0, "dtype": "f32+f64", "data": "d",
+            "e2e": {"value": 1.5, "unit": "configs/hour"},
+            "config": {"workload": "w", "iters_total": 10, "iters_min_max": [1, 9],
+                       "fp64_only": {"value": 1.0, "e2e": 0.9, "ms_per_step": 9.0}},
+            "roofline": {"kernel": "k", "frac": 0.5, "unit": "GB/s", "achieved": 3.0,
+                         "per_kernel": {}},
+            "clocks": {"sm_mhz": 1800.0}}
+    c = b.compact_line(line)
+    assert (c["metric"], c["value"], c["e2e"], c["workload"]) == ("m", 2.0, 1.5, "w")
+    assert c["iters_total"] == 10 and c["iters_min_max"] == [1, 9]
+    assert c["fp64_only"] == {"value": 1.0, "e2e": 0.9}
+    assert c["roofline"] == {"kernel": "k", "frac": 0.5, "unit": "GB/s", "achieved": 3.0}
+    assert c["clocks"] == {"sm_mhz": 1800.0}
