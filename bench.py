@@ -1211,6 +1211,47 @@ def ensemble_main(args, rank, world, local):
         "gpu_launches": o["launches"],
         "clocks": clk.summary(),
     }
+    # roofline: the kernel with the largest share of the batch's device time,
+    # from per-kernel event times of each shape and phase (gfix_profile_landau:
+    # CG iterations of the same kernels, on one configuration of the shape)
+    # weighted by the iterations the batch spent in that shape and phase
+    peak, peak_src = peaks()
+    share = []
+    i0 = 0
+    for cnt, dims in E_GROUPS:
+        its = o["iters"][i0:i0 + cnt]
+        it32 = sum(x[1] for x in its) if prec == "mixed" else 0
+        it64 = sum(x[0] for x in its) - it32
+        phases = ((("fp32", 1, it32), ("polish", 2, it64)) if prec == "mixed"
+                  else (("fp64", 0, it64),))
+        for tag, code, n_it in phases:
+            if n_it <= 0:
+                continue
+            pms, pby = np.zeros(7), np.zeros(7)
+            pp = _eparams("fp64")
+            pp.precision = code
+            check(lib.gfix_profile_landau(pristine[i0].data_ptr(), cds[i0], C.byref(pp),
+                                          args.profile_iters,
+                                          pms.ctypes.data_as(C.POINTER(C.c_double)),
+                                          pby.ctypes.data_as(C.POINTER(C.c_double))))
+            for k in range(6):
+                share.append((pms[k] * n_it, tag, dims, k, pms[k], pby[k]))
+        i0 += cnt
+    if share:
+        tot = sum(x[0] for x in share)
+        top = max(share, key=lambda x: x[0])
+        _, tag, dims, k, k_ms, k_by = top
+        achieved = k_by / (k_ms * 1e-3) / 1e9
+        line["roofline"] = {"bound": "hbm",
+                            "kernel": "%s (%s, %s)" % (KERNELS[k], tag, "x".join(map(str, dims))),
+                            "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "peak_source": peak_src,
+                            "frac_of_nominal": achieved / HBM_NOMINAL_GBS,
+                            # no ncu capture of these shapes: their fields fit
+                            # in L2, so scaling the 32^3x64 one would mislead
+                            "traffic": None,
+                            "algorithmic_bytes": k_by,
+                            "share_of_fix": top[0] / tot if tot else None}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             f64 = out["fp64"]["device"]["iters"]
