@@ -84,3 +84,46 @@ def flush_c_stdio():
     """Flush the C library's stdio buffers (output of printf in the library)."""
     libc = C.CDLL(None)
     libc.fflush(None)
+
+
+# GLU input file for its own program: gauge fixing of a NERSC configuration
+# (GFTYPE LANDAU or COULOMB), with the other sections GLU's parser reads
+GLU_INPUT = """MODE = GAUGE_FIXING
+HEADER = NERSC
+	DIM_0 = {d0}
+	DIM_1 = {d1}
+	DIM_2 = {d2}
+	DIM_3 = {d3}
+CONFNO = 400
+RANDOM_TRANSFORM = NO
+SEED = 0
+GFTYPE = {gftype}
+	GF_TUNE = {tune}
+	ACCURACY = 14
+	MAX_ITERS = {max_iters}
+CUTTYPE = GLUON_PROPS
+	FIELD_DEFINITION = LINEAR
+	MOM_CUT = CYLINDER_CUT
+	MAX_T = 7
+	MAXMOM = 4
+	CYL_WIDTH = 2.0
+	ANGLE = 60
+	OUTPUT = ./
+SMEARTYPE = APE
+	DIRECTION = ALL
+	SMITERS = 100
+	ALPHA1 = 0.6
+	ALPHA2 = 0.4
+	ALPHA3 = 0.2
+U1_MEAS = U1_RECTANGLE
+	U1_ALPHA = 0.07957753876221914
+	U1_CHARGE = -1.0
+CONFIG_INFO = glu_b200_boundary_test
+	STORAGE = NERSC_GAUGE
+BETA = 6.0
+	ITERS = 1500
+	MEASURE = 1
+	OVER_ITERS = 4
+	SAVE = 25
+	THERM = 100
+"""

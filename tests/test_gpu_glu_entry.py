@@ -23,7 +23,8 @@ if not torch.cuda.is_available():
     pytest.skip("no CUDA device", allow_module_level=True)
 
 from glu_b200 import _lib, gfix  # noqa: E402
-from glu_structs import FftwStuff, Site, SiteLattice, fftw_fields, flush_c_stdio, set_latt  # noqa: E402
+from glu_structs import (GLU_INPUT as INPUT, FftwStuff, Site, SiteLattice,  # noqa: E402
+                         fftw_fields, flush_c_stdio, set_latt)
 
 ROOT = Path(__file__).resolve().parents[1]
 GOLDEN = ROOT / "tests" / "golden"
@@ -211,45 +212,7 @@ def test_chunked_staging_of_a_large_site_lattice(lib, hb24x16, capfd):
 
 # --- GLU's own program, relinked ------------------------------------------
 
-INPUT = """MODE = GAUGE_FIXING
-HEADER = NERSC
-	DIM_0 = {d0}
-	DIM_1 = {d1}
-	DIM_2 = {d2}
-	DIM_3 = {d3}
-CONFNO = 400
-RANDOM_TRANSFORM = NO
-SEED = 0
-GFTYPE = {gftype}
-	GF_TUNE = {tune}
-	ACCURACY = 14
-	MAX_ITERS = {max_iters}
-CUTTYPE = GLUON_PROPS
-	FIELD_DEFINITION = LINEAR
-	MOM_CUT = CYLINDER_CUT
-	MAX_T = 7
-	MAXMOM = 4
-	CYL_WIDTH = 2.0
-	ANGLE = 60
-	OUTPUT = ./
-SMEARTYPE = APE
-	DIRECTION = ALL
-	SMITERS = 100
-	ALPHA1 = 0.6
-	ALPHA2 = 0.4
-	ALPHA3 = 0.2
-U1_MEAS = U1_RECTANGLE
-	U1_ALPHA = 0.07957753876221914
-	U1_CHARGE = -1.0
-CONFIG_INFO = glu_b200_boundary_test
-	STORAGE = NERSC_GAUGE
-BETA = 6.0
-	ITERS = 1500
-	MEASURE = 1
-	OVER_ITERS = 4
-	SAVE = 25
-	THERM = 100
-"""
+
 
 
 def _run(binary, tmp_path, gftype, tune, tag):
